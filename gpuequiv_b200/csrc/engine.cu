@@ -1,0 +1,1696 @@
+// engine.cu - the energy-game fixpoint on the B200.
+//
+// Reference path: EnergyGame::run -> GPURunner::execute_gpu
+// (src/energygame.rs:379-383, :1461-1523) with the attack shaders
+// (attack_update.wgsl:77-113, attack_minimize.wgsl:180-235) and the defend
+// shaders (defend_update.wgsl:73-101, defend_iterative.wgsl:283-368).
+//
+// The reference runs a Jacobi worklist: every round it gathers the successor
+// energies of all queued positions on the host, uploads them, runs the four
+// shaders, maps the results back and rebuilds the queues from the reverse
+// graph.  Here the whole loop stays on the device:
+//
+//   * The game (CSR + reverse CSR), the per-position energy lists and the
+//     frontier queues are resident in HBM.  An energy list is a slice of one
+//     energy arena; position v's descriptor desc[v] = (offset << 24 | count).
+//   * k_round: one warp per frontier position reads its successors' lists
+//     straight from the arena (no gather copy), applies the inverse edge
+//     update, minimises (attacker) or intersects up-sets (defender), writes
+//     the new list to fresh arena space and, if the list changed, appends
+//     its predecessors to the next frontier (deduplicated by round stamps).
+//   * k_commit: publishes the new descriptors (Jacobi: every position of a
+//     round reads the lists of the previous round) and flips the frontier.
+//   * Rounds are launched as CUDA graphs of several rounds each; the host
+//     reads one small counter block per graph launch to detect termination.
+//
+// Results are identical to the reference's: the same positions are recomputed
+// in the same rounds from the same inputs.  The one scheduling difference is
+// that the reference delays a defender by a round when its preallocated
+// suprema list overflows (energygame.rs:919-923); here the combination is
+// bounded by a 4096-bit up-set bitmap and never needs a retry.  Such delays
+// cannot change the final lists: both update operators are monotone on
+// up-closed sets, every position is recomputed after its successors' last
+// change, so the worklist ends in the least fixpoint whatever the round in
+// which a position is recomputed; the attacker and multi-successor defender
+// lists are the minimal elements of that fixpoint, and a single-successor
+// defender's list is the image of its successor's list.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "codec.cuh"
+#include "geq_internal.h"
+
+namespace geq {
+
+#ifndef GEQ_CHECKED
+#define GEQ_CHECKED 0
+#endif
+
+constexpr uint32_t FULL = 0xffffffffu;
+constexpr unsigned long long NONE_DESC = ~0ull;
+constexpr uint32_t CNT_MASK = (1u << 24) - 1u;
+constexpr uint32_t ALLOC_CHUNK = 256;
+constexpr int WARPS_PER_BLOCK = 8;
+constexpr int BLOCK = 32 * WARPS_PER_BLOCK;
+// per-warp shared memory (u32 words)
+constexpr int SM_BM = 0;      // 128 words: bitmap
+constexpr int SM_BM2 = 128;   // 128 words: second bitmap (own / old list)
+constexpr int SM_TMP = 256;   // 32 words: segment map / compaction
+constexpr int SM_WORDS = 288;
+// device error bits (Ctr::error)
+constexpr uint32_t DERR_LIST = 1u;     // a list longer than 2^24 - 1 energies
+constexpr uint32_t DERR_BOUNDS = 2u;   // checked build: index out of range
+constexpr uint32_t DERR_SCRATCH = 4u;  // list-path combination too large
+
+// Device-resident control block.  Mutable pointers live here (not in the
+// kernel parameters) so that captured CUDA graphs stay valid across arena
+// compactions.
+struct Ctr {
+  uint32_t *arena;
+  unsigned long long arena_cap;
+  unsigned long long arena_top;
+  uint32_t fsize[2];
+  uint32_t cur;
+  uint32_t stamp;  // stamp of the current frontier
+  uint32_t overflow;
+  uint32_t halt;
+  uint32_t error;
+  uint32_t err_line;
+  uint32_t done_blocks;
+  uint32_t pad;
+  unsigned long long positions, edges, bytes, rounds;
+};
+
+struct KParams {
+  const uint32_t *row, *col, *wt, *rrow, *rcol;
+  const uint8_t *flags;
+  unsigned long long *desc;
+  uint32_t *mark;
+  uint32_t *front0, *front1;
+  unsigned long long *slot_new;
+  Ctr *ctr;
+  unsigned long long n_nodes, n_edges;
+  uint32_t el, mx, eb, em, ub, um;
+  uint32_t small_limit;
+};
+
+__device__ __forceinline__ unsigned long long mkdesc(unsigned long long off, uint32_t cnt) {
+  return (off << 24) | (unsigned long long)cnt;
+}
+__device__ __forceinline__ uint32_t dcnt(unsigned long long d) { return (uint32_t)(d & CNT_MASK); }
+__device__ __forceinline__ unsigned long long doff(unsigned long long d) { return d >> 24; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+#if GEQ_CHECKED
+__device__ __noinline__ void report_bounds(Ctr *c, int line) {
+  atomicOr(&c->error, DERR_BOUNDS);
+  atomicMax(&c->err_line, (uint32_t)line);
+  atomicExch(&c->halt, 1u);
+}
+#define CHECK_IDX(c, idx, size) \
+  (((unsigned long long)(idx) < (unsigned long long)(size)) ? true : (report_bounds((c), __LINE__), false))
+#else
+#define CHECK_IDX(c, idx, size) true
+#endif
+
+// Guarded loads: in the checked build an out-of-range index records an
+// error and reads 0 instead of touching memory.
+template <class T>
+__device__ __forceinline__ T ld(const T *a, unsigned long long i, unsigned long long n, Ctr *c) {
+  return CHECK_IDX(c, i, n) ? a[i] : T(0);
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, uint32_t lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(FULL, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  return x;
+}
+
+// ---- per-warp arena allocator ------------------------------------------
+struct WarpAlloc {
+  unsigned long long cur, end;
+  // Reserve `cnt` energies.  Lane-uniform.  false on arena overflow.
+  __device__ __forceinline__ bool alloc(uint32_t cnt, Ctr *c, unsigned long long cap, uint32_t lane,
+                                        unsigned long long &out) {
+    if (cur + cnt > end) {
+      unsigned long long grab = cnt > ALLOC_CHUNK ? cnt : ALLOC_CHUNK;
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(&c->arena_top, grab);
+      base = __shfl_sync(FULL, base, 0);
+      if (base + grab > cap) {
+        if (lane == 0) atomicExch(&c->overflow, 1u);
+        cur = end = 0;
+        return false;
+      }
+      cur = base;
+      end = base + grab;
+    }
+    out = cur;
+    cur += cnt;
+    return true;
+  }
+};
+
+// ---- bitmap up-set algebra over {0..3}^6 (CodecStd) ----------------------
+// A 4096-bit set indexed by the packed energy is spread over the warp: lane l
+// holds bits [128l, 128l+128) as w0 (low 64) and w1.  Element i of the
+// energy is bits [2i, 2i+2) of the index, so dims 0-2 move bits inside a
+// word, dim 3 moves between w0/w1 and between lane pairs, dims 4-5 move
+// between lanes.
+struct BM {
+  unsigned long long w0, w1;
+};
+__device__ __forceinline__ unsigned long long cl012(unsigned long long x) {
+  x |= (x & 0x7777777777777777ull) << 1;
+  x |= (x & 0x3333333333333333ull) << 2;
+  x |= (x & 0x0FFF0FFF0FFF0FFFull) << 4;
+  x |= (x & 0x00FF00FF00FF00FFull) << 8;
+  x |= (x & 0x0000FFFFFFFFFFFFull) << 16;
+  x |= (x & 0x00000000FFFFFFFFull) << 32;
+  return x;
+}
+// Upward closure: every energy >= some member.
+__device__ __forceinline__ BM up_closure(BM b, uint32_t lane) {
+  b.w0 = cl012(b.w0);
+  b.w1 = cl012(b.w1);
+  b.w1 |= b.w0;
+  unsigned long long t = __shfl_up_sync(FULL, b.w1, 1);
+  if (lane & 1u) { b.w0 |= t; b.w1 |= t; }
+  const uint32_t v4 = (lane >> 1) & 3u, v5 = (lane >> 3) & 3u;
+  unsigned long long t0 = __shfl_up_sync(FULL, b.w0, 2), t1 = __shfl_up_sync(FULL, b.w1, 2);
+  if (v4 >= 1u) { b.w0 |= t0; b.w1 |= t1; }
+  t0 = __shfl_up_sync(FULL, b.w0, 4);
+  t1 = __shfl_up_sync(FULL, b.w1, 4);
+  if (v4 >= 2u) { b.w0 |= t0; b.w1 |= t1; }
+  t0 = __shfl_up_sync(FULL, b.w0, 8);
+  t1 = __shfl_up_sync(FULL, b.w1, 8);
+  if (v5 >= 1u) { b.w0 |= t0; b.w1 |= t1; }
+  t0 = __shfl_up_sync(FULL, b.w0, 16);
+  t1 = __shfl_up_sync(FULL, b.w1, 16);
+  if (v5 >= 2u) { b.w0 |= t0; b.w1 |= t1; }
+  return b;
+}
+__device__ __forceinline__ unsigned long long st012(unsigned long long x) {
+  return ((x & 0x7777777777777777ull) << 1) | ((x & 0x0FFF0FFF0FFF0FFFull) << 4) |
+         ((x & 0x0000FFFFFFFFFFFFull) << 16);
+}
+// One step up in any single element: {e + unit_i}.
+__device__ __forceinline__ BM step_up(BM b, uint32_t lane) {
+  BM s;
+  s.w0 = st012(b.w0);
+  s.w1 = st012(b.w1) | b.w0;
+  unsigned long long t = __shfl_up_sync(FULL, b.w1, 1);
+  if (lane & 1u) s.w0 |= t;
+  const uint32_t v4 = (lane >> 1) & 3u, v5 = (lane >> 3) & 3u;
+  unsigned long long t0 = __shfl_up_sync(FULL, b.w0, 2), t1 = __shfl_up_sync(FULL, b.w1, 2);
+  if (v4 >= 1u) { s.w0 |= t0; s.w1 |= t1; }
+  t0 = __shfl_up_sync(FULL, b.w0, 8);
+  t1 = __shfl_up_sync(FULL, b.w1, 8);
+  if (v5 >= 1u) { s.w0 |= t0; s.w1 |= t1; }
+  return s;
+}
+__device__ __forceinline__ BM bm_load(const uint32_t *sm, uint32_t lane) {
+  BM b;
+  b.w0 = (unsigned long long)sm[4 * lane] | ((unsigned long long)sm[4 * lane + 1] << 32);
+  b.w1 = (unsigned long long)sm[4 * lane + 2] | ((unsigned long long)sm[4 * lane + 3] << 32);
+  return b;
+}
+__device__ __forceinline__ void bm_set(uint32_t *sm, uint32_t idx) {
+  idx &= 0xFFFu;
+  atomicOr(&sm[idx >> 5], 1u << (idx & 31u));
+}
+
+// Write the members of `m` (ascending index order) as packed energies.
+__device__ __forceinline__ void bm_emit(BM m, uint32_t lane, uint32_t *arena, unsigned long long off,
+                                        uint32_t excl) {
+  unsigned long long k = off + excl;
+  unsigned long long w = m.w0;
+  while (w) {
+    uint32_t b = (uint32_t)__ffsll((long long)w) - 1u;
+    arena[k++] = lane * 128u + b;
+    w &= w - 1ull;
+  }
+  w = m.w1;
+  while (w) {
+    uint32_t b = (uint32_t)__ffsll((long long)w) - 1u;
+    arena[k++] = lane * 128u + 64u + b;
+    w &= w - 1ull;
+  }
+}
+
+template <class Cd>
+__device__ __forceinline__ Cd make_codec(const KParams &p);
+template <>
+__device__ __forceinline__ CodecStd make_codec<CodecStd>(const KParams &) { return CodecStd{}; }
+template <>
+__device__ __forceinline__ CodecGen make_codec<CodecGen>(const KParams &p) {
+  return CodecGen(p.el, p.mx, p.eb, p.em, p.ub, p.um);
+}
+
+enum : int { R_UNCHANGED = 0, R_CHANGED = 1, R_OVERFLOW = 2, R_SKIPPED = 3, R_ERROR = 4 };
+struct Res {
+  int st;
+  unsigned long long off;
+  uint32_t cnt;
+};
+
+struct WarpCtx {
+  const KParams &p;
+  Ctr *c;
+  uint32_t *arena;
+  unsigned long long cap;
+  uint32_t lane;
+  uint32_t *sm;
+  WarpAlloc &wa;
+  unsigned long long &edges, &bytes;
+};
+
+// Successor descriptor of edge k (lane-local).
+struct EdgeInfo {
+  uint32_t u, cw;
+  unsigned long long ow;
+};
+__device__ __forceinline__ EdgeInfo edge_info(const WarpCtx &x, unsigned long long k) {
+  EdgeInfo e{0, 0, 0};
+  uint32_t w = ld(x.p.col, k, x.p.n_edges, x.c);
+  e.u = ld(x.p.wt, k, x.p.n_edges, x.c);
+  unsigned long long d = ld(x.p.desc, w, x.p.n_nodes, x.c);
+  e.cw = dcnt(d);
+  e.ow = doff(d);
+  return e;
+}
+
+// ---- attacker ------------------------------------------------------------
+// attack_update.wgsl:77-113 + attack_minimize.wgsl:180-235: candidates are
+// the inverse-updated successor energies followed by the own energies; keep
+// the minimal ones (on ties the later copy, so own energies win); the
+// position changed iff a kept candidate came from a successor.
+template <class Cd>
+__device__ Res attack_small(const WarpCtx &x, const Cd &cd, uint32_t v, unsigned long long e0, uint32_t d,
+                            uint32_t cv, unsigned long long ov, bool &fits) {
+  const uint32_t lane = x.lane;
+  EdgeInfo ei{0, 0, 0};
+  if (lane < d) ei = edge_info(x, e0 + lane);
+  const uint32_t incl = warp_incl_scan(ei.cw, lane);
+  const uint32_t tot = __shfl_sync(FULL, incl, 31);
+  const uint32_t K = tot + cv;
+  if (K > x.p.small_limit) {
+    fits = false;
+    return Res{R_UNCHANGED, 0, 0};
+  }
+  fits = true;
+  x.bytes += 16ull * d + 4ull * tot;
+  const uint32_t excl = incl - ei.cw;
+  for (uint32_t k = excl; k < incl; k++) x.sm[SM_TMP + k] = lane;
+  __syncwarp();
+  const uint32_t i = lane;
+  const uint32_t ed = (i < tot) ? x.sm[SM_TMP + i] : 0u;
+  __syncwarp();
+  const unsigned long long ow_e = __shfl_sync(FULL, ei.ow, ed);
+  const uint32_t ex_e = __shfl_sync(FULL, excl, ed);
+  const uint32_t u_e = __shfl_sync(FULL, ei.u, ed);
+  const bool valid = i < K;
+  uint32_t cnd = 0;
+  if (i < tot) cnd = cd.upd(cd.to_t(ld(x.arena, ow_e + (i - ex_e), x.cap, x.c)), u_e);
+  else if (valid) cnd = cd.to_t(ld(x.arena, ov + (i - tot), x.cap, x.c));
+  bool killed = false;
+  for (uint32_t j = 0; j < K; j++) {
+    uint32_t cj = __shfl_sync(FULL, cnd, j);
+    if (valid && j != i) {
+      bool eq = cj == cnd;
+      if ((eq && i < j) || (!eq && t_leq(cj, cnd))) killed = true;
+    }
+  }
+  const bool kept = valid && !killed;
+  const uint32_t bal = __ballot_sync(FULL, kept);
+  const bool changed = __ballot_sync(FULL, kept && i < tot) != 0u;
+  if (!changed) return Res{R_UNCHANGED, 0, 0};
+  const uint32_t cnt = __popc(bal);
+  unsigned long long off = 0;
+  if (!x.wa.alloc(cnt, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
+  if (kept) {
+    unsigned long long k = off + __popc(bal & lanemask_lt());
+    if (CHECK_IDX(x.c, k, x.cap)) x.arena[k] = cd.to_p(cnd);
+  }
+  x.bytes += 4ull * cnt;
+  return Res{R_CHANGED, off, cnt};
+}
+
+// Large attacker positions on STANDARD: candidates go into a 4096-bit set;
+// minimal members = set minus the strict up-closure of the set.
+__device__ Res attack_bitmap(const WarpCtx &x, const CodecStd &cd, uint32_t v, unsigned long long e0,
+                             unsigned long long e1, uint32_t cv, unsigned long long ov) {
+  const uint32_t lane = x.lane;
+  for (uint32_t k = lane; k < 256u; k += 32u) x.sm[SM_BM + k] = 0u;
+  __syncwarp();
+  unsigned long long tot = 0;
+  for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
+    EdgeInfo ei{0, 0, 0};
+    if (k0 + lane < e1) ei = edge_info(x, k0 + lane);
+    const uint32_t nk = (uint32_t)min(32ull, e1 - k0);
+    for (uint32_t j = 0; j < nk; j++) {
+      const uint32_t cwj = __shfl_sync(FULL, ei.cw, j);
+      const unsigned long long owj = __shfl_sync(FULL, ei.ow, j);
+      const uint32_t uj = __shfl_sync(FULL, ei.u, j);
+      tot += cwj;
+      for (uint32_t q = lane; q < cwj; q += 32u)
+        bm_set(x.sm + SM_BM, cd.to_p(cd.upd(cd.to_t(ld(x.arena, owj + q, x.cap, x.c)), uj)));
+    }
+  }
+  x.bytes += 16ull * (e1 - e0) + 4ull * tot;
+  for (uint32_t q = lane; q < cv; q += 32u) {
+    uint32_t idx = ld(x.arena, ov + q, x.cap, x.c);
+    bm_set(x.sm + SM_BM, idx);
+    bm_set(x.sm + SM_BM2, idx);
+  }
+  __syncwarp();
+  const BM b = bm_load(x.sm + SM_BM, lane);
+  const BM own = bm_load(x.sm + SM_BM2, lane);
+  __syncwarp();
+  const BM su = up_closure(step_up(b, lane), lane);
+  BM m;
+  m.w0 = b.w0 & ~su.w0;
+  m.w1 = b.w1 & ~su.w1;
+  const bool changed = __ballot_sync(FULL, ((m.w0 & ~own.w0) | (m.w1 & ~own.w1)) != 0ull) != 0u;
+  if (!changed) return Res{R_UNCHANGED, 0, 0};
+  const uint32_t c = (uint32_t)(__popcll(m.w0) + __popcll(m.w1));
+  const uint32_t incl = warp_incl_scan(c, lane);
+  const uint32_t total = __shfl_sync(FULL, incl, 31);
+  unsigned long long off = 0;
+  if (!x.wa.alloc(total, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
+  if (CHECK_IDX(x.c, off + total - 1, x.cap)) bm_emit(m, lane, x.arena, off, incl - c);
+  x.bytes += 4ull * total;
+  return Res{R_CHANGED, off, total};
+}
+
+// Large attacker positions on other confs: candidates in arena scratch,
+// pairwise minimisation.  Same tie rule as attack_minimize.wgsl.
+template <class Cd>
+__device__ Res attack_list(const WarpCtx &x, const Cd &cd, uint32_t v, unsigned long long e0,
+                           unsigned long long e1, uint32_t cv, unsigned long long ov) {
+  const uint32_t lane = x.lane;
+  unsigned long long K = cv;
+  for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
+    EdgeInfo ei{0, 0, 0};
+    if (k0 + lane < e1) ei = edge_info(x, k0 + lane);
+    uint32_t incl = warp_incl_scan(ei.cw, lane);
+    K += __shfl_sync(FULL, incl, 31);
+  }
+  if (K > CNT_MASK) {
+    if (lane == 0) { atomicOr(&x.c->error, DERR_SCRATCH); atomicExch(&x.c->halt, 1u); }
+    return Res{R_ERROR, 0, 0};
+  }
+  unsigned long long sc = 0;
+  if (!x.wa.alloc((uint32_t)K, x.c, x.cap, lane, sc)) return Res{R_OVERFLOW, 0, 0};
+  unsigned long long pos = 0;
+  for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
+    EdgeInfo ei{0, 0, 0};
+    if (k0 + lane < e1) ei = edge_info(x, k0 + lane);
+    const uint32_t nk = (uint32_t)min(32ull, e1 - k0);
+    for (uint32_t j = 0; j < nk; j++) {
+      const uint32_t cwj = __shfl_sync(FULL, ei.cw, j);
+      const unsigned long long owj = __shfl_sync(FULL, ei.ow, j);
+      const uint32_t uj = __shfl_sync(FULL, ei.u, j);
+      for (uint32_t q = lane; q < cwj; q += 32u)
+        if (CHECK_IDX(x.c, sc + pos + q, x.cap))
+          x.arena[sc + pos + q] = cd.upd(cd.to_t(ld(x.arena, owj + q, x.cap, x.c)), uj);
+      pos += cwj;
+    }
+  }
+  x.bytes += 16ull * (e1 - e0) + 4ull * pos;
+  const unsigned long long tot = pos;
+  for (uint32_t q = lane; q < cv; q += 32u)
+    if (CHECK_IDX(x.c, sc + tot + q, x.cap)) x.arena[sc + tot + q] = cd.to_t(ld(x.arena, ov + q, x.cap, x.c));
+  __syncwarp();
+  unsigned long long out = 0;
+  if (!x.wa.alloc((uint32_t)K, x.c, x.cap, lane, out)) return Res{R_OVERFLOW, 0, 0};
+  uint32_t cnt = 0;
+  bool changed = false;
+  for (unsigned long long i0 = 0; i0 < K; i0 += 32) {
+    const unsigned long long i = i0 + lane;
+    bool kept = false;
+    uint32_t ci = 0;
+    if (i < K) {
+      ci = ld(x.arena, sc + i, x.cap, x.c);
+      kept = true;
+      for (unsigned long long j = 0; j < K; j++) {
+        if (j == i) continue;
+        uint32_t cj = ld(x.arena, sc + j, x.cap, x.c);
+        bool eq = cj == ci;
+        if ((eq && i < j) || (!eq && t_leq(cj, ci))) { kept = false; break; }
+      }
+    }
+    const uint32_t bal = __ballot_sync(FULL, kept);
+    if (__ballot_sync(FULL, kept && i < tot)) changed = true;
+    if (kept) {
+      unsigned long long k = out + cnt + __popc(bal & lanemask_lt());
+      if (CHECK_IDX(x.c, k, x.cap)) x.arena[k] = cd.to_p(ci);
+    }
+    cnt += __popc(bal);
+  }
+  if (!changed) return Res{R_UNCHANGED, 0, 0};
+  x.bytes += 4ull * cnt;
+  return Res{R_CHANGED, out, cnt};
+}
+
+// ---- defender --------------------------------------------------------------
+// Reference semantics (energygame.rs:896-944 with defend_iterative.wgsl):
+// the new list is min{ a_1 v ... v a_d : a_k in upd_k(A_{w_k}) } (the first
+// successor's updated list is taken as is when there is only one successor);
+// the position changed iff the new list is not equal to the old one under
+// EnergyArray's PartialEq (energy.rs:334-350: same length and every new
+// energy occurs in the old list).
+
+// changed-test for a new list held in lanes (n <= 32) against the old list.
+template <class Cd>
+__device__ bool differs_small(const WarpCtx &x, const Cd &cd, uint32_t newp, uint32_t n, uint32_t cv,
+                              unsigned long long ov) {
+  if (n != cv) return true;
+  const uint32_t lane = x.lane;
+  const uint32_t o = (lane < cv) ? ld(x.arena, ov + lane, x.cap, x.c) : 0u;
+  bool found = false;
+  for (uint32_t j = 0; j < cv; j++) found |= (__shfl_sync(FULL, o, j) == newp);
+  return __ballot_sync(FULL, lane < n && !found) != 0u;
+}
+
+template <class Cd>
+__device__ Res defend_single(const WarpCtx &x, const Cd &cd, const EdgeInfo &e, uint32_t cv,
+                             unsigned long long ov) {
+  const uint32_t lane = x.lane;
+  const uint32_t n = e.cw;
+  x.bytes += 16ull + 4ull * n;
+  bool changed;
+  if (n != cv) {
+    changed = true;
+  } else if (n <= 32u) {
+    uint32_t np = (lane < n) ? cd.to_p(cd.upd(cd.to_t(ld(x.arena, e.ow + lane, x.cap, x.c)), e.u)) : 0u;
+    changed = differs_small(x, cd, np, n, cv, ov);
+  } else if (Cd::kBitmap) {
+    for (uint32_t k = lane; k < 128u; k += 32u) x.sm[SM_BM2 + k] = 0u;
+    __syncwarp();
+    for (uint32_t q = lane; q < cv; q += 32u) bm_set(x.sm + SM_BM2, ld(x.arena, ov + q, x.cap, x.c));
+    __syncwarp();
+    bool miss = false;
+    for (uint32_t q = lane; q < n; q += 32u) {
+      uint32_t idx = cd.to_p(cd.upd(cd.to_t(ld(x.arena, e.ow + q, x.cap, x.c)), e.u)) & 0xFFFu;
+      miss |= ((x.sm[SM_BM2 + (idx >> 5)] >> (idx & 31u)) & 1u) == 0u;
+    }
+    changed = __ballot_sync(FULL, miss) != 0u;
+    __syncwarp();
+  } else {
+    bool miss = false;
+    for (uint32_t q = lane; q < n; q += 32u) {
+      uint32_t np = cd.to_p(cd.upd(cd.to_t(ld(x.arena, e.ow + q, x.cap, x.c)), e.u));
+      bool found = false;
+      for (uint32_t j = 0; j < cv && !found; j++) found = ld(x.arena, ov + j, x.cap, x.c) == np;
+      miss |= !found;
+    }
+    changed = __ballot_sync(FULL, miss) != 0u;
+  }
+  if (!changed) return Res{R_UNCHANGED, 0, 0};
+  unsigned long long off = 0;
+  if (!x.wa.alloc(n, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
+  for (uint32_t q = lane; q < n; q += 32u)
+    if (CHECK_IDX(x.c, off + q, x.cap))
+      x.arena[off + q] = cd.to_p(cd.upd(cd.to_t(ld(x.arena, e.ow + q, x.cap, x.c)), e.u));
+  x.bytes += 4ull * n;
+  return Res{R_CHANGED, off, n};
+}
+
+// Fold of up to 32 successors whose pairwise combinations stay <= 32: the
+// running antichain lives in one register per lane.
+template <class Cd>
+__device__ Res defend_small(const WarpCtx &x, const Cd &cd, unsigned long long e0, uint32_t d, uint32_t cv,
+                            unsigned long long ov, bool &fits) {
+  const uint32_t lane = x.lane;
+  EdgeInfo ei{0, 0, 0};
+  if (lane < d) ei = edge_info(x, e0 + lane);
+  uint32_t s = __shfl_sync(FULL, ei.cw, 0);
+  fits = false;
+  if (s > x.p.small_limit) return Res{R_UNCHANGED, 0, 0};
+  {
+    const unsigned long long ow0 = __shfl_sync(FULL, ei.ow, 0);
+    const uint32_t u0 = __shfl_sync(FULL, ei.u, 0);
+    uint32_t S = (lane < s) ? cd.upd(cd.to_t(ld(x.arena, ow0 + lane, x.cap, x.c)), u0) : 0u;
+    for (uint32_t k = 1; k < d; k++) {
+      const uint32_t cb = __shfl_sync(FULL, ei.cw, k);
+      const unsigned long long ob = __shfl_sync(FULL, ei.ow, k);
+      const uint32_t ub = __shfl_sync(FULL, ei.u, k);
+      const uint32_t combos = s * cb;
+      if (combos > x.p.small_limit) return Res{R_UNCHANGED, 0, 0};  // fits stays false
+      const uint32_t l = lane;
+      const bool valid = l < combos;
+      const uint32_t a = __shfl_sync(FULL, S, valid ? (l % s) : 0u);
+      uint32_t cc = 0;
+      if (valid) cc = a | cd.upd(cd.to_t(ld(x.arena, ob + l / s, x.cap, x.c)), ub);
+      bool killed = false;
+      for (uint32_t j = 0; j < combos; j++) {
+        uint32_t cj = __shfl_sync(FULL, cc, j);
+        if (valid && j != l) {
+          bool eq = cj == cc;
+          if ((eq && l > j) || (!eq && t_leq(cj, cc))) killed = true;
+        }
+      }
+      const bool kept = valid && !killed;
+      const uint32_t bal = __ballot_sync(FULL, kept);
+      if (kept) x.sm[SM_TMP + __popc(bal & lanemask_lt())] = cc;
+      __syncwarp();
+      s = __popc(bal);
+      S = (lane < s) ? x.sm[SM_TMP + lane] : 0u;
+      __syncwarp();
+    }
+    fits = true;
+    unsigned long long tot = 0;
+    if (lane < d) tot = ei.cw;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(FULL, tot, o);
+    x.bytes += 16ull * d + 4ull * tot;
+    const uint32_t np = (lane < s) ? cd.to_p(S) : 0u;
+    if (!differs_small(x, cd, np, s, cv, ov)) return Res{R_UNCHANGED, 0, 0};
+    unsigned long long off = 0;
+    if (!x.wa.alloc(s, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
+    if (lane < s && CHECK_IDX(x.c, off + lane, x.cap)) x.arena[off + lane] = np;
+    x.bytes += 4ull * s;
+    return Res{R_CHANGED, off, s};
+  }
+}
+
+// STANDARD defender with large lists: intersect the up-closures of the
+// updated successor lists in a 4096-bit set, then take its minimal members.
+__device__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0,
+                             unsigned long long e1, uint32_t cv, unsigned long long ov) {
+  const uint32_t lane = x.lane;
+  BM acc;
+  acc.w0 = ~0ull;
+  acc.w1 = ~0ull;
+  unsigned long long tot = 0;
+  for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
+    EdgeInfo ei{0, 0, 0};
+    if (k0 + lane < e1) ei = edge_info(x, k0 + lane);
+    const uint32_t nk = (uint32_t)min(32ull, e1 - k0);
+    for (uint32_t j = 0; j < nk; j++) {
+      const uint32_t cwj = __shfl_sync(FULL, ei.cw, j);
+      const unsigned long long owj = __shfl_sync(FULL, ei.ow, j);
+      const uint32_t uj = __shfl_sync(FULL, ei.u, j);
+      tot += cwj;
+      for (uint32_t k = lane; k < 128u; k += 32u) x.sm[SM_BM + k] = 0u;
+      __syncwarp();
+      for (uint32_t q = lane; q < cwj; q += 32u)
+        bm_set(x.sm + SM_BM, cd.to_p(cd.upd(cd.to_t(ld(x.arena, owj + q, x.cap, x.c)), uj)));
+      __syncwarp();
+      const BM u = up_closure(bm_load(x.sm + SM_BM, lane), lane);
+      __syncwarp();
+      acc.w0 &= u.w0;
+      acc.w1 &= u.w1;
+    }
+  }
+  x.bytes += 16ull * (e1 - e0) + 4ull * tot;
+  const BM st = step_up(acc, lane);
+  BM m;
+  m.w0 = acc.w0 & ~st.w0;
+  m.w1 = acc.w1 & ~st.w1;
+  for (uint32_t k = lane; k < 128u; k += 32u) x.sm[SM_BM2 + k] = 0u;
+  __syncwarp();
+  for (uint32_t q = lane; q < cv; q += 32u) bm_set(x.sm + SM_BM2, ld(x.arena, ov + q, x.cap, x.c));
+  __syncwarp();
+  const BM old = bm_load(x.sm + SM_BM2, lane);
+  __syncwarp();
+  const uint32_t c = (uint32_t)(__popcll(m.w0) + __popcll(m.w1));
+  const uint32_t incl = warp_incl_scan(c, lane);
+  const uint32_t total = __shfl_sync(FULL, incl, 31);
+  const bool changed =
+      total != cv || __ballot_sync(FULL, ((m.w0 & ~old.w0) | (m.w1 & ~old.w1)) != 0ull) != 0u;
+  if (!changed) return Res{R_UNCHANGED, 0, 0};
+  unsigned long long off = 0;
+  if (!x.wa.alloc(total, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
+  if (CHECK_IDX(x.c, off + total - 1, x.cap)) bm_emit(m, lane, x.arena, off, incl - c);
+  x.bytes += 4ull * total;
+  return Res{R_CHANGED, off, total};
+}
+
+// Other confs with large lists: the fold of defend_iterative.wgsl with the
+// running list and the combinations in arena scratch.
+template <class Cd>
+__device__ Res defend_list(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
+                           uint32_t cv, unsigned long long ov) {
+  const uint32_t lane = x.lane;
+  EdgeInfo f{0, 0, 0};
+  if (lane == 0) f = edge_info(x, e0);
+  f.cw = __shfl_sync(FULL, f.cw, 0);
+  f.ow = __shfl_sync(FULL, f.ow, 0);
+  f.u = __shfl_sync(FULL, f.u, 0);
+  unsigned long long S = 0;
+  uint32_t s = f.cw;
+  if (!x.wa.alloc(s, x.c, x.cap, lane, S)) return Res{R_OVERFLOW, 0, 0};
+  for (uint32_t q = lane; q < s; q += 32u)
+    if (CHECK_IDX(x.c, S + q, x.cap)) x.arena[S + q] = cd.upd(cd.to_t(ld(x.arena, f.ow + q, x.cap, x.c)), f.u);
+  unsigned long long tot = s;
+  __syncwarp();
+  for (unsigned long long k = e0 + 1; k < e1; k++) {
+    EdgeInfo b{0, 0, 0};
+    if (lane == 0) b = edge_info(x, k);
+    b.cw = __shfl_sync(FULL, b.cw, 0);
+    b.ow = __shfl_sync(FULL, b.ow, 0);
+    b.u = __shfl_sync(FULL, b.u, 0);
+    tot += b.cw;
+    const unsigned long long combos = (unsigned long long)s * b.cw;
+    if (combos > (1ull << 22)) {
+      if (lane == 0) { atomicOr(&x.c->error, DERR_SCRATCH); atomicExch(&x.c->halt, 1u); }
+      return Res{R_ERROR, 0, 0};
+    }
+    unsigned long long C = 0, N = 0;
+    if (!x.wa.alloc((uint32_t)combos, x.c, x.cap, lane, C)) return Res{R_OVERFLOW, 0, 0};
+    if (!x.wa.alloc((uint32_t)combos, x.c, x.cap, lane, N)) return Res{R_OVERFLOW, 0, 0};
+    for (unsigned long long l = lane; l < combos; l += 32)
+      if (CHECK_IDX(x.c, C + l, x.cap))
+        x.arena[C + l] = ld(x.arena, S + l % s, x.cap, x.c) |
+                         cd.upd(cd.to_t(ld(x.arena, b.ow + l / s, x.cap, x.c)), b.u);
+    __syncwarp();
+    uint32_t cnt = 0;
+    for (unsigned long long l0 = 0; l0 < combos; l0 += 32) {
+      const unsigned long long l = l0 + lane;
+      bool kept = false;
+      uint32_t cl = 0;
+      if (l < combos) {
+        cl = ld(x.arena, C + l, x.cap, x.c);
+        kept = true;
+        for (unsigned long long j = 0; j < combos; j++) {
+          if (j == l) continue;
+          uint32_t cj = ld(x.arena, C + j, x.cap, x.c);
+          bool eq = cj == cl;
+          if ((eq && l > j) || (!eq && t_leq(cj, cl))) { kept = false; break; }
+        }
+      }
+      const uint32_t bal = __ballot_sync(FULL, kept);
+      if (kept) {
+        unsigned long long kk = N + cnt + __popc(bal & lanemask_lt());
+        if (CHECK_IDX(x.c, kk, x.cap)) x.arena[kk] = cl;
+      }
+      cnt += __popc(bal);
+    }
+    __syncwarp();
+    S = N;
+    s = cnt;
+  }
+  x.bytes += 16ull * (e1 - e0) + 4ull * tot;
+  // changed test: same length and every new energy among the old ones
+  bool changed = s != cv;
+  if (!changed) {
+    bool miss = false;
+    for (uint32_t q = lane; q < s; q += 32u) {
+      uint32_t np = cd.to_p(ld(x.arena, S + q, x.cap, x.c));
+      bool found = false;
+      for (uint32_t j = 0; j < cv && !found; j++) found = ld(x.arena, ov + j, x.cap, x.c) == np;
+      miss |= !found;
+    }
+    changed = __ballot_sync(FULL, miss) != 0u;
+  }
+  if (!changed) return Res{R_UNCHANGED, 0, 0};
+  unsigned long long off = 0;
+  if (!x.wa.alloc(s, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
+  for (uint32_t q = lane; q < s; q += 32u)
+    if (CHECK_IDX(x.c, off + q, x.cap)) x.arena[off + q] = cd.to_p(ld(x.arena, S + q, x.cap, x.c));
+  x.bytes += 4ull * s;
+  return Res{R_CHANGED, off, s};
+}
+
+template <class Cd>
+__device__ Res solve_position(const WarpCtx &x, const Cd &cd, uint32_t v) {
+  const uint32_t lane = x.lane;
+  const unsigned long long e0 = ld(x.p.row, v, x.p.n_nodes + 1, x.c);
+  const unsigned long long e1 = ld(x.p.row, (unsigned long long)v + 1, x.p.n_nodes + 1, x.c);
+  const uint32_t d = (uint32_t)(e1 - e0);
+  const unsigned long long dv = ld(x.p.desc, v, x.p.n_nodes, x.c);
+  const uint32_t cv = dcnt(dv);
+  const unsigned long long ov = doff(dv);
+  const bool attacker = ld(x.p.flags, v, x.p.n_nodes, x.c) & 1u;
+  if (d == 0) return Res{R_SKIPPED, 0, 0};
+  if (attacker) {
+    x.edges += d;
+    x.bytes += 12ull + 4ull * cv;
+    if (d <= 32u && x.p.small_limit > 0) {
+      bool fits = false;
+      Res r = attack_small(x, cd, v, e0, d, cv, ov, fits);
+      if (fits) return r;
+    }
+    if constexpr (Cd::kBitmap) return attack_bitmap(x, cd, v, e0, e1, cv, ov);
+    else return attack_list(x, cd, v, e0, e1, cv, ov);
+  }
+  // defender: skipped while a successor has no energies (energygame.rs:789-792)
+  bool empty = false;
+  for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
+    bool e = false;
+    if (k0 + lane < e1) {
+      uint32_t w = ld(x.p.col, k0 + lane, x.p.n_edges, x.c);
+      e = dcnt(ld(x.p.desc, w, x.p.n_nodes, x.c)) == 0u;
+    }
+    if (__ballot_sync(FULL, e)) { empty = true; break; }
+  }
+  if (empty) return Res{R_SKIPPED, 0, 0};
+  x.edges += d;
+  x.bytes += 12ull;
+  if (d == 1u) {
+    EdgeInfo e{0, 0, 0};
+    if (lane == 0) e = edge_info(x, e0);
+    e.cw = __shfl_sync(FULL, e.cw, 0);
+    e.ow = __shfl_sync(FULL, e.ow, 0);
+    e.u = __shfl_sync(FULL, e.u, 0);
+    return defend_single(x, cd, e, cv, ov);
+  }
+  if (d <= 32u && x.p.small_limit > 0) {
+    bool fits = false;
+    Res r = defend_small(x, cd, e0, d, cv, ov, fits);
+    if (fits) return r;
+  }
+  if constexpr (Cd::kBitmap) return defend_bitmap(x, cd, e0, e1, cv, ov);
+  else return defend_list(x, cd, e0, e1, cv, ov);
+}
+
+// Append the predecessors of v (reverse CSR) to the next frontier once.
+__device__ void push_preds(const KParams &p, Ctr *c, uint32_t v, uint32_t *NF, uint32_t *nf_size,
+                           uint32_t stamp, uint32_t lane) {
+  const unsigned long long b = ld(p.rrow, v, p.n_nodes + 1, c), e = ld(p.rrow, (unsigned long long)v + 1, p.n_nodes + 1, c);
+  for (unsigned long long k0 = b; k0 < e; k0 += 32) {
+    const unsigned long long k = k0 + lane;
+    bool first = false;
+    uint32_t u = 0;
+    if (k < e) {
+      u = ld(p.rcol, k, p.n_edges, c);
+      if (CHECK_IDX(c, u, p.n_nodes)) first = atomicMax(&p.mark[u], stamp) < stamp;
+    }
+    const uint32_t bal = __ballot_sync(FULL, first);
+    if (bal) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(nf_size, (uint32_t)__popc(bal));
+      base = __shfl_sync(FULL, base, 0);
+      if (first) {
+        uint32_t slot = base + __popc(bal & lanemask_lt());
+        if (CHECK_IDX(c, slot, p.n_nodes)) NF[slot] = u;
+      }
+    }
+  }
+}
+
+template <class Cd>
+__global__ void __launch_bounds__(BLOCK) k_round(KParams p) {
+  __shared__ uint32_t smem[WARPS_PER_BLOCK * SM_WORDS];
+  Ctr *c = p.ctr;
+  if (c->halt) return;
+  const uint32_t cur = c->cur;
+  const uint32_t fs = c->fsize[cur];
+  if (fs == 0) return;
+  const uint32_t *F = cur ? p.front1 : p.front0;
+  uint32_t *NF = cur ? p.front0 : p.front1;
+  uint32_t *nf_size = &c->fsize[cur ^ 1u];
+  const uint32_t stamp = c->stamp + 1u;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t *sm = smem + (threadIdx.x >> 5) * SM_WORDS;
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  Cd cd = make_codec<Cd>(p);
+  WarpAlloc wa{0, 0};
+  unsigned long long edges = 0, bytes = 0, positions = 0;
+  WarpCtx x{p, c, c->arena, c->arena_cap, lane, sm, wa, edges, bytes};
+  for (uint32_t slot = gw; slot < fs; slot += nw) {
+    const uint32_t v = ld(F, slot, p.n_nodes, c);
+    Res r = solve_position(x, cd, v);
+    if (r.st != R_SKIPPED) positions++;
+    if (lane == 0 && CHECK_IDX(c, slot, p.n_nodes))
+      p.slot_new[slot] = (r.st == R_CHANGED) ? mkdesc(r.off, r.cnt) : NONE_DESC;
+    if (r.st == R_CHANGED) {
+      if (r.cnt > CNT_MASK && lane == 0) { atomicOr(&c->error, DERR_LIST); atomicExch(&c->halt, 1u); }
+      push_preds(p, c, v, NF, nf_size, stamp, lane);
+    } else if (r.st == R_OVERFLOW) {
+      // retry next round after the arena has been compacted
+      if (lane == 0 && atomicMax(&p.mark[v], stamp) < stamp) {
+        uint32_t s = atomicAdd(nf_size, 1u);
+        if (CHECK_IDX(c, s, p.n_nodes)) NF[s] = v;
+      }
+    }
+  }
+  if (lane == 0 && positions) {
+    atomicAdd(&c->positions, positions);
+    atomicAdd(&c->edges, edges);
+    atomicAdd(&c->bytes, bytes);
+  }
+}
+
+// Publish the round's new descriptors and advance to the next frontier.
+__global__ void k_commit(KParams p) {
+  Ctr *c = p.ctr;
+  // k_round only raises `overflow` (never `halt`) for arena exhaustion, so
+  // the round that overflowed still commits its finished positions; the
+  // last block then halts the remaining rounds of the graph until the host
+  // has compacted the arena.
+  if (c->halt) return;
+  const uint32_t cur = c->cur;
+  const uint32_t fs = c->fsize[cur];
+  if (fs == 0) return;
+  const uint32_t *F = cur ? p.front1 : p.front0;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < fs; s += gridDim.x * blockDim.x) {
+    const unsigned long long d = p.slot_new[s];
+    if (d != NONE_DESC) {
+      const uint32_t v = F[s];
+      if (CHECK_IDX(c, v, p.n_nodes)) p.desc[v] = d;
+    }
+  }
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&c->done_blocks, 1u) == gridDim.x - 1u;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    c->fsize[cur] = 0u;
+    c->cur = cur ^ 1u;
+    c->stamp = c->stamp + 1u;
+    c->rounds = c->rounds + 1ull;
+    c->done_blocks = 0u;
+    if (c->overflow) c->halt = 1u;
+    __threadfence();
+  }
+}
+
+}  // namespace geq
+
+// ===========================================================================
+// Support kernels: scan, reverse CSR, initial state, compaction, download.
+// ===========================================================================
+namespace geq {
+
+constexpr int SCAN_T = 1024;
+constexpr int SCAN_ITEMS = 8;
+constexpr int SCAN_TILE = SCAN_T * SCAN_ITEMS;
+
+__device__ __forceinline__ unsigned long long block_excl_scan(unsigned long long x, unsigned long long *ws,
+                                                              unsigned long long &total) {
+  const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  unsigned long long incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned long long y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  if (lane == 31u) ws[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    unsigned long long s = (lane < blockDim.x / 32) ? ws[lane] : 0ull;
+    unsigned long long si = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      unsigned long long y = __shfl_up_sync(FULL, si, o);
+      if (lane >= (uint32_t)o) si += y;
+    }
+    ws[lane] = si - s;
+    if (lane == 31u) ws[32] = si;
+  }
+  __syncthreads();
+  total = ws[32];
+  unsigned long long r = ws[w] + incl - x;
+  __syncthreads();
+  return r;
+}
+
+__global__ void k_scan_reduce(const uint32_t *in, unsigned long long n, unsigned long long *part) {
+  __shared__ unsigned long long ws[33];
+  unsigned long long base = (unsigned long long)blockIdx.x * SCAN_TILE + (unsigned long long)threadIdx.x * SCAN_ITEMS;
+  unsigned long long s = 0;
+  for (int i = 0; i < SCAN_ITEMS; i++)
+    if (base + i < n) s += in[base + i];
+  unsigned long long total;
+  block_excl_scan(s, ws, total);
+  if (threadIdx.x == 0) part[blockIdx.x] = total;
+}
+
+// Exclusive scan of the per-tile sums, one block.
+__global__ void k_scan_partials(unsigned long long *part, unsigned long long nb) {
+  __shared__ unsigned long long ws[33];
+  unsigned long long carry = 0;
+  for (unsigned long long b0 = 0; b0 < nb; b0 += SCAN_T) {
+    unsigned long long i = b0 + threadIdx.x;
+    unsigned long long x = i < nb ? part[i] : 0ull;
+    unsigned long long total;
+    unsigned long long e = block_excl_scan(x, ws, total);
+    if (i < nb) part[i] = carry + e;
+    carry += total;
+  }
+}
+
+__global__ void k_scan_apply(const uint32_t *in, unsigned long long n, const unsigned long long *part,
+                             unsigned long long *out) {
+  __shared__ unsigned long long ws[33];
+  unsigned long long base = (unsigned long long)blockIdx.x * SCAN_TILE + (unsigned long long)threadIdx.x * SCAN_ITEMS;
+  uint32_t v[SCAN_ITEMS];
+  unsigned long long s = 0;
+  for (int i = 0; i < SCAN_ITEMS; i++) {
+    v[i] = (base + i < n) ? in[base + i] : 0u;
+    s += v[i];
+  }
+  unsigned long long total;
+  unsigned long long e = block_excl_scan(s, ws, total) + part[blockIdx.x];
+  for (int i = 0; i < SCAN_ITEMS; i++) {
+    if (base + i < n) out[base + i] = e;
+    e += v[i];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) out[n] = e;
+}
+
+__global__ void k_desc_counts(const unsigned long long *desc, unsigned long long n, uint32_t *cnt) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n;
+       v += (unsigned long long)gridDim.x * blockDim.x)
+    cnt[v] = dcnt(desc[v]);
+}
+
+__global__ void k_indegree(const uint32_t *col, unsigned long long m, unsigned long long n, uint32_t *indeg,
+                           uint32_t *err) {
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < m;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t w = col[k];
+    if (w < n) atomicAdd(&indeg[w], 1u);
+    else atomicOr(err, 1u);
+  }
+}
+
+__global__ void k_u64_to_u32(const unsigned long long *in, unsigned long long n, uint32_t *out) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)in[i];
+}
+
+__global__ void k_fill_reverse(const uint32_t *row, const uint32_t *col, unsigned long long n, uint32_t *cursor,
+                               uint32_t *rcol) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n;
+       v += (unsigned long long)gridDim.x * blockDim.x) {
+    for (uint32_t k = row[v]; k < row[v + 1]; k++) {
+      uint32_t w = col[k];
+      uint32_t pos = atomicAdd(&cursor[w], 1u);
+      rcol[pos] = (uint32_t)v;
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t game_of(const unsigned long long *base, uint32_t n_games,
+                                            unsigned long long x) {
+  // largest g with base[g] <= x
+  uint32_t lo = 0, hi = n_games;
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (base[mid] <= x) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Shift per-game local ids of a concatenated batch into the global id space.
+__global__ void k_fix_rows(uint32_t *row, unsigned long long n, const unsigned long long *node_base,
+                           const unsigned long long *edge_base, uint32_t n_games) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n;
+       v += (unsigned long long)gridDim.x * blockDim.x)
+    row[v] += (uint32_t)edge_base[game_of(node_base, n_games, v)];
+}
+__global__ void k_fix_cols(uint32_t *col, unsigned long long m, const unsigned long long *node_base,
+                           const unsigned long long *edge_base, uint32_t n_games,
+                           const unsigned long long *game_nodes, uint32_t *err) {
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < m;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t g = game_of(edge_base, n_games, k);
+    uint32_t w = col[k];
+    if (w >= game_nodes[g]) atomicOr(err, 1u);
+    col[k] = w + (uint32_t)node_base[g];
+  }
+}
+
+__global__ void k_init_reach(unsigned long long *desc, const uint32_t *reach, unsigned long long n_reach,
+                             unsigned long long zero_off) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_reach;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    desc[reach[i]] = mkdesc(zero_off, 1u);
+}
+
+// initialize_visit_lists (energygame.rs:1461-1465): predecessors of to_reach.
+__global__ void k_init_frontier(KParams p, const uint32_t *reach, unsigned long long n_reach) {
+  Ctr *c = p.ctr;
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long gw = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long i = gw; i < n_reach; i += nw)
+    push_preds(p, c, reach[i], p.front0, &c->fsize[0], c->stamp, lane);
+}
+
+__global__ void k_compact(unsigned long long *desc, unsigned long long n, const unsigned long long *noff,
+                          const uint32_t *src, uint32_t *dst) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long gw = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long v = gw; v < n; v += nw) {
+    const unsigned long long d = desc[v];
+    const uint32_t c = dcnt(d);
+    const unsigned long long o = doff(d), no = noff[v];
+    for (uint32_t q = lane; q < c; q += 32u) dst[no + q] = src[o + q];
+    if (lane == 0) desc[v] = mkdesc(no, c);
+  }
+}
+
+__global__ void k_gather(const unsigned long long *desc, unsigned long long n, const unsigned long long *goff,
+                         const uint32_t *arena, uint32_t *out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long gw = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long v = gw; v < n; v += nw) {
+    const unsigned long long d = desc[v];
+    const uint32_t c = dcnt(d);
+    const unsigned long long o = doff(d), go = goff[v];
+    for (uint32_t q = lane; q < c; q += 32u) out[go + q] = arena[o + q];
+  }
+}
+
+// Per-game offsets relative to the game's first energy: game g owns entries
+// [node_base[g] + g, node_base[g+1] + g] of `rel`.
+__global__ void k_rel_offsets(const unsigned long long *goff, unsigned long long n,
+                              const unsigned long long *node_base, uint32_t n_games, unsigned long long *rel) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n + n_games;
+       v += (unsigned long long)gridDim.x * blockDim.x) {
+    if (v < n) {
+      uint32_t g = game_of(node_base, n_games, v);
+      rel[v + g] = goff[v] - goff[node_base[g]];
+    } else {
+      uint32_t g = (uint32_t)(v - n);
+      rel[node_base[g + 1] + g] = goff[node_base[g + 1]] - goff[node_base[g]];
+    }
+  }
+}
+
+// Counts of selected positions (sel = global ids).
+__global__ void k_sel_counts(const unsigned long long *desc, const uint32_t *sel, unsigned long long k,
+                             uint32_t *cnt) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    cnt[i] = dcnt(desc[sel[i]]);
+}
+__global__ void k_sel_gather(const unsigned long long *desc, const uint32_t *sel, unsigned long long k,
+                             const unsigned long long *goff, const uint32_t *arena, uint32_t *out) {
+  const uint32_t lane = threadIdx.x & 31u;
+  const unsigned long long gw = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long i = gw; i < k; i += nw) {
+    const unsigned long long d = desc[sel[i]];
+    const uint32_t c = dcnt(d);
+    const unsigned long long o = doff(d), go = goff[i];
+    for (uint32_t q = lane; q < c; q += 32u) out[go + q] = arena[o + q];
+  }
+}
+
+__global__ void k_set_arena(Ctr *c, uint32_t *arena, unsigned long long cap, unsigned long long top) {
+  c->arena = arena;
+  c->arena_cap = cap;
+  c->arena_top = top;
+  c->overflow = 0u;
+  c->halt = 0u;
+}
+
+// ===========================================================================
+// Host side
+// ===========================================================================
+#define CU(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(e_ == cudaErrorMemoryAllocation ? GEQ_ERR_OUT_OF_MEMORY : GEQ_ERR_CUDA,    \
+                  "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));        \
+  } while (0)
+
+template <class T>
+static geq_status dalloc(T *&p, size_t n) {
+  p = nullptr;
+  if (n == 0) n = 1;
+  CU(cudaMalloc((void **)&p, n * sizeof(T)));
+  return GEQ_OK;
+}
+template <class T>
+static void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+struct Engine::State {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Ctr *h_ctr = nullptr;  // pinned
+  // scan scratch
+  unsigned long long *part = nullptr;
+  size_t part_cap = 0;
+  uint32_t *cnt = nullptr;
+  size_t cnt_cap = 0;
+  // pinned staging
+  char *stage = nullptr;
+  size_t stage_cap = 0;
+  uint32_t *d_err = nullptr;
+  int grid_blocks = 0;
+};
+
+struct DeviceGamesImpl {
+  Conf conf;
+  bool generic = false;
+  uint32_t n_games = 0;
+  std::vector<unsigned long long> node_base, edge_base;  // n_games + 1
+  unsigned long long N = 0, M = 0;
+  uint32_t *row = nullptr, *col = nullptr, *wt = nullptr, *rrow = nullptr, *rcol = nullptr;
+  uint8_t *flags = nullptr;
+  unsigned long long *desc = nullptr, *desc_init = nullptr, *slot_new = nullptr;
+  uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr;
+  uint32_t *init_data = nullptr;
+  unsigned long long init_total = 0;
+  uint32_t *arena[2] = {nullptr, nullptr};
+  unsigned long long arena_cap[2] = {0, 0};
+  int arena_cur = 0;
+  uint32_t *reach = nullptr;
+  unsigned long long n_reach = 0;
+  unsigned long long *d_node_base = nullptr;
+  Ctr *ctr = nullptr;
+  uint32_t next_stamp = 1;
+  cudaGraphExec_t gexec = nullptr;
+  uint32_t graph_rounds = 0;
+  KParams kp{};
+};
+
+static geq_status scan_u32(Engine::State &s, const uint32_t *in, unsigned long long n, unsigned long long *out,
+                           unsigned long long &launches) {
+  unsigned long long nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+  if (nb == 0) nb = 1;
+  if (s.part_cap < nb) {
+    dfree(s.part);
+    size_t cap = std::max<size_t>(nb, 1024);
+    geq_status st = dalloc(s.part, cap);
+    if (st) return st;
+    s.part_cap = cap;
+  }
+  k_scan_reduce<<<(unsigned)nb, SCAN_T, 0, s.stream>>>(in, n, s.part);
+  k_scan_partials<<<1, SCAN_T, 0, s.stream>>>(s.part, nb);
+  k_scan_apply<<<(unsigned)nb, SCAN_T, 0, s.stream>>>(in, n, s.part, out);
+  launches += 3;
+  CU(cudaGetLastError());
+  return GEQ_OK;
+}
+
+static geq_status ensure_cnt(Engine::State &s, size_t n) {
+  if (s.cnt_cap >= n) return GEQ_OK;
+  dfree(s.cnt);
+  size_t cap = std::max<size_t>(n, 1 << 16);
+  geq_status st = dalloc(s.cnt, cap);
+  if (st) return st;
+  s.cnt_cap = cap;
+  return GEQ_OK;
+}
+
+static geq_status ensure_stage(Engine::State &s, size_t bytes) {
+  if (s.stage_cap >= bytes) return GEQ_OK;
+  if (s.stage) cudaFreeHost(s.stage);
+  s.stage = nullptr;
+  size_t cap = std::max<size_t>(bytes, 1 << 20);
+  cap = std::max(cap, s.stage_cap * 3 / 2);
+  CU(cudaHostAlloc((void **)&s.stage, cap, cudaHostAllocDefault));
+  s.stage_cap = cap;
+  return GEQ_OK;
+}
+
+geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(GEQ_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+  if (device < 0 || device >= n) return fail(GEQ_ERR_NO_DEVICE, "device %d out of range (%d)", device, n);
+  CU(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, device));
+  std::unique_ptr<Engine> eng(new Engine());
+  eng->st.reset(new State());
+  eng->n_sms = prop.multiProcessorCount;
+  eng->total_mem = prop.totalGlobalMem;
+  eng->name = prop.name;
+  State &s = *eng->st;
+  CU(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+  CU(cudaEventCreate(&s.ev0));
+  CU(cudaEventCreate(&s.ev1));
+  CU(cudaHostAlloc((void **)&s.h_ctr, sizeof(Ctr), cudaHostAllocDefault));
+  CU(cudaMalloc((void **)&s.d_err, sizeof(uint32_t)));
+  int bps = 0;
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_round<CodecStd>, BLOCK, 0));
+  eng->tuning.blocks_per_sm = (uint32_t)std::max(1, std::min(bps, 8));
+  eng->tuning.rounds_per_graph = 8;
+  eng->tuning.small_limit = 32;
+  out = std::move(eng);
+  return GEQ_OK;
+}
+
+Engine::~Engine() {
+  if (!st) return;
+  State &s = *st;
+  if (s.stream) cudaStreamSynchronize(s.stream);
+  dfree(s.part);
+  dfree(s.cnt);
+  dfree(s.d_err);
+  if (s.stage) cudaFreeHost(s.stage);
+  if (s.h_ctr) cudaFreeHost(s.h_ctr);
+  if (s.ev0) cudaEventDestroy(s.ev0);
+  if (s.ev1) cudaEventDestroy(s.ev1);
+  if (s.stream) cudaStreamDestroy(s.stream);
+}
+
+static void free_games(DeviceGamesImpl &dg) {
+  // cudaFree synchronises with outstanding work on the device
+  if (dg.gexec) cudaGraphExecDestroy(dg.gexec);
+  dg.gexec = nullptr;
+  dfree(dg.row); dfree(dg.col); dfree(dg.wt); dfree(dg.rrow); dfree(dg.rcol); dfree(dg.flags);
+  dfree(dg.desc); dfree(dg.desc_init); dfree(dg.slot_new); dfree(dg.mark); dfree(dg.front0);
+  dfree(dg.front1); dfree(dg.init_data); dfree(dg.arena[0]); dfree(dg.arena[1]); dfree(dg.reach);
+  dfree(dg.d_node_base); dfree(dg.ctr);
+}
+
+void destroy_games(DeviceGamesImpl *p) {
+  if (!p) return;
+  free_games(*p);
+  delete p;
+}
+
+// Pack the games into pinned staging and move them to the device.
+geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
+  State &s = *st;
+  if (games.empty()) return fail(GEQ_ERR_INVALID_INPUT, "no games");
+  GamesPtr dg(new DeviceGamesImpl());
+  dg->conf = Conf(games[0].g.conf);
+  if (!dg->conf.supported())
+    return fail(GEQ_ERR_UNSUPPORTED, "EnergyConf {%u, %u} is outside the device codecs", dg->conf.elements,
+                dg->conf.max);
+  dg->generic = !dg->conf.standard() || (tuning.flags & GEQ_TUNE_FORCE_GENERIC);
+  dg->n_games = (uint32_t)games.size();
+  dg->node_base.assign(dg->n_games + 1, 0);
+  dg->edge_base.assign(dg->n_games + 1, 0);
+  unsigned long long init_total = 0, n_reach = 0;
+  bool any_init = false;
+  for (uint32_t g = 0; g < dg->n_games; g++) {
+    const GameInput &gi = games[g];
+    if (!(Conf(gi.g.conf) == dg->conf)) return fail(GEQ_ERR_INVALID_INPUT, "games of one batch need one EnergyConf");
+    dg->node_base[g + 1] = dg->node_base[g] + gi.g.n_vertices;
+    dg->edge_base[g + 1] = dg->edge_base[g] + gi.g.row_offsets[gi.g.n_vertices];
+    if (gi.init) { any_init = true; init_total += gi.init->offsets[gi.init->n_vertices]; }
+    else init_total += 0;
+    n_reach += gi.n_reach;
+  }
+  dg->N = dg->node_base.back();
+  dg->M = dg->edge_base.back();
+  if (dg->N >= 0xFFFFFFF0ull || dg->M >= 0xFFFFFFF0ull)
+    return fail(GEQ_ERR_INVALID_INPUT, "too many positions/edges for 32-bit ids (%llu, %llu)", dg->N, dg->M);
+  const unsigned long long N = dg->N, M = dg->M;
+  // arena layout: [zero energy][initial lists ...]
+  dg->init_total = 1 + init_total;
+  dg->n_reach = n_reach;
+  // staging layout
+  size_t off_row = 0, off_col = off_row + (N + 1) * 4, off_wt = off_col + M * 4, off_flags = off_wt + M * 4;
+  size_t off_reach = (off_flags + N + 15) & ~size_t(15);
+  size_t off_init = off_reach + n_reach * 4;
+  size_t off_desc = off_init + dg->init_total * 4;
+  off_desc = (off_desc + 15) & ~size_t(15);
+  size_t off_base = off_desc + (any_init ? N * 8 : 0);
+  size_t total_bytes = off_base + (dg->n_games + 1) * 8 * 3;
+  geq_status stt = ensure_stage(s, total_bytes);
+  if (stt) return stt;
+  char *H = s.stage;
+  uint32_t *h_row = (uint32_t *)(H + off_row), *h_col = (uint32_t *)(H + off_col), *h_wt = (uint32_t *)(H + off_wt);
+  uint8_t *h_flags = (uint8_t *)(H + off_flags);
+  uint32_t *h_reach = (uint32_t *)(H + off_reach), *h_init = (uint32_t *)(H + off_init);
+  unsigned long long *h_desc = (unsigned long long *)(H + off_desc);
+  unsigned long long *h_nb = (unsigned long long *)(H + off_base);
+  unsigned long long *h_eb = h_nb + (dg->n_games + 1);
+  unsigned long long *h_gn = h_eb + (dg->n_games + 1);
+  unsigned long long ri = 0, ii = 1;
+  h_init[0] = 0;  // the zero energy of standard initialisation
+  for (uint32_t g = 0; g < dg->n_games; g++) {
+    const GameInput &gi = games[g];
+    const uint32_t n = gi.g.n_vertices;
+    const unsigned long long nb = dg->node_base[g], eb = dg->edge_base[g], m = dg->edge_base[g + 1] - eb;
+    std::memcpy(h_row + nb, gi.g.row_offsets, (size_t)n * 4);
+    if (m) {
+      std::memcpy(h_col + eb, gi.g.column_indices, (size_t)m * 4);
+      std::memcpy(h_wt + eb, gi.g.weights, (size_t)m * 4);
+    }
+    std::memcpy(h_flags + nb, gi.g.attacker_pos, n);
+    for (uint32_t i = 0; i < gi.n_reach; i++) h_reach[ri++] = gi.to_reach[i] + (uint32_t)nb;
+    if (any_init) {
+      if (gi.init) {
+        const unsigned long long t = gi.init->offsets[n];
+        std::memcpy(h_init + ii, gi.init->data, (size_t)t * 4);
+        for (uint32_t v = 0; v < n; v++) {
+          unsigned long long o = gi.init->offsets[v], c = gi.init->offsets[v + 1] - o;
+          h_desc[nb + v] = ((ii + o) << 24) | c;
+        }
+        ii += t;
+      } else {
+        for (uint32_t v = 0; v < n; v++) h_desc[nb + v] = 0ull;
+        for (uint32_t i = 0; i < gi.n_reach; i++) h_desc[nb + gi.to_reach[i]] = (0ull << 24) | 1ull;
+      }
+    }
+    h_nb[g] = nb;
+    h_eb[g] = eb;
+    h_gn[g] = n;
+  }
+  h_row[N] = (uint32_t)M;
+  h_nb[dg->n_games] = N;
+  h_eb[dg->n_games] = M;
+  h_gn[dg->n_games] = 0;
+
+  // device allocations
+  geq_status a = GEQ_OK;
+  if ((a = dalloc(dg->row, N + 1)) || (a = dalloc(dg->col, M)) || (a = dalloc(dg->wt, M)) ||
+      (a = dalloc(dg->rrow, N + 1)) || (a = dalloc(dg->rcol, M)) || (a = dalloc(dg->flags, N)) ||
+      (a = dalloc(dg->desc, N)) || (a = dalloc(dg->desc_init, N)) || (a = dalloc(dg->slot_new, N)) ||
+      (a = dalloc(dg->mark, N)) || (a = dalloc(dg->front0, N)) || (a = dalloc(dg->front1, N)) ||
+      (a = dalloc(dg->init_data, dg->init_total)) || (a = dalloc(dg->reach, n_reach)) ||
+      (a = dalloc(dg->d_node_base, 3 * (dg->n_games + 1))) || (a = dalloc(dg->ctr, 1))) {
+    free_games(*dg);
+    return a;
+  }
+  unsigned long long cap = std::max<unsigned long long>(4ull * (dg->init_total + N) + (1ull << 20), 1ull << 22);
+  if ((a = dalloc(dg->arena[0], cap))) { free_games(*dg); return a; }
+  dg->arena_cap[0] = cap;
+  cudaStream_t S = s.stream;
+#define CUF(call)                        \
+  do {                                   \
+    cudaError_t e_ = (call);             \
+    if (e_ != cudaSuccess) {             \
+      free_games(*dg);                   \
+      return fail(GEQ_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    }                                    \
+  } while (0)
+  CUF(cudaMemcpyAsync(dg->row, h_row, (N + 1) * 4, cudaMemcpyHostToDevice, S));
+  if (M) {
+    CUF(cudaMemcpyAsync(dg->col, h_col, M * 4, cudaMemcpyHostToDevice, S));
+    CUF(cudaMemcpyAsync(dg->wt, h_wt, M * 4, cudaMemcpyHostToDevice, S));
+  }
+  if (N) CUF(cudaMemcpyAsync(dg->flags, h_flags, N, cudaMemcpyHostToDevice, S));
+  if (n_reach) CUF(cudaMemcpyAsync(dg->reach, h_reach, n_reach * 4, cudaMemcpyHostToDevice, S));
+  CUF(cudaMemcpyAsync(dg->init_data, h_init, dg->init_total * 4, cudaMemcpyHostToDevice, S));
+  CUF(cudaMemcpyAsync(dg->d_node_base, h_nb, 3 * (dg->n_games + 1) * 8, cudaMemcpyHostToDevice, S));
+  if (any_init) {
+    if (N) CUF(cudaMemcpyAsync(dg->desc_init, h_desc, N * 8, cudaMemcpyHostToDevice, S));
+  } else {
+    if (N) CUF(cudaMemsetAsync(dg->desc_init, 0, N * 8, S));
+    if (n_reach) k_init_reach<<<std::min<unsigned long long>((n_reach + 255) / 256, 4096), 256, 0, S>>>(dg->desc_init, dg->reach, n_reach, 0ull);
+  }
+  if (N) CUF(cudaMemsetAsync(dg->mark, 0, N * 4, S));
+  CUF(cudaMemsetAsync(s.d_err, 0, 4, S));
+  const unsigned grid = (unsigned)std::max(1, n_sms * 8);
+  if (dg->n_games > 1) {
+    k_fix_rows<<<grid, 256, 0, S>>>(dg->row, N, dg->d_node_base, dg->d_node_base + (dg->n_games + 1), dg->n_games);
+    k_fix_cols<<<grid, 256, 0, S>>>(dg->col, M, dg->d_node_base, dg->d_node_base + (dg->n_games + 1), dg->n_games,
+                                    dg->d_node_base + 2 * (dg->n_games + 1), s.d_err);
+  } else {
+    // single game: validate successor ids on the device as well
+    k_fix_cols<<<grid, 256, 0, S>>>(dg->col, M, dg->d_node_base, dg->d_node_base + (dg->n_games + 1), 1,
+                                    dg->d_node_base + 2 * (dg->n_games + 1), s.d_err);
+  }
+  // reverse CSR
+  geq_status es = ensure_cnt(s, N + 1);
+  if (es) { free_games(*dg); return es; }
+  CUF(cudaMemsetAsync(s.cnt, 0, (N + 1) * 4, S));
+  k_indegree<<<grid, 256, 0, S>>>(dg->col, M, N, s.cnt, s.d_err);
+  unsigned long long *roff = nullptr;
+  if ((a = dalloc(roff, N + 1))) { free_games(*dg); return a; }
+  unsigned long long launches = 0;
+  if ((a = scan_u32(s, s.cnt, N, roff, launches))) { cudaFree(roff); free_games(*dg); return a; }
+  k_u64_to_u32<<<grid, 256, 0, S>>>(roff, N + 1, dg->rrow);
+  CUF(cudaMemcpyAsync(s.cnt, dg->rrow, N * 4, cudaMemcpyDeviceToDevice, S));
+  k_fill_reverse<<<grid, 256, 0, S>>>(dg->row, dg->col, N, s.cnt, dg->rcol);
+  uint32_t h_err = 0;
+  CUF(cudaMemcpyAsync(&s.h_ctr->pad, s.d_err, 4, cudaMemcpyDeviceToHost, S));
+  CUF(cudaStreamSynchronize(S));
+  h_err = s.h_ctr->pad;
+  cudaFree(roff);
+  CUF(cudaGetLastError());
+  if (h_err) {
+    free_games(*dg);
+    return fail(GEQ_ERR_INVALID_INPUT, "a successor index is out of range");
+  }
+#undef CUF
+  KParams &kp = dg->kp;
+  kp.row = dg->row; kp.col = dg->col; kp.wt = dg->wt; kp.rrow = dg->rrow; kp.rcol = dg->rcol;
+  kp.flags = dg->flags; kp.desc = dg->desc; kp.mark = dg->mark; kp.front0 = dg->front0; kp.front1 = dg->front1;
+  kp.slot_new = dg->slot_new; kp.ctr = dg->ctr; kp.n_nodes = N; kp.n_edges = M;
+  kp.el = dg->conf.elements; kp.mx = dg->conf.max; kp.eb = dg->conf.energy_bits(); kp.em = dg->conf.energy_mask();
+  kp.ub = dg->conf.update_bits(); kp.um = dg->conf.update_mask();
+  kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
+  out = std::move(dg);
+  return GEQ_OK;
+}
+
+static geq_status compact(Engine &E, DeviceGamesImpl &dg, unsigned long long &launches) {
+  Engine::State &s = *E.st;
+  cudaStream_t S = s.stream;
+  const unsigned long long N = dg.N;
+  geq_status a = ensure_cnt(s, N + 1);
+  if (a) return a;
+  unsigned long long *noff = nullptr;
+  if ((a = dalloc(noff, N + 1))) return a;
+  const unsigned grid = (unsigned)std::max(1, E.n_sms * 8);
+  k_desc_counts<<<grid, 256, 0, S>>>(dg.desc, N, s.cnt);
+  launches++;
+  if ((a = scan_u32(s, s.cnt, N, noff, launches))) { cudaFree(noff); return a; }
+  unsigned long long total = 0;
+  CU(cudaMemcpyAsync(&total, noff + N, 8, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  const int alt = dg.arena_cur ^ 1;
+  unsigned long long need = std::max<unsigned long long>(dg.arena_cap[dg.arena_cur], 4 * total + (1ull << 20));
+  if (dg.arena_cap[alt] < need) {
+    dfree(dg.arena[alt]);
+    dg.arena_cap[alt] = 0;
+    if ((a = dalloc(dg.arena[alt], need))) { cudaFree(noff); return a; }
+    dg.arena_cap[alt] = need;
+  }
+  k_compact<<<grid, 256, 0, S>>>(dg.desc, N, noff, dg.arena[dg.arena_cur], dg.arena[alt]);
+  k_set_arena<<<1, 1, 0, S>>>(dg.ctr, dg.arena[alt], dg.arena_cap[alt], total);
+  launches += 2;
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(S));
+  cudaFree(noff);
+  dg.arena_cur = alt;
+  return GEQ_OK;
+}
+
+template <class Cd>
+static void launch_round(Engine &E, DeviceGamesImpl &dg, cudaStream_t S) {
+  const unsigned grid = (unsigned)std::max<uint32_t>(1, E.n_sms * E.tuning.blocks_per_sm);
+  k_round<Cd><<<grid, BLOCK, 0, S>>>(dg.kp);
+  k_commit<<<(unsigned)std::max(1, E.n_sms * 2), 256, 0, S>>>(dg.kp);
+}
+
+geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  unsigned long long launches = 0, compactions = 0;
+  // restart from the uploaded initial state
+  const int a0 = dg.arena_cur;
+  CU(cudaEventRecord(s.ev0, S));
+  if (dg.N) CU(cudaMemcpyAsync(dg.desc, dg.desc_init, dg.N * 8, cudaMemcpyDeviceToDevice, S));
+  CU(cudaMemcpyAsync(dg.arena[a0], dg.init_data, dg.init_total * 4, cudaMemcpyDeviceToDevice, S));
+  if (dg.next_stamp > 0xF0000000u) {
+    if (dg.N) CU(cudaMemsetAsync(dg.mark, 0, dg.N * 4, S));
+    dg.next_stamp = 1;
+  }
+  Ctr h{};
+  h.arena = dg.arena[a0];
+  h.arena_cap = dg.arena_cap[a0];
+  h.arena_top = dg.init_total;
+  h.stamp = dg.next_stamp;
+  *s.h_ctr = h;
+  CU(cudaMemcpyAsync(dg.ctr, s.h_ctr, sizeof(Ctr), cudaMemcpyHostToDevice, S));
+  if (dg.n_reach) {
+    const unsigned grid = (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>((dg.n_reach + 7) / 8, (unsigned long long)n_sms * 16));
+    k_init_frontier<<<grid, 256, 0, S>>>(dg.kp, dg.reach, dg.n_reach);
+    launches++;
+  }
+  CU(cudaGetLastError());
+  const bool use_graph = !(tuning.flags & GEQ_TUNE_NO_GRAPH);
+  const uint32_t R = use_graph ? std::max<uint32_t>(1, tuning.rounds_per_graph) : 1;
+  if (use_graph && (!dg.gexec || dg.graph_rounds != R)) {
+    if (dg.gexec) { cudaGraphExecDestroy(dg.gexec); dg.gexec = nullptr; }
+    cudaStream_t cs;
+    CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t graph;
+    cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      for (uint32_t r = 0; r < R; r++) {
+        if (dg.generic) launch_round<CodecGen>(*this, dg, cs);
+        else launch_round<CodecStd>(*this, dg, cs);
+      }
+      ce = cudaStreamEndCapture(cs, &graph);
+    }
+    if (ce == cudaSuccess) {
+      ce = cudaGraphInstantiate(&dg.gexec, graph, 0);
+      cudaGraphDestroy(graph);
+    }
+    cudaStreamDestroy(cs);
+    if (ce != cudaSuccess) return fail(GEQ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    dg.graph_rounds = R;
+  }
+  // The device work of every launch is bounded; this bounds the host loop in
+  // case the frontier never empties (GEQ_SOLVE_TIMEOUT_S seconds, default 600).
+  const char *lim_env = std::getenv("GEQ_SOLVE_TIMEOUT_S");
+  const double limit_s = lim_env ? std::atof(lim_env) : 600.0;
+  const auto t_start = std::chrono::steady_clock::now();
+  for (unsigned long long iter = 0;; iter++) {
+    if (use_graph) {
+      CU(cudaGraphLaunch(dg.gexec, S));
+    } else {
+      if (dg.generic) launch_round<CodecGen>(*this, dg, S);
+      else launch_round<CodecStd>(*this, dg, S);
+    }
+    launches += 2ull * R;
+    CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
+    CU(cudaStreamSynchronize(S));
+    const Ctr c = *s.h_ctr;
+    if (c.error) {
+      const char *what = (c.error & DERR_BOUNDS) ? "index out of range" :
+                         (c.error & DERR_LIST) ? "energy list too long" : "combination too large";
+      return fail((c.error & DERR_BOUNDS) ? GEQ_ERR_INTERNAL : GEQ_ERR_OUT_OF_MEMORY,
+                  "device error %u (%s, line %u)", c.error, what, c.err_line);
+    }
+    if (c.overflow || c.arena_top > c.arena_cap - c.arena_cap / 4) {
+      geq_status a = compact(*this, dg, launches);
+      if (a) return a;
+      compactions++;
+      if (c.overflow) continue;
+    }
+    if (c.fsize[c.cur] == 0) break;
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    if (el > limit_s) return fail(GEQ_ERR_TIMEOUT, "no fixpoint after %llu rounds (%.0f s)", c.rounds, el);
+  }
+  CU(cudaEventRecord(s.ev1, S));
+  CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  const Ctr c = *s.h_ctr;
+  dg.next_stamp = c.stamp + 2u;
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s.ev0, s.ev1);
+    stats->rounds = c.rounds;
+    stats->positions_computed = c.positions;
+    stats->edges_relaxed = c.edges;
+    stats->algorithmic_bytes = c.bytes;
+    stats->arena_compactions = compactions;
+    stats->kernel_launches = launches;
+    stats->device_ms = ms;
+  }
+  return GEQ_OK;
+}
+
+geq_status Engine::download(DeviceGamesImpl &dg, geq_solution &sol) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  const unsigned long long N = dg.N;
+  unsigned long long launches = 0;
+  geq_status a = ensure_cnt(s, N + 1);
+  if (a) return a;
+  unsigned long long *goff = nullptr, *rel = nullptr;
+  uint32_t *out = nullptr;
+  if ((a = dalloc(goff, N + 1))) return a;
+  if ((a = dalloc(rel, N + dg.n_games))) { cudaFree(goff); return a; }
+  const unsigned grid = (unsigned)std::max(1, n_sms * 8);
+  k_desc_counts<<<grid, 256, 0, S>>>(dg.desc, N, s.cnt);
+  if ((a = scan_u32(s, s.cnt, N, goff, launches))) { cudaFree(goff); cudaFree(rel); return a; }
+  unsigned long long total = 0;
+  CU(cudaMemcpyAsync(&total, goff + N, 8, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  if ((a = dalloc(out, total))) { cudaFree(goff); cudaFree(rel); return a; }
+  k_gather<<<grid, 256, 0, S>>>(dg.desc, N, goff, dg.arena[dg.arena_cur], out);
+  k_rel_offsets<<<grid, 256, 0, S>>>(goff, N, dg.d_node_base, dg.n_games, rel);
+  sol.energy_size = 1;
+  sol.offsets.resize(N + dg.n_games);
+  sol.data.resize(total);
+  CU(cudaMemcpyAsync(sol.offsets.data(), rel, (N + dg.n_games) * 8, cudaMemcpyDeviceToHost, S));
+  if (total) CU(cudaMemcpyAsync(sol.data.data(), out, total * 4, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  CU(cudaGetLastError());
+  cudaFree(goff);
+  cudaFree(rel);
+  cudaFree(out);
+  sol.n_vertices.resize(dg.n_games);
+  sol.offsets_base.resize(dg.n_games);
+  sol.data_base.resize(dg.n_games);
+  for (uint32_t g = 0; g < dg.n_games; g++) {
+    sol.n_vertices[g] = (uint32_t)(dg.node_base[g + 1] - dg.node_base[g]);
+    sol.offsets_base[g] = dg.node_base[g] + g;
+  }
+  // data base of each game = global offset of its first position; recover it
+  // from the relative offsets by accumulating the game totals.
+  unsigned long long db = 0;
+  for (uint32_t g = 0; g < dg.n_games; g++) {
+    sol.data_base[g] = db;
+    db += sol.offsets[sol.offsets_base[g] + sol.n_vertices[g]];
+  }
+  return GEQ_OK;
+}
+
+geq_status Engine::download_selected(DeviceGamesImpl &dg, const std::vector<uint32_t> &first,
+                                     const std::vector<uint32_t> &count, geq_solution &sol) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  const uint32_t G = (uint32_t)first.size();
+  std::vector<uint32_t> sel;
+  for (uint32_t g = 0; g < G; g++)
+    for (uint32_t i = 0; i < count[g]; i++) sel.push_back((uint32_t)(dg.node_base[g] + first[g] + i));
+  const unsigned long long K = sel.size();
+  unsigned long long launches = 0;
+  geq_status a = ensure_cnt(s, K + 1);
+  if (a) return a;
+  uint32_t *d_sel = nullptr, *out = nullptr;
+  unsigned long long *goff = nullptr;
+  if ((a = dalloc(d_sel, K))) return a;
+  if ((a = dalloc(goff, K + 1))) { cudaFree(d_sel); return a; }
+  if (K) CU(cudaMemcpyAsync(d_sel, sel.data(), K * 4, cudaMemcpyHostToDevice, S));
+  const unsigned grid = (unsigned)std::max(1, n_sms * 8);
+  k_sel_counts<<<grid, 256, 0, S>>>(dg.desc, d_sel, K, s.cnt);
+  if ((a = scan_u32(s, s.cnt, K, goff, launches))) { cudaFree(d_sel); cudaFree(goff); return a; }
+  std::vector<unsigned long long> off(K + 1);
+  CU(cudaMemcpyAsync(off.data(), goff, (K + 1) * 8, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  const unsigned long long total = off[K];
+  if ((a = dalloc(out, total))) { cudaFree(d_sel); cudaFree(goff); return a; }
+  k_sel_gather<<<grid, 256, 0, S>>>(dg.desc, d_sel, K, goff, dg.arena[dg.arena_cur], out);
+  sol.energy_size = 1;
+  sol.data.resize(total);
+  if (total) CU(cudaMemcpyAsync(sol.data.data(), out, total * 4, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  CU(cudaGetLastError());
+  cudaFree(d_sel);
+  cudaFree(goff);
+  cudaFree(out);
+  sol.n_vertices.assign(count.begin(), count.end());
+  sol.offsets_base.resize(G);
+  sol.data_base.resize(G);
+  sol.offsets.clear();
+  sol.offsets.reserve(K + G);
+  unsigned long long k = 0;
+  for (uint32_t g = 0; g < G; g++) {
+    sol.offsets_base[g] = sol.offsets.size();
+    sol.data_base[g] = off[k];
+    for (uint32_t i = 0; i <= count[g]; i++) sol.offsets.push_back(off[k + i] - off[k]);
+    k += count[g];
+  }
+  return GEQ_OK;
+}
+
+}  // namespace geq

@@ -1,0 +1,112 @@
+// geq_internal.h - declarations shared by the sources of libgeq.so.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/geq.h"
+
+namespace geq {
+
+// ---- EnergyConf arithmetic (src/energy.rs:36-78) --------------------------
+inline uint32_t lzcnt32(uint32_t x) { return x == 0 ? 32u : (uint32_t)__builtin_clz(x); }
+inline uint32_t next_pow2(uint32_t x) { return x <= 1 ? 1u : 1u << (32 - lzcnt32(x - 1)); }
+struct Conf {
+  uint32_t elements = 6, max = 3;
+  Conf() = default;
+  Conf(uint32_t e, uint32_t m) : elements(e), max(m) {}
+  explicit Conf(geq_energy_conf c) : elements(c.elements), max(c.max) {}
+  uint32_t energy_bits() const { return next_pow2(32 - lzcnt32(max)); }
+  uint32_t energy_mask() const { return 0xffffffffu >> (32 - energy_bits()); }
+  uint32_t energy_size() const { return (energy_bits() * elements + 31) / 32; }
+  uint32_t update_bits() const { return next_pow2(32 - lzcnt32(elements + 2)); }
+  uint32_t update_mask() const { return 0xffffffffu >> (32 - update_bits()); }
+  uint32_t update_size() const { return (update_bits() * elements + 31) / 32; }
+  bool standard() const { return elements == 6 && max == 3; }
+  // Device codecs: one energy word, one update word, thermometer code of
+  // elements*max bits in a u32.
+  bool supported() const {
+    return elements >= 1 && max >= 1 && energy_size() == 1 && update_size() == 1 &&
+           (uint64_t)elements * max <= 32;
+  }
+  bool operator==(const Conf &o) const { return elements == o.elements && max == o.max; }
+};
+
+// ---- errors -----------------------------------------------------------------
+void set_last_error(const std::string &msg);
+geq_status fail(geq_status st, const char *fmt, ...);
+
+// ---- host-side game description handed to the device engine --------------
+struct GameInput {
+  geq_game_graph g{};
+  const geq_energy_lists *init = nullptr;  // may be null
+  const uint32_t *to_reach = nullptr;
+  uint32_t n_reach = 0;
+  std::vector<uint32_t> reach_storage;  // standard reach when none was given
+};
+
+// Validation of a graph view (TryFrom<SerdeGameGraph> checks,
+// energygame.rs:65-83, plus update-code checks).
+geq_status validate_graph(const geq_game_graph &g);
+geq_status validate_lists(const geq_game_graph &g, const geq_energy_lists *l);
+
+}  // namespace geq
+
+// ---- opaque objects of the C ABI ------------------------------------------
+struct geq_solution {
+  uint32_t energy_size = 1;
+  std::vector<uint32_t> n_vertices;     // per game
+  std::vector<uint64_t> offsets_base;   // per game: index into `offsets`
+  std::vector<uint64_t> data_base;      // per game: first word in `data`
+  std::vector<uint64_t> offsets;        // per game n+1 entries, relative
+  std::vector<uint32_t> data;
+  geq_solve_stats stats{};
+};
+
+namespace geq {
+class Engine;
+struct DeviceGamesImpl;
+// Releases the device memory of uploaded games and the object itself.
+void destroy_games(DeviceGamesImpl *p);
+struct GamesDeleter {
+  void operator()(DeviceGamesImpl *p) const { destroy_games(p); }
+};
+using GamesPtr = std::unique_ptr<DeviceGamesImpl, GamesDeleter>;
+}  // namespace geq
+
+struct geq_context {
+  int device = 0;
+  std::unique_ptr<geq::Engine> engine;
+};
+
+struct geq_device_games {
+  geq::GamesPtr impl;
+};
+
+namespace geq {
+
+// Engine: owns the CUDA stream, events, pinned staging and the kernels.
+class Engine {
+ public:
+  static geq_status create(int device, std::unique_ptr<Engine> &out);
+  ~Engine();
+  geq_status upload(std::vector<GameInput> &games, GamesPtr &out);
+  geq_status solve(DeviceGamesImpl &dg, geq_solve_stats *stats);
+  // All positions of all games.
+  geq_status download(DeviceGamesImpl &dg, geq_solution &sol);
+  // Only the listed positions: game g's local positions first_g .. first_g+count_g-1
+  // become game g of the solution.
+  geq_status download_selected(DeviceGamesImpl &dg, const std::vector<uint32_t> &first,
+                               const std::vector<uint32_t> &count, geq_solution &sol);
+  geq_tuning tuning{};
+  int n_sms = 0;
+  uint64_t total_mem = 0;
+  std::string name;
+
+  struct State;
+  std::unique_ptr<State> st;
+};
+
+}  // namespace geq

@@ -1,0 +1,325 @@
+"""TransitionSystem, GameBuild and Equivalence (mirror of src/lib.rs,
+src/gamebuild.rs and src/equivalence.rs) over libgeq."""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from ._lib import check, geq_game_graph, geq_position, lib
+from .energy import Energy, EnergyArray, EnergyConf
+from .energygame import Context, GameGraph, _lists_from_solution, _stats_of, default_context
+
+_u32 = C.POINTER(C.c_uint32)
+_i32 = C.POINTER(C.c_int32)
+_u64 = C.POINTER(C.c_uint64)
+_Z32 = np.zeros(1, dtype=np.uint32)
+_ZI32 = np.zeros(1, dtype=np.int32)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+class TransitionSystem:
+    """Labelled transition system (lib.rs:172-536).  Label 0 is tau."""
+
+    def __init__(self, edges: Iterable[tuple[int, int, int]] | None = None, *, _handle=None):
+        if _handle is not None:
+            self.h = _handle
+            return
+        e = np.asarray(list(edges or []), dtype=np.int64).reshape(-1, 3)
+        self.h = TransitionSystem._from_arrays(e[:, 0], e[:, 1], e[:, 2])
+
+    @staticmethod
+    def _from_arrays(src, dst, lab):
+        s = np.ascontiguousarray(src, dtype=np.uint32)
+        d = np.ascontiguousarray(dst, dtype=np.uint32)
+        l = np.ascontiguousarray(lab, dtype=np.int32)
+        h = C.c_void_p()
+        n = len(s)
+        check(lib.geq_lts_from_edges(n, _p(s if n else _Z32, _u32), _p(d if n else _Z32, _u32),
+                                     _p(l if n else _ZI32, _i32), C.byref(h)))
+        return h
+
+    @classmethod
+    def from_arrays(cls, src, dst, label) -> "TransitionSystem":
+        return cls(_handle=cls._from_arrays(src, dst, label))
+
+    @classmethod
+    def from_csv_file(cls, path: str) -> "TransitionSystem":
+        """lib.rs:364-406: lines `from,to,label`; label "i" is tau."""
+        h = C.c_void_p()
+        check(lib.geq_lts_from_csv_file(str(path).encode(), C.byref(h)))
+        return cls(_handle=h)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.h.value:
+                lib.geq_lts_free(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    def n_vertices(self) -> int:
+        return lib.geq_lts_n_vertices(self.h)
+
+    def n_transitions(self) -> int:
+        return lib.geq_lts_n_transitions(self.h)
+
+    def inner(self):
+        """Label-sorted adjacency as (offsets, targets, labels) arrays."""
+        n, m = self.n_vertices(), self.n_transitions()
+        off = np.zeros(n + 1, dtype=np.uint64)
+        tg = np.zeros(max(m, 1), dtype=np.uint32)
+        lb = np.zeros(max(m, 1), dtype=np.int32)
+        lib.geq_lts_transitions(self.h, _p(off, _u64), _p(tg, _u32), _p(lb, _i32))
+        return off, tg[:m], lb[:m]
+
+    def adj(self, p: int) -> list[tuple[int, int]]:
+        off, tg, lb = self.inner()
+        return [(int(tg[k]), int(lb[k])) for k in range(int(off[p]), int(off[p + 1]))]
+
+    def signature_refinement(self) -> tuple[np.ndarray, int]:
+        """lib.rs:444-464: (partition, number of bisimilarity classes)."""
+        n = self.n_vertices()
+        part = np.zeros(max(n, 1), dtype=np.uint64)
+        cnt = C.c_uint64()
+        check(lib.geq_lts_signature_refinement(self.h, _p(part, _u64), C.byref(cnt)))
+        return part[:n], cnt.value
+
+    def bisimilar_minimize(self) -> tuple["TransitionSystem", np.ndarray]:
+        """lib.rs:413-432: (minimised LTS, process -> class mapping)."""
+        n = self.n_vertices()
+        mapping = np.zeros(max(n, 1), dtype=np.uint64)
+        h = C.c_void_p()
+        check(lib.geq_lts_bisimilar_minimize(self.h, C.byref(h), _p(mapping, _u64)))
+        return TransitionSystem(_handle=h), mapping[:n]
+
+    def compare(self, p: int, q: int, context: Context | None = None) -> EnergyArray:
+        """lib.rs:275-283: energies of Attack(p, {q}) in the minimised system."""
+        return compare_batch([(self, p, q)], context=context, minimize=True)[0]
+
+    def compare_unminimized(self, p: int, q: int, context: Context | None = None) -> EnergyArray:
+        """lib.rs:291-296."""
+        return compare_batch([(self, p, q)], context=context, minimize=False)[0]
+
+    def equivalences(self, context: Context | None = None) -> "Equivalence":
+        """lib.rs:329-334."""
+        return Equivalence._compute(self, True, context)
+
+    def equivalences_unminimized(self, context: Context | None = None) -> "Equivalence":
+        """lib.rs:338-343."""
+        return Equivalence._compute(self, False, context)
+
+
+def compare_batch(jobs: Sequence[tuple[TransitionSystem, int, int]], context: Context | None = None,
+                  minimize: bool = True, return_stats: bool = False):
+    """TransitionSystem::compare for many (lts, p, q) jobs, all games solved in
+    one set of device rounds."""
+    ctx = context or default_context()
+    n = len(jobs)
+    hs = (C.c_void_p * max(n, 1))(*[j[0].h.value for j in jobs])
+    ps = np.array([j[1] for j in jobs] or [0], dtype=np.uint32)
+    qs = np.array([j[2] for j in jobs] or [0], dtype=np.uint32)
+    sol = C.c_void_p()
+    check(lib.geq_compare_batch(ctx.h, n, hs, _p(ps, _u32), _p(qs, _u32), 1 if minimize else 0, C.byref(sol)))
+    try:
+        out = [_lists_from_solution(sol, i, EnergyConf.STANDARD)[0] for i in range(n)]
+        stats = _stats_of(sol)
+    finally:
+        lib.geq_solution_free(sol)
+    return (out, stats) if return_stats else out
+
+
+# ---- GameBuild ---------------------------------------------------------------
+class Position(tuple):
+    """Position (gamepos.rs:210-251) as (kind, p, q, qx)."""
+
+    __slots__ = ()
+
+    def __new__(cls, kind: str, p: int, q=(), qx=()):
+        return super().__new__(cls, (kind, int(p), tuple(int(x) for x in q), tuple(int(x) for x in qx)))
+
+    @classmethod
+    def attack(cls, p, q):
+        return cls("attack", p, q)
+
+    @classmethod
+    def clause(cls, p, q):
+        return cls("clause", p, (q,))
+
+    @classmethod
+    def defend(cls, p, q, qx):
+        return cls("defend", p, q, qx)
+
+    kind = property(lambda s: s[0])
+    p = property(lambda s: s[1])
+    q = property(lambda s: s[2])
+    qx = property(lambda s: s[3])
+
+    def is_attack(self) -> bool:
+        return self[0] in ("attack", "clause")
+
+
+class StartInfo:
+    """StartInfo (equivalence.rs:19-38)."""
+
+    def __init__(self, starting_points, n_processes):
+        self.starting_points = starting_points
+        self.n_processes = n_processes
+
+
+class GameBuild:
+    """GameBuild (gamebuild.rs:139-266): the generated game and its positions."""
+
+    def __init__(self, handle):
+        self.h = handle
+        g = geq_game_graph()
+        lib.geq_game_build_graph(self.h, C.byref(g))
+        n = g.n_vertices
+        row = np.ctypeslib.as_array(g.row_offsets, shape=(n + 1,)).copy()
+        m = int(row[-1])
+        col = np.ctypeslib.as_array(g.column_indices, shape=(m,)).copy() if m else np.zeros(0, np.uint32)
+        wt = np.ctypeslib.as_array(g.weights, shape=(m,)).copy() if m else np.zeros(0, np.uint32)
+        att = np.ctypeslib.as_array(g.attacker_pos, shape=(n,)).copy() if n else np.zeros(0, np.uint8)
+        self.game = GameGraph.from_csr(row, col, wt.reshape(-1, 1), att, EnergyConf.STANDARD)
+        self.n_starting_points = lib.geq_game_build_n_starting_points(self.h)
+        self._nodes = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.h.value:
+                lib.geq_game_build_free(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    @property
+    def nodes(self) -> list[Position]:
+        if self._nodes is None:
+            kinds = ("attack", "clause", "defend")
+            out = []
+            pos = geq_position()
+            for i in range(self.game.n_vertices()):
+                check(lib.geq_game_build_position(self.h, i, C.byref(pos)))
+                q = [pos.q[k] for k in range(pos.n_q)]
+                qx = [pos.qx[k] for k in range(pos.n_qx)]
+                out.append(Position(kinds[pos.kind], pos.p, q, qx))
+            self._nodes = out
+        return self._nodes
+
+    def starting_points(self) -> list[Position]:
+        return [p for p in self.nodes[:self.n_starting_points] if p.kind == "attack"]
+
+    @classmethod
+    def compare(cls, lts: TransitionSystem, p: int, q: int) -> "GameBuild":
+        h = C.c_void_p()
+        check(lib.geq_game_build_compare(lts.h, p, q, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def compare_all(cls, lts: TransitionSystem) -> tuple["GameBuild", StartInfo]:
+        h = C.c_void_p()
+        check(lib.geq_game_build_compare_all(lts.h, C.byref(h)))
+        b = cls(h)
+        return b, StartInfo(b.starting_points(), lts.n_vertices())
+
+    @classmethod
+    def compare_multiple(cls, lts: TransitionSystem, processes: Sequence[int]) -> tuple["GameBuild", StartInfo]:
+        pr = np.ascontiguousarray(processes, dtype=np.uint32)
+        h = C.c_void_p()
+        check(lib.geq_game_build_compare_multiple(lts.h, _p(pr if pr.size else _Z32, _u32), len(pr), C.byref(h)))
+        b = cls(h)
+        return b, StartInfo(b.starting_points(), lts.n_vertices())
+
+
+# ---- Equivalence -------------------------------------------------------------
+class EquivalenceRelation:
+    """EquivalenceRelation (equivalence.rs:180-247) as class representatives."""
+
+    def __init__(self, classes: np.ndarray, n_classes: int):
+        self.classes = classes
+        self.n_classes = n_classes
+
+    def __len__(self):
+        return len(self.classes)
+
+    def find(self, p: int) -> int:
+        return int(self.classes[p])
+
+    def count_classes(self) -> int:
+        return self.n_classes
+
+    def class_of(self, proc: int) -> list[int]:
+        c = self.classes[proc]
+        return [int(i) for i in np.nonzero(self.classes == c)[0]]
+
+    def get_classes(self) -> list[list[int]]:
+        order: dict[int, int] = {}
+        out: list[list[int]] = []
+        for i, c in enumerate(self.classes):
+            c = int(c)
+            if c not in order:
+                order[c] = len(out)
+                out.append([])
+            out[order[c]].append(i)
+        return out
+
+    def equiv(self, p: int, q: int) -> bool:
+        return self.classes[p] == self.classes[q]
+
+
+class Equivalence:
+    """Equivalence (equivalence.rs:41-175)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    @classmethod
+    def _compute(cls, lts: TransitionSystem, minimize: bool, context: Context | None):
+        ctx = context or default_context()
+        h = C.c_void_p()
+        check(lib.geq_equivalences(ctx.h, lts.h, 1 if minimize else 0, C.byref(h)))
+        return cls(h)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.h.value:
+                lib.geq_equivalence_free(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
+
+    @property
+    def n_processes(self) -> int:
+        return lib.geq_equivalence_n_processes(self.h)
+
+    def n_starting_points(self) -> int:
+        return lib.geq_equivalence_n_starting_points(self.h)
+
+    def energies(self, p: int, q: int) -> EnergyArray | None:
+        d = _u32()
+        n = C.c_uint64()
+        if not lib.geq_equivalence_energies(self.h, p, q, C.byref(d), C.byref(n)):
+            return None
+        a = np.ctypeslib.as_array(d, shape=(n.value,)).copy() if n.value else np.zeros(0, np.uint32)
+        return EnergyArray(a.reshape(-1, 1), EnergyConf.STANDARD)
+
+    def preorder(self, p: int, q: int, equivalence: Energy) -> bool:
+        return bool(lib.geq_equivalence_preorder(self.h, p, q, _p(equivalence.data, _u32)))
+
+    def equiv(self, p: int, q: int, equivalence: Energy) -> bool:
+        return bool(lib.geq_equivalence_equiv(self.h, p, q, _p(equivalence.data, _u32)))
+
+    def relation(self, equivalence: Energy) -> EquivalenceRelation:
+        n = self.n_processes
+        cls_ = np.zeros(max(n, 1), dtype=np.uint32)
+        nc = C.c_uint32()
+        check(lib.geq_equivalence_relation(self.h, _p(equivalence.data, _u32), _p(cls_, _u32), C.byref(nc)))
+        return EquivalenceRelation(cls_[:n], nc.value)
+
+
+__all__ = ["TransitionSystem", "compare_batch", "Position", "StartInfo", "GameBuild", "Equivalence",
+           "EquivalenceRelation"]

@@ -1,0 +1,289 @@
+/*
+ * geq.h - C ABI of the B200 energy-game solver (libgeq.so).
+ *
+ * This is the drop-in boundary for the energy-game path of the gpuequiv
+ * crate: a Rust (or any FFI) host that owns `GameGraph`/`EnergyGame`/
+ * `TransitionSystem` values passes plain pointers and sizes here instead of
+ * running the wgpu pipelines.  Every entry point names the reference
+ * interface (file:line inside the crate) it replaces.
+ *
+ * Conventions
+ *  - Energies and updates use the crate's packed layout (src/energy.rs:143-179,
+ *    :543-588): an energy is `energy_size` u32 words, an update `update_size`
+ *    words.  Energy lists are CSR: position v owns energies
+ *    offsets[v] .. offsets[v+1] (counted in energies, not words).
+ *  - Host buffers passed in are borrowed for the duration of the call.
+ *    Objects returned through `**out` are owned by the caller and released
+ *    with the matching *_free function.  Views filled by *_view / *_lists
+ *    functions point into the owning object and live as long as it does.
+ *  - Every function that can fail returns a geq_status; the detail message of
+ *    the last failure on the calling thread is geq_last_error().
+ *  - A geq_context is bound to one CUDA device and one stream.  It may be used
+ *    from one thread at a time; create one context per host thread for
+ *    concurrency.
+ *  - There is no CPU fallback: without a usable CUDA device the solver entry
+ *    points return GEQ_ERR_NO_DEVICE.
+ */
+#ifndef GEQ_H
+#define GEQ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+#define GEQ_ABI_VERSION 1
+
+/* Error codes.  Replaces gpuequiv::Error (src/error.rs:3-40) and the
+ * TryFrom<SerdeGameGraph> checks (src/energygame.rs:65-83). */
+typedef enum geq_status {
+  GEQ_OK = 0,
+  GEQ_ERR_NO_DEVICE = 1,     /* Error::NoAdapter / Error::NoDevice */
+  GEQ_ERR_OUT_OF_MEMORY = 2, /* device or pinned host allocation failed */
+  GEQ_ERR_INVALID_INPUT = 3, /* malformed graph / energies / arguments */
+  GEQ_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
+  GEQ_ERR_UNSUPPORTED = 5,   /* EnergyConf outside the device codecs */
+  GEQ_ERR_CUDA = 6,          /* other CUDA runtime failure (~Error::BufferMap) */
+  GEQ_ERR_IO = 7,            /* CSVError::IOError */
+  GEQ_ERR_PARSE = 8,         /* CSVError::MissingField / ParseError */
+  GEQ_ERR_BUSY = 9,          /* serving: admission budget exhausted */
+  GEQ_ERR_INTERNAL = 10
+} geq_status;
+
+const char *geq_status_string(geq_status s);
+/* Detail of the last failure on this thread ("" if none). */
+const char *geq_last_error(void);
+int geq_abi_version(void);
+
+/* ---- EnergyConf (src/energy.rs:36-78) ---------------------------------- */
+typedef struct geq_energy_conf {
+  uint32_t elements;
+  uint32_t max;
+} geq_energy_conf;
+/* EnergyConf::STANDARD = {6, 3} (energy.rs:44) */
+uint32_t geq_conf_energy_bits(geq_energy_conf c);  /* energy.rs:56-59 */
+uint32_t geq_conf_energy_size(geq_energy_conf c);  /* energy.rs:49-53 */
+uint32_t geq_conf_energy_mask(geq_energy_conf c);  /* energy.rs:61-63 */
+uint32_t geq_conf_update_bits(geq_energy_conf c);  /* energy.rs:70-73 */
+uint32_t geq_conf_update_size(geq_energy_conf c);  /* energy.rs:65-68 */
+uint32_t geq_conf_update_mask(geq_energy_conf c);  /* energy.rs:75-77 */
+/* 1 if the solver kernels accept this conf (energy and update fit one word
+ * and elements*max <= 32), else 0. */
+int geq_conf_supported(geq_energy_conf c);
+
+/* ---- Energy / Update packing ------------------------------------------- */
+/* Energy::new (energy.rs:88-93, pack_energy :143-162).  n_values <= elements;
+ * missing values are 0.  GEQ_ERR_INVALID_INPUT where the crate returns None. */
+geq_status geq_energy_pack(geq_energy_conf c, const uint32_t *values, uint32_t n_values,
+                           uint32_t *out_words);
+/* From<&Energy> for Vec<u32> (energy.rs:164-179): `elements` values. */
+void geq_energy_unpack(geq_energy_conf c, const uint32_t *words, uint32_t *out_values);
+/* Update::new via Upd::from(i32) (energy.rs:474-490, :510-515, pack_upd
+ * :543-565): 0 Zero, -1 Decrement, k >= 1 Min(k). */
+geq_status geq_update_pack(geq_energy_conf c, const int32_t *values, uint32_t n_values,
+                           uint32_t *out_words);
+/* From<&Update> for Vec<i32> (energy.rs:567-602). */
+void geq_update_unpack(geq_energy_conf c, const uint32_t *words, int32_t *out_values);
+/* EnergyArray::test_equivalence (energy.rs:307-318): 1 if no energy of the
+ * list is <= `equivalence` (the equivalence holds), else 0. */
+int geq_test_equivalence(geq_energy_conf c, const uint32_t *energies, uint64_t n_energies,
+                         const uint32_t *equivalence_words);
+
+/* ---- GameGraph (src/energygame.rs:120-138) ------------------------------ */
+/* CSR view of a game graph in host memory.  Mirrors the pub fields
+ * column_indices / row_offsets / weights / attacker_pos; the reverse graph is
+ * derived on the device. */
+typedef struct geq_game_graph {
+  geq_energy_conf conf;
+  uint32_t n_vertices;
+  const uint32_t *row_offsets;    /* n_vertices + 1 */
+  const uint32_t *column_indices; /* row_offsets[n_vertices] */
+  const uint32_t *weights;        /* row_offsets[n_vertices] * update_size words */
+  const uint8_t *attacker_pos;    /* n_vertices, 0 or 1 */
+} geq_game_graph;
+
+/* Energy lists (Vec<EnergyArray>). */
+typedef struct geq_energy_lists {
+  uint32_t n_vertices;
+  uint32_t energy_size;    /* words per energy */
+  const uint64_t *offsets; /* n_vertices + 1 */
+  const uint32_t *data;    /* offsets[n_vertices] * energy_size words */
+} geq_energy_lists;
+
+/* EnergyGame::standard_reach (energygame.rs:347-352): writes the defender
+ * positions without successors to out (capacity n_vertices), returns count. */
+uint32_t geq_standard_reach(const geq_game_graph *g, uint32_t *out);
+
+/* ---- device context ----------------------------------------------------- */
+/* Replaces GPUCommon::get_gpu (src/energygame/gpuutils.rs:15-31). */
+typedef struct geq_context geq_context;
+geq_status geq_context_create(int device, geq_context **out);
+void geq_context_destroy(geq_context *ctx);
+/* Name of the device, number of SMs and total memory (for reports). */
+geq_status geq_context_info(const geq_context *ctx, char *name, size_t name_len, int *n_sms,
+                            uint64_t *total_mem);
+
+/* ---- solving ------------------------------------------------------------ */
+typedef struct geq_solve_stats {
+  uint64_t rounds;              /* worklist rounds until the fixpoint */
+  uint64_t positions_computed;  /* position recomputations */
+  uint64_t edges_relaxed;       /* (v, w) relaxations */
+  uint64_t algorithmic_bytes;   /* bytes the algorithm must move: per edge
+                                   relaxation 16 + 4|A_w|, per recomputed
+                                   position 12 (+4|A_v| for an attacker's own
+                                   list), +4 per energy written */
+  uint64_t arena_compactions;   /* energy-arena garbage collections */
+  uint64_t kernel_launches;     /* kernels launched by the solve */
+  double device_ms;             /* device time of the solve (CUDA events) */
+} geq_solve_stats;
+
+/* Result of a solve: one or more games, each with its per-position lists. */
+typedef struct geq_solution geq_solution;
+uint32_t geq_solution_n_games(const geq_solution *s);
+/* Lists of game `game` (borrowed from the solution). */
+geq_status geq_solution_lists(const geq_solution *s, uint32_t game, geq_energy_lists *out);
+void geq_solution_stats(const geq_solution *s, geq_solve_stats *out);
+void geq_solution_free(geq_solution *s);
+
+/* EnergyGame::run (energygame.rs:379-383) on EnergyGame { graph, energies,
+ * to_reach } (:329-338).  `initial` may be NULL: then every position starts
+ * empty except the to_reach positions, which start with {0}
+ * (EnergyGame::with_reach, :355-365).  Host buffers in, host buffers out. */
+geq_status geq_energy_game_run(geq_context *ctx, const geq_game_graph *graph,
+                               const geq_energy_lists *initial, const uint32_t *to_reach,
+                               uint32_t n_to_reach, geq_solution **out);
+
+/* Many independent games solved together in one set of device rounds (the
+ * batched form; no reference counterpart beyond calling EnergyGame::run once
+ * per game).  initial / to_reach / n_to_reach are arrays of n_games entries;
+ * initial may be NULL (all games with_reach-initialised) and
+ * to_reach may be NULL (all games standard_reach). */
+geq_status geq_energy_game_run_batch(geq_context *ctx, uint32_t n_games,
+                                     const geq_game_graph *graphs,
+                                     const geq_energy_lists *const *initial,
+                                     const uint32_t *const *to_reach,
+                                     const uint32_t *n_to_reach, geq_solution **out);
+
+/* Device-resident games: upload once, solve repeatedly (each solve restarts
+ * from the uploaded initial energies), download on demand.  Used to time the
+ * solver with inputs already in HBM. */
+typedef struct geq_device_games geq_device_games;
+geq_status geq_device_games_create(geq_context *ctx, uint32_t n_games,
+                                   const geq_game_graph *graphs,
+                                   const geq_energy_lists *const *initial,
+                                   const uint32_t *const *to_reach,
+                                   const uint32_t *n_to_reach, geq_device_games **out);
+geq_status geq_device_games_solve(geq_context *ctx, geq_device_games *dg,
+                                  geq_solve_stats *stats);
+geq_status geq_device_games_download(geq_context *ctx, geq_device_games *dg,
+                                     geq_solution **out);
+void geq_device_games_free(geq_device_games *dg);
+
+/* Solver tuning (autotuner output).  Zero fields keep the current value. */
+typedef struct geq_tuning {
+  uint32_t blocks_per_sm;     /* resident 256-thread blocks per SM of the round kernel */
+  uint32_t rounds_per_graph;  /* worklist rounds captured per CUDA graph launch */
+  uint32_t small_limit;       /* candidates handled in registers per position (1..32) */
+  uint32_t flags;             /* GEQ_TUNE_* bits */
+} geq_tuning;
+#define GEQ_TUNE_FORCE_GENERIC 1u /* generic codec even for STANDARD (cross-check) */
+#define GEQ_TUNE_FORCE_LARGE 2u   /* bypass the register paths (cross-check) */
+#define GEQ_TUNE_NO_GRAPH 4u      /* launch rounds one by one instead of graphs */
+geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t);
+void geq_context_get_tuning(const geq_context *ctx, geq_tuning *t);
+
+/* ---- TransitionSystem (src/lib.rs) -------------------------------------- */
+typedef struct geq_lts geq_lts;
+/* FromIterator<(u32, u32, i32)> (lib.rs:523-536): edges (src, dst, label). */
+geq_status geq_lts_from_edges(uint64_t n_edges, const uint32_t *src, const uint32_t *dst,
+                              const int32_t *label, geq_lts **out);
+/* TransitionSystem::from_csv_file (lib.rs:364-406). */
+geq_status geq_lts_from_csv_file(const char *path, geq_lts **out);
+uint32_t geq_lts_n_vertices(const geq_lts *l);
+uint64_t geq_lts_n_transitions(const geq_lts *l);
+/* Adjacency lists sorted by label (inner(), lib.rs:496-499):
+ * offsets[n+1], targets[m], labels[m]. */
+void geq_lts_transitions(const geq_lts *l, uint64_t *offsets, uint32_t *targets,
+                         int32_t *labels);
+/* TransitionSystem::signature_refinement (lib.rs:444-464). */
+geq_status geq_lts_signature_refinement(const geq_lts *l, uint64_t *partition,
+                                        uint64_t *n_classes);
+/* TransitionSystem::bisimilar_minimize (lib.rs:413-432). */
+geq_status geq_lts_bisimilar_minimize(const geq_lts *l, geq_lts **reduced, uint64_t *mapping);
+void geq_lts_free(geq_lts *l);
+
+/* ---- GameBuild (src/gamebuild.rs) --------------------------------------- */
+typedef struct geq_game_build geq_game_build;
+/* GameBuild::compare (gamebuild.rs:165-170) */
+geq_status geq_game_build_compare(const geq_lts *l, uint32_t p, uint32_t q,
+                                  geq_game_build **out);
+/* GameBuild::compare_all (gamebuild.rs:200-215) */
+geq_status geq_game_build_compare_all(const geq_lts *l, geq_game_build **out);
+/* GameBuild::compare_multiple (gamebuild.rs:176-194) */
+geq_status geq_game_build_compare_multiple(const geq_lts *l, const uint32_t *processes,
+                                           uint32_t n_processes, geq_game_build **out);
+/* The generated GameGraph (borrowed view). */
+void geq_game_build_graph(const geq_game_build *b, geq_game_graph *out);
+uint32_t geq_game_build_n_starting_points(const geq_game_build *b);
+/* Position (gamepos.rs:210-215): kind 0 Attack, 1 Clause, 2 Defend.  For a
+ * Clause, q has one element. */
+typedef struct geq_position {
+  uint32_t kind;
+  uint32_t p;
+  const uint32_t *q;
+  uint32_t n_q;
+  const uint32_t *qx;
+  uint32_t n_qx;
+} geq_position;
+geq_status geq_game_build_position(const geq_game_build *b, uint32_t idx, geq_position *out);
+void geq_game_build_free(geq_game_build *b);
+
+/* ---- whole algorithm (lib.rs:275-343, src/equivalence.rs) --------------- */
+/* TransitionSystem::compare (minimize != 0) / compare_unminimized: the
+ * solution holds one game with a single position: the energies of the start
+ * position Attack(p, {q}). */
+geq_status geq_compare(geq_context *ctx, const geq_lts *l, uint32_t p, uint32_t q, int minimize,
+                       geq_solution **out);
+/* compare() for many (lts, p, q) jobs; every game solved in one batch.  The
+ * solution holds n_jobs games of one position each. */
+geq_status geq_compare_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts,
+                             const uint32_t *p, const uint32_t *q, int minimize,
+                             geq_solution **out);
+
+/* TransitionSystem::equivalences (minimize != 0) / equivalences_unminimized. */
+typedef struct geq_equivalence geq_equivalence;
+geq_status geq_equivalences(geq_context *ctx, const geq_lts *l, int minimize,
+                            geq_equivalence **out);
+/* Equivalence::energies (equivalence.rs:96-98): 0 if (p, q) was no start. */
+int geq_equivalence_energies(const geq_equivalence *e, uint32_t p, uint32_t q,
+                             const uint32_t **data, uint64_t *n_energies);
+/* Equivalence::preorder / equiv (equivalence.rs:125-144); `equivalence` is a
+ * packed STANDARD energy (std_equivalences, energy.rs:212-224). */
+int geq_equivalence_preorder(const geq_equivalence *e, uint32_t p, uint32_t q,
+                             const uint32_t *equivalence);
+int geq_equivalence_equiv(const geq_equivalence *e, uint32_t p, uint32_t q,
+                          const uint32_t *equivalence);
+/* Equivalence::relation (equivalence.rs:154-170): class representative of
+ * every (original) process, written to classes[n_processes]; returns the
+ * number of classes in *n_classes.  Representatives are the smallest member
+ * of each class. */
+geq_status geq_equivalence_relation(const geq_equivalence *e, const uint32_t *equivalence,
+                                    uint32_t *classes, uint32_t *n_classes);
+uint32_t geq_equivalence_n_processes(const geq_equivalence *e);
+uint32_t geq_equivalence_n_starting_points(const geq_equivalence *e);
+void geq_equivalence_free(geq_equivalence *e);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GEQ_H */
