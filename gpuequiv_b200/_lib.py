@@ -1,6 +1,6 @@
 """ctypes binding of libgeq.so (include/geq.h).
 
-The library is built in-tree (``python -m gpuequiv_b200.build``).  There is
+The library is built in-tree (``python gpuequiv_b200/build.py``).  There is
 no fallback: if the shared library is missing the import fails loudly, and
 without a CUDA device the solver calls raise ``GeqError(NO_DEVICE)``.
 
@@ -32,7 +32,8 @@ class geq_energy_lists(C.Structure):
 class geq_solve_stats(C.Structure):
     _fields_ = [("rounds", C.c_uint64), ("positions_computed", C.c_uint64), ("edges_relaxed", C.c_uint64),
                 ("algorithmic_bytes", C.c_uint64), ("arena_compactions", C.c_uint64),
-                ("kernel_launches", C.c_uint64), ("device_ms", C.c_double)]
+                ("kernel_launches", C.c_uint64), ("device_ms", C.c_double),
+                ("round_kernel_ms", C.c_double), ("round_kernel_launches", C.c_uint64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -51,6 +52,8 @@ class geq_position(C.Structure):
 TUNE_FORCE_GENERIC = 1
 TUNE_FORCE_LARGE = 2
 TUNE_NO_GRAPH = 4
+TUNE_PROFILE = 8
+TUNE_NO_THREAD_PATH = 16
 
 STATUS = {0: "OK", 1: "NO_DEVICE", 2: "OUT_OF_MEMORY", 3: "INVALID_INPUT", 4: "TIMEOUT",
           5: "UNSUPPORTED", 6: "CUDA", 7: "IO", 8: "PARSE", 9: "BUSY", 10: "INTERNAL"}
@@ -118,6 +121,7 @@ _SIGS = {
     "geq_lts_free": ([vp], None),
     "geq_game_build_compare": ([vp, C.c_uint32, C.c_uint32, C.POINTER(vp)], C.c_int),
     "geq_game_build_compare_all": ([vp, C.POINTER(vp)], C.c_int),
+    "geq_game_build_compare_bounded": ([vp, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(vp)], C.c_int),
     "geq_game_build_compare_multiple": ([vp, u32p, C.c_uint32, C.POINTER(vp)], C.c_int),
     "geq_game_build_graph": ([vp, C.POINTER(geq_game_graph)], None),
     "geq_game_build_n_starting_points": ([vp], C.c_uint32),
@@ -144,7 +148,7 @@ def library_path() -> str:
 def _load():
     path = library_path()
     if not os.path.exists(path):
-        raise ImportError(f"{path} is missing: build it with `python -m gpuequiv_b200.build`")
+        raise ImportError(f"{path} is missing: build it with `python gpuequiv_b200/build.py`")
     L = C.CDLL(path)
     for name, (args, res) in _SIGS.items():
         f = getattr(L, name)

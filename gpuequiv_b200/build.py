@@ -1,7 +1,9 @@
 """Build libgeq.so (the C-ABI solver library) in-tree for sm_100a.
 
-    python -m gpuequiv_b200.build            # gpuequiv_b200/libgeq.so
-    python -m gpuequiv_b200.build --checked  # gpuequiv_b200/libgeq_checked.so
+    python gpuequiv_b200/build.py            # gpuequiv_b200/libgeq.so
+    python gpuequiv_b200/build.py --checked  # gpuequiv_b200/libgeq_checked.so
+
+(Run it as a script: importing the package loads the library it builds.)
 
 The checked variant compiles every device load/store of the solver with an
 index check that records the offending line and stops the solve instead of

@@ -39,20 +39,8 @@ geq_status validate_graph(const geq_game_graph &g) {
   const uint64_t m = g.row_offsets[g.n_vertices];
   if (m && (!g.column_indices || !g.weights)) return fail(GEQ_ERR_INVALID_INPUT, "edges without column_indices/weights");
   if (g.n_vertices && !g.attacker_pos) return fail(GEQ_ERR_INVALID_INPUT, "attacker_pos is NULL");
-  for (uint64_t k = 0; k < m; k++)
-    if (g.column_indices[k] >= g.n_vertices) return fail(GEQ_ERR_INVALID_INPUT, "Node index too high (edge %llu)", (unsigned long long)k);
-  if (c.supported()) {
-    const uint32_t ub = c.update_bits(), um = c.update_mask();
-    for (uint64_t k = 0; k < m; k++) {
-      uint32_t u = g.weights[k];
-      for (uint32_t i = 0; i < c.elements; i++) {
-        uint32_t code = (u >> (i * ub)) & um;
-        if (code > c.elements + 1) return fail(GEQ_ERR_INVALID_INPUT, "update code %u names no element (edge %llu)", code, (unsigned long long)k);
-      }
-      if (c.elements * ub < 32 && (u >> (c.elements * ub)) != 0)
-        return fail(GEQ_ERR_INVALID_INPUT, "update padding bits set (edge %llu)", (unsigned long long)k);
-    }
-  }
+  // Successor ids and update codes are checked on the device during the
+  // upload (k_fix_cols, k_check_weights), which reports GEQ_ERR_INVALID_INPUT.
   return GEQ_OK;
 }
 
@@ -271,7 +259,7 @@ geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t) {
   geq_status st = ctx_engine(ctx, e);
   if (st) return st;
   if (!t) return fail(GEQ_ERR_INVALID_INPUT, "tuning is NULL");
-  if (t->blocks_per_sm) e->tuning.blocks_per_sm = std::min<uint32_t>(t->blocks_per_sm, 8);
+  if (t->blocks_per_sm) e->tuning.blocks_per_sm = std::min<uint32_t>(std::max<uint32_t>(t->blocks_per_sm, 2), 4);
   if (t->rounds_per_graph) e->tuning.rounds_per_graph = std::min<uint32_t>(t->rounds_per_graph, 256);
   if (t->small_limit) e->tuning.small_limit = std::min<uint32_t>(t->small_limit, 32);
   e->tuning.flags = t->flags;
@@ -428,6 +416,19 @@ geq_status geq_game_build_compare(const geq_lts *l, uint32_t p, uint32_t q, geq_
   if (p >= l->l.n || q >= l->l.n) return fail(GEQ_ERR_INVALID_INPUT, "process out of range");
   std::unique_ptr<geq_game_build> b(new geq_game_build());
   GameBuilder::compare(l->l, p, q, b->b);
+  *out = b.release();
+  return GEQ_OK;
+}
+
+geq_status geq_game_build_compare_bounded(const geq_lts *l, uint32_t p, uint32_t q, uint64_t max_positions,
+                                          geq_game_build **out) {
+  if (!l || !out) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  *out = nullptr;
+  if (p >= l->l.n || q >= l->l.n) return fail(GEQ_ERR_INVALID_INPUT, "process out of range");
+  std::unique_ptr<geq_game_build> b(new geq_game_build());
+  b->b.max_positions = max_positions;
+  GameBuilder::compare(l->l, p, q, b->b);
+  if (b->b.truncated) return fail(GEQ_ERR_OUT_OF_MEMORY, "game exceeds %llu positions", (unsigned long long)max_positions);
   *out = b.release();
   return GEQ_OK;
 }

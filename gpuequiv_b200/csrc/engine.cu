@@ -38,10 +38,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <set>
+#include <thread>
 #include <vector>
 
 #include "codec.cuh"
@@ -63,7 +67,9 @@ constexpr int BLOCK = 32 * WARPS_PER_BLOCK;
 constexpr int SM_BM = 0;      // 128 words: bitmap
 constexpr int SM_BM2 = 128;   // 128 words: second bitmap (own / old list)
 constexpr int SM_TMP = 256;   // 32 words: segment map / compaction
-constexpr int SM_WORDS = 288;
+constexpr int SM_PINC = 288;  // 32 words: predecessor counts (inclusive scan)
+constexpr int SM_PBEG = 320;  // 32 words: predecessor row starts
+constexpr int SM_WORDS = 352;
 // device error bits (Ctr::error)
 constexpr uint32_t DERR_LIST = 1u;     // a list longer than 2^24 - 1 energies
 constexpr uint32_t DERR_BOUNDS = 2u;   // checked build: index out of range
@@ -99,13 +105,26 @@ struct KParams {
   unsigned long long n_nodes, n_edges;
   uint32_t el, mx, eb, em, ub, um;
   uint32_t small_limit;
+  uint32_t thread_path;  // 1: lane-per-position path for small positions
+  uint32_t ib, ibm, inl; // inline descriptors: bits per energy, its mask, capacity
 };
 
+// Energy-list descriptors (one u64 per position):
+//   inline (bit 63 set): count in bits 60..62, energy i in bits [i*ib, i*ib+ib)
+//          with ib = elements * energy_bits (12 for STANDARD: up to 5 energies)
+//   arena  (bit 63 clear): arena offset in bits 24..62, count in bits 0..23
+// Almost every list of the spectroscopy games fits inline, so reading a
+// successor's list is one 8-byte load and writing a result needs no arena.
+constexpr unsigned long long INLINE_BIT = 1ull << 63;
 __device__ __forceinline__ unsigned long long mkdesc(unsigned long long off, uint32_t cnt) {
   return (off << 24) | (unsigned long long)cnt;
 }
-__device__ __forceinline__ uint32_t dcnt(unsigned long long d) { return (uint32_t)(d & CNT_MASK); }
-__device__ __forceinline__ unsigned long long doff(unsigned long long d) { return d >> 24; }
+__device__ __forceinline__ bool dinl(unsigned long long d) { return (d >> 63) != 0ull; }
+__device__ __forceinline__ uint32_t dcnt(unsigned long long d) {
+  return dinl(d) ? (uint32_t)((d >> 60) & 7ull) : (uint32_t)(d & CNT_MASK);
+}
+__device__ __forceinline__ unsigned long long doff(unsigned long long d) { return (d >> 24) & ((1ull << 39) - 1ull); }
+__device__ __forceinline__ unsigned long long inl_hdr(uint32_t n) { return INLINE_BIT | ((unsigned long long)n << 60); }
 __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -129,6 +148,12 @@ __device__ __noinline__ void report_bounds(Ctr *c, int line) {
 template <class T>
 __device__ __forceinline__ T ld(const T *a, unsigned long long i, unsigned long long n, Ctr *c) {
   return CHECK_IDX(c, i, n) ? a[i] : T(0);
+}
+
+// Energy q of the list behind descriptor d.
+__device__ __forceinline__ uint32_t lelem(unsigned long long d, uint32_t q, const uint32_t *arena,
+                                          unsigned long long cap, Ctr *c, uint32_t ib, uint32_t ibm) {
+  return dinl(d) ? ((uint32_t)(d >> (q * ib)) & ibm) : ld(arena, doff(d) + q, cap, c);
 }
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t x, uint32_t lane) {
@@ -234,24 +259,6 @@ __device__ __forceinline__ void bm_set(uint32_t *sm, uint32_t idx) {
   atomicOr(&sm[idx >> 5], 1u << (idx & 31u));
 }
 
-// Write the members of `m` (ascending index order) as packed energies.
-__device__ __forceinline__ void bm_emit(BM m, uint32_t lane, uint32_t *arena, unsigned long long off,
-                                        uint32_t excl) {
-  unsigned long long k = off + excl;
-  unsigned long long w = m.w0;
-  while (w) {
-    uint32_t b = (uint32_t)__ffsll((long long)w) - 1u;
-    arena[k++] = lane * 128u + b;
-    w &= w - 1ull;
-  }
-  w = m.w1;
-  while (w) {
-    uint32_t b = (uint32_t)__ffsll((long long)w) - 1u;
-    arena[k++] = lane * 128u + 64u + b;
-    w &= w - 1ull;
-  }
-}
-
 template <class Cd>
 __device__ __forceinline__ Cd make_codec(const KParams &p);
 template <>
@@ -264,8 +271,7 @@ __device__ __forceinline__ CodecGen make_codec<CodecGen>(const KParams &p) {
 enum : int { R_UNCHANGED = 0, R_CHANGED = 1, R_OVERFLOW = 2, R_SKIPPED = 3, R_ERROR = 4 };
 struct Res {
   int st;
-  unsigned long long off;
-  uint32_t cnt;
+  unsigned long long d;  // the new descriptor when st == R_CHANGED
 };
 
 struct WarpCtx {
@@ -277,32 +283,102 @@ struct WarpCtx {
   uint32_t *sm;
   WarpAlloc &wa;
   unsigned long long &edges, &bytes;
+  __device__ __forceinline__ uint32_t elem(unsigned long long d, uint32_t q) const {
+    return lelem(d, q, arena, cap, c, p.ib, p.ibm);
+  }
 };
 
-// Successor descriptor of edge k (lane-local).
+// Successor of edge k: its update and list descriptor (lane-local).
 struct EdgeInfo {
   uint32_t u, cw;
-  unsigned long long ow;
+  unsigned long long d;
 };
 __device__ __forceinline__ EdgeInfo edge_info(const WarpCtx &x, unsigned long long k) {
   EdgeInfo e{0, 0, 0};
-  uint32_t w = ld(x.p.col, k, x.p.n_edges, x.c);
+  const uint32_t w = ld(x.p.col, k, x.p.n_edges, x.c);
   e.u = ld(x.p.wt, k, x.p.n_edges, x.c);
-  unsigned long long d = ld(x.p.desc, w, x.p.n_nodes, x.c);
-  e.cw = dcnt(d);
-  e.ow = doff(d);
+  e.d = ld(x.p.desc, w, x.p.n_nodes, x.c);
+  e.cw = dcnt(e.d);
   return e;
 }
+__device__ __forceinline__ EdgeInfo shfl_edge(const EdgeInfo &e, uint32_t src) {
+  EdgeInfo r;
+  r.u = __shfl_sync(FULL, e.u, src);
+  r.cw = __shfl_sync(FULL, e.cw, src);
+  r.d = __shfl_sync(FULL, e.d, src);
+  return r;
+}
 
-// ---- attacker ------------------------------------------------------------
+__device__ __forceinline__ unsigned long long warp_or64(unsigned long long x) {
+  const uint32_t lo = __reduce_or_sync(FULL, (uint32_t)x), hi = __reduce_or_sync(FULL, (uint32_t)(x >> 32));
+  return ((unsigned long long)hi << 32) | lo;
+}
+
+// Store a new list of `cnt` energies held one per lane (`val` at `rank` where
+// `has`): inline when it fits, else in fresh arena space.
+__device__ Res warp_store(const WarpCtx &x, uint32_t val, bool has, uint32_t rank, uint32_t cnt) {
+  x.bytes += 4ull * cnt;
+  if (cnt <= x.p.inl) {
+    const unsigned long long part = has ? ((unsigned long long)val << (rank * x.p.ib)) : 0ull;
+    return Res{R_CHANGED, inl_hdr(cnt) | warp_or64(part)};
+  }
+  unsigned long long off = 0;
+  if (!x.wa.alloc(cnt, x.c, x.cap, x.lane, off)) return Res{R_OVERFLOW, 0};
+  if (has && CHECK_IDX(x.c, off + rank, x.cap)) x.arena[off + rank] = val;
+  return Res{R_CHANGED, mkdesc(off, cnt)};
+}
+
+// Store the members of bitmap `m` (ascending index order).
+__device__ Res bm_store(const WarpCtx &x, BM m) {
+  const uint32_t lane = x.lane;
+  const uint32_t c = (uint32_t)(__popcll(m.w0) + __popcll(m.w1));
+  const uint32_t incl = warp_incl_scan(c, lane);
+  const uint32_t total = __shfl_sync(FULL, incl, 31);
+  uint32_t rank = incl - c;
+  x.bytes += 4ull * total;
+  if (total <= x.p.inl) {
+    unsigned long long part = 0;
+    for (unsigned long long w = m.w0; w; w &= w - 1ull, rank++)
+      part |= (unsigned long long)(lane * 128u + (uint32_t)__ffsll((long long)w) - 1u) << (rank * x.p.ib);
+    for (unsigned long long w = m.w1; w; w &= w - 1ull, rank++)
+      part |= (unsigned long long)(lane * 128u + 64u + (uint32_t)__ffsll((long long)w) - 1u) << (rank * x.p.ib);
+    return Res{R_CHANGED, inl_hdr(total) | warp_or64(part)};
+  }
+  unsigned long long off = 0;
+  if (!x.wa.alloc(total, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0};
+  if (CHECK_IDX(x.c, off + total - 1, x.cap)) {
+    unsigned long long k = off + rank;
+    for (unsigned long long w = m.w0; w; w &= w - 1ull) x.arena[k++] = lane * 128u + (uint32_t)__ffsll((long long)w) - 1u;
+    for (unsigned long long w = m.w1; w; w &= w - 1ull) x.arena[k++] = lane * 128u + 64u + (uint32_t)__ffsll((long long)w) - 1u;
+  }
+  return Res{R_CHANGED, mkdesc(off, total)};
+}
+
+// Store a list of `cnt` packed energies that sits in arena scratch at `src`.
+__device__ Res scratch_store(const WarpCtx &x, unsigned long long src, uint32_t cnt) {
+  if (cnt <= x.p.inl) {
+    const uint32_t lane = x.lane;
+    const uint32_t v = lane < cnt ? ld(x.arena, src + lane, x.cap, x.c) : 0u;
+    return warp_store(x, v, lane < cnt, lane, cnt);
+  }
+  unsigned long long off = 0;
+  if (!x.wa.alloc(cnt, x.c, x.cap, x.lane, off)) return Res{R_OVERFLOW, 0};
+  for (uint32_t q = x.lane; q < cnt; q += 32u)
+    if (CHECK_IDX(x.c, off + q, x.cap)) x.arena[off + q] = ld(x.arena, src + q, x.cap, x.c);
+  x.bytes += 4ull * cnt;
+  return Res{R_CHANGED, mkdesc(off, cnt)};
+}
+
+// ---- attacker (warp routines) ------------------------------------------------
 // attack_update.wgsl:77-113 + attack_minimize.wgsl:180-235: candidates are
 // the inverse-updated successor energies followed by the own energies; keep
 // the minimal ones (on ties the later copy, so own energies win); the
 // position changed iff a kept candidate came from a successor.
 template <class Cd>
-__device__ Res attack_small(const WarpCtx &x, const Cd &cd, uint32_t v, unsigned long long e0, uint32_t d,
-                            uint32_t cv, unsigned long long ov, bool &fits) {
+__device__ Res attack_small(const WarpCtx &x, const Cd &cd, unsigned long long e0, uint32_t d,
+                            unsigned long long dv, bool &fits) {
   const uint32_t lane = x.lane;
+  const uint32_t cv = dcnt(dv);
   EdgeInfo ei{0, 0, 0};
   if (lane < d) ei = edge_info(x, e0 + lane);
   const uint32_t incl = warp_incl_scan(ei.cw, lane);
@@ -310,7 +386,7 @@ __device__ Res attack_small(const WarpCtx &x, const Cd &cd, uint32_t v, unsigned
   const uint32_t K = tot + cv;
   if (K > x.p.small_limit) {
     fits = false;
-    return Res{R_UNCHANGED, 0, 0};
+    return Res{R_UNCHANGED, 0};
   }
   fits = true;
   x.bytes += 16ull * d + 4ull * tot;
@@ -320,41 +396,34 @@ __device__ Res attack_small(const WarpCtx &x, const Cd &cd, uint32_t v, unsigned
   const uint32_t i = lane;
   const uint32_t ed = (i < tot) ? x.sm[SM_TMP + i] : 0u;
   __syncwarp();
-  const unsigned long long ow_e = __shfl_sync(FULL, ei.ow, ed);
+  const unsigned long long d_e = __shfl_sync(FULL, ei.d, ed);
   const uint32_t ex_e = __shfl_sync(FULL, excl, ed);
   const uint32_t u_e = __shfl_sync(FULL, ei.u, ed);
   const bool valid = i < K;
   uint32_t cnd = 0;
-  if (i < tot) cnd = cd.upd(cd.to_t(ld(x.arena, ow_e + (i - ex_e), x.cap, x.c)), u_e);
-  else if (valid) cnd = cd.to_t(ld(x.arena, ov + (i - tot), x.cap, x.c));
+  if (i < tot) cnd = cd.upd(cd.to_t(x.elem(d_e, i - ex_e)), u_e);
+  else if (valid) cnd = cd.to_t(x.elem(dv, i - tot));
   bool killed = false;
   for (uint32_t j = 0; j < K; j++) {
-    uint32_t cj = __shfl_sync(FULL, cnd, j);
+    const uint32_t cj = __shfl_sync(FULL, cnd, j);
     if (valid && j != i) {
-      bool eq = cj == cnd;
+      const bool eq = cj == cnd;
       if ((eq && i < j) || (!eq && t_leq(cj, cnd))) killed = true;
     }
   }
   const bool kept = valid && !killed;
   const uint32_t bal = __ballot_sync(FULL, kept);
   const bool changed = __ballot_sync(FULL, kept && i < tot) != 0u;
-  if (!changed) return Res{R_UNCHANGED, 0, 0};
-  const uint32_t cnt = __popc(bal);
-  unsigned long long off = 0;
-  if (!x.wa.alloc(cnt, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
-  if (kept) {
-    unsigned long long k = off + __popc(bal & lanemask_lt());
-    if (CHECK_IDX(x.c, k, x.cap)) x.arena[k] = cd.to_p(cnd);
-  }
-  x.bytes += 4ull * cnt;
-  return Res{R_CHANGED, off, cnt};
+  if (!changed) return Res{R_UNCHANGED, 0};
+  return warp_store(x, cd.to_p(cnd), kept, __popc(bal & lanemask_lt()), __popc(bal));
 }
 
 // Large attacker positions on STANDARD: candidates go into a 4096-bit set;
 // minimal members = set minus the strict up-closure of the set.
-__device__ Res attack_bitmap(const WarpCtx &x, const CodecStd &cd, uint32_t v, unsigned long long e0,
-                             unsigned long long e1, uint32_t cv, unsigned long long ov) {
+__device__ Res attack_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0, unsigned long long e1,
+                             unsigned long long dv) {
   const uint32_t lane = x.lane;
+  const uint32_t cv = dcnt(dv);
   for (uint32_t k = lane; k < 256u; k += 32u) x.sm[SM_BM + k] = 0u;
   __syncwarp();
   unsigned long long tot = 0;
@@ -363,17 +432,14 @@ __device__ Res attack_bitmap(const WarpCtx &x, const CodecStd &cd, uint32_t v, u
     if (k0 + lane < e1) ei = edge_info(x, k0 + lane);
     const uint32_t nk = (uint32_t)min(32ull, e1 - k0);
     for (uint32_t j = 0; j < nk; j++) {
-      const uint32_t cwj = __shfl_sync(FULL, ei.cw, j);
-      const unsigned long long owj = __shfl_sync(FULL, ei.ow, j);
-      const uint32_t uj = __shfl_sync(FULL, ei.u, j);
-      tot += cwj;
-      for (uint32_t q = lane; q < cwj; q += 32u)
-        bm_set(x.sm + SM_BM, cd.to_p(cd.upd(cd.to_t(ld(x.arena, owj + q, x.cap, x.c)), uj)));
+      const EdgeInfo e = shfl_edge(ei, j);
+      tot += e.cw;
+      for (uint32_t q = lane; q < e.cw; q += 32u) bm_set(x.sm + SM_BM, cd.to_p(cd.upd(cd.to_t(x.elem(e.d, q)), e.u)));
     }
   }
   x.bytes += 16ull * (e1 - e0) + 4ull * tot;
   for (uint32_t q = lane; q < cv; q += 32u) {
-    uint32_t idx = ld(x.arena, ov + q, x.cap, x.c);
+    const uint32_t idx = x.elem(dv, q);
     bm_set(x.sm + SM_BM, idx);
     bm_set(x.sm + SM_BM2, idx);
   }
@@ -386,58 +452,49 @@ __device__ Res attack_bitmap(const WarpCtx &x, const CodecStd &cd, uint32_t v, u
   m.w0 = b.w0 & ~su.w0;
   m.w1 = b.w1 & ~su.w1;
   const bool changed = __ballot_sync(FULL, ((m.w0 & ~own.w0) | (m.w1 & ~own.w1)) != 0ull) != 0u;
-  if (!changed) return Res{R_UNCHANGED, 0, 0};
-  const uint32_t c = (uint32_t)(__popcll(m.w0) + __popcll(m.w1));
-  const uint32_t incl = warp_incl_scan(c, lane);
-  const uint32_t total = __shfl_sync(FULL, incl, 31);
-  unsigned long long off = 0;
-  if (!x.wa.alloc(total, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
-  if (CHECK_IDX(x.c, off + total - 1, x.cap)) bm_emit(m, lane, x.arena, off, incl - c);
-  x.bytes += 4ull * total;
-  return Res{R_CHANGED, off, total};
+  if (!changed) return Res{R_UNCHANGED, 0};
+  return bm_store(x, m);
 }
 
 // Large attacker positions on other confs: candidates in arena scratch,
-// pairwise minimisation.  Same tie rule as attack_minimize.wgsl.
+// pairwise minimisation (same tie rule).
 template <class Cd>
-__device__ Res attack_list(const WarpCtx &x, const Cd &cd, uint32_t v, unsigned long long e0,
-                           unsigned long long e1, uint32_t cv, unsigned long long ov) {
+__device__ Res attack_list(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
+                           unsigned long long dv) {
   const uint32_t lane = x.lane;
+  const uint32_t cv = dcnt(dv);
   unsigned long long K = cv;
   for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
     EdgeInfo ei{0, 0, 0};
     if (k0 + lane < e1) ei = edge_info(x, k0 + lane);
-    uint32_t incl = warp_incl_scan(ei.cw, lane);
+    const uint32_t incl = warp_incl_scan(ei.cw, lane);
     K += __shfl_sync(FULL, incl, 31);
   }
   if (K > CNT_MASK) {
     if (lane == 0) { atomicOr(&x.c->error, DERR_SCRATCH); atomicExch(&x.c->halt, 1u); }
-    return Res{R_ERROR, 0, 0};
+    return Res{R_ERROR, 0};
   }
   unsigned long long sc = 0;
-  if (!x.wa.alloc((uint32_t)K, x.c, x.cap, lane, sc)) return Res{R_OVERFLOW, 0, 0};
+  if (!x.wa.alloc((uint32_t)K, x.c, x.cap, lane, sc)) return Res{R_OVERFLOW, 0};
   unsigned long long pos = 0;
   for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
     EdgeInfo ei{0, 0, 0};
     if (k0 + lane < e1) ei = edge_info(x, k0 + lane);
     const uint32_t nk = (uint32_t)min(32ull, e1 - k0);
     for (uint32_t j = 0; j < nk; j++) {
-      const uint32_t cwj = __shfl_sync(FULL, ei.cw, j);
-      const unsigned long long owj = __shfl_sync(FULL, ei.ow, j);
-      const uint32_t uj = __shfl_sync(FULL, ei.u, j);
-      for (uint32_t q = lane; q < cwj; q += 32u)
-        if (CHECK_IDX(x.c, sc + pos + q, x.cap))
-          x.arena[sc + pos + q] = cd.upd(cd.to_t(ld(x.arena, owj + q, x.cap, x.c)), uj);
-      pos += cwj;
+      const EdgeInfo e = shfl_edge(ei, j);
+      for (uint32_t q = lane; q < e.cw; q += 32u)
+        if (CHECK_IDX(x.c, sc + pos + q, x.cap)) x.arena[sc + pos + q] = cd.upd(cd.to_t(x.elem(e.d, q)), e.u);
+      pos += e.cw;
     }
   }
   x.bytes += 16ull * (e1 - e0) + 4ull * pos;
   const unsigned long long tot = pos;
   for (uint32_t q = lane; q < cv; q += 32u)
-    if (CHECK_IDX(x.c, sc + tot + q, x.cap)) x.arena[sc + tot + q] = cd.to_t(ld(x.arena, ov + q, x.cap, x.c));
+    if (CHECK_IDX(x.c, sc + tot + q, x.cap)) x.arena[sc + tot + q] = cd.to_t(x.elem(dv, q));
   __syncwarp();
   unsigned long long out = 0;
-  if (!x.wa.alloc((uint32_t)K, x.c, x.cap, lane, out)) return Res{R_OVERFLOW, 0, 0};
+  if (!x.wa.alloc((uint32_t)K, x.c, x.cap, lane, out)) return Res{R_OVERFLOW, 0};
   uint32_t cnt = 0;
   bool changed = false;
   for (unsigned long long i0 = 0; i0 < K; i0 += 32) {
@@ -449,25 +506,25 @@ __device__ Res attack_list(const WarpCtx &x, const Cd &cd, uint32_t v, unsigned 
       kept = true;
       for (unsigned long long j = 0; j < K; j++) {
         if (j == i) continue;
-        uint32_t cj = ld(x.arena, sc + j, x.cap, x.c);
-        bool eq = cj == ci;
+        const uint32_t cj = ld(x.arena, sc + j, x.cap, x.c);
+        const bool eq = cj == ci;
         if ((eq && i < j) || (!eq && t_leq(cj, ci))) { kept = false; break; }
       }
     }
     const uint32_t bal = __ballot_sync(FULL, kept);
     if (__ballot_sync(FULL, kept && i < tot)) changed = true;
     if (kept) {
-      unsigned long long k = out + cnt + __popc(bal & lanemask_lt());
+      const unsigned long long k = out + cnt + __popc(bal & lanemask_lt());
       if (CHECK_IDX(x.c, k, x.cap)) x.arena[k] = cd.to_p(ci);
     }
     cnt += __popc(bal);
   }
-  if (!changed) return Res{R_UNCHANGED, 0, 0};
-  x.bytes += 4ull * cnt;
-  return Res{R_CHANGED, out, cnt};
+  __syncwarp();
+  if (!changed) return Res{R_UNCHANGED, 0};
+  return scratch_store(x, out, cnt);
 }
 
-// ---- defender --------------------------------------------------------------
+// ---- defender (warp routines) --------------------------------------------------
 // Reference semantics (energygame.rs:896-944 with defend_iterative.wgsl):
 // the new list is min{ a_1 v ... v a_d : a_k in upd_k(A_{w_k}) } (the first
 // successor's updated list is taken as is when there is only one successor);
@@ -476,37 +533,36 @@ __device__ Res attack_list(const WarpCtx &x, const Cd &cd, uint32_t v, unsigned 
 // energy occurs in the old list).
 
 // changed-test for a new list held in lanes (n <= 32) against the old list.
-template <class Cd>
-__device__ bool differs_small(const WarpCtx &x, const Cd &cd, uint32_t newp, uint32_t n, uint32_t cv,
-                              unsigned long long ov) {
+__device__ bool differs_small(const WarpCtx &x, uint32_t newp, uint32_t n, unsigned long long dv) {
+  const uint32_t cv = dcnt(dv);
   if (n != cv) return true;
   const uint32_t lane = x.lane;
-  const uint32_t o = (lane < cv) ? ld(x.arena, ov + lane, x.cap, x.c) : 0u;
+  const uint32_t o = (lane < cv) ? x.elem(dv, lane) : 0u;
   bool found = false;
   for (uint32_t j = 0; j < cv; j++) found |= (__shfl_sync(FULL, o, j) == newp);
   return __ballot_sync(FULL, lane < n && !found) != 0u;
 }
 
 template <class Cd>
-__device__ Res defend_single(const WarpCtx &x, const Cd &cd, const EdgeInfo &e, uint32_t cv,
-                             unsigned long long ov) {
+__device__ Res defend_single(const WarpCtx &x, const Cd &cd, const EdgeInfo &e, unsigned long long dv) {
   const uint32_t lane = x.lane;
+  const uint32_t cv = dcnt(dv);
   const uint32_t n = e.cw;
   x.bytes += 16ull + 4ull * n;
   bool changed;
   if (n != cv) {
     changed = true;
   } else if (n <= 32u) {
-    uint32_t np = (lane < n) ? cd.to_p(cd.upd(cd.to_t(ld(x.arena, e.ow + lane, x.cap, x.c)), e.u)) : 0u;
-    changed = differs_small(x, cd, np, n, cv, ov);
+    const uint32_t np = (lane < n) ? cd.to_p(cd.upd(cd.to_t(x.elem(e.d, lane)), e.u)) : 0u;
+    changed = differs_small(x, np, n, dv);
   } else if (Cd::kBitmap) {
     for (uint32_t k = lane; k < 128u; k += 32u) x.sm[SM_BM2 + k] = 0u;
     __syncwarp();
-    for (uint32_t q = lane; q < cv; q += 32u) bm_set(x.sm + SM_BM2, ld(x.arena, ov + q, x.cap, x.c));
+    for (uint32_t q = lane; q < cv; q += 32u) bm_set(x.sm + SM_BM2, x.elem(dv, q));
     __syncwarp();
     bool miss = false;
     for (uint32_t q = lane; q < n; q += 32u) {
-      uint32_t idx = cd.to_p(cd.upd(cd.to_t(ld(x.arena, e.ow + q, x.cap, x.c)), e.u)) & 0xFFFu;
+      const uint32_t idx = cd.to_p(cd.upd(cd.to_t(x.elem(e.d, q)), e.u)) & 0xFFFu;
       miss |= ((x.sm[SM_BM2 + (idx >> 5)] >> (idx & 31u)) & 1u) == 0u;
     }
     changed = __ballot_sync(FULL, miss) != 0u;
@@ -514,86 +570,78 @@ __device__ Res defend_single(const WarpCtx &x, const Cd &cd, const EdgeInfo &e, 
   } else {
     bool miss = false;
     for (uint32_t q = lane; q < n; q += 32u) {
-      uint32_t np = cd.to_p(cd.upd(cd.to_t(ld(x.arena, e.ow + q, x.cap, x.c)), e.u));
+      const uint32_t np = cd.to_p(cd.upd(cd.to_t(x.elem(e.d, q)), e.u));
       bool found = false;
-      for (uint32_t j = 0; j < cv && !found; j++) found = ld(x.arena, ov + j, x.cap, x.c) == np;
+      for (uint32_t j = 0; j < cv && !found; j++) found = x.elem(dv, j) == np;
       miss |= !found;
     }
     changed = __ballot_sync(FULL, miss) != 0u;
   }
-  if (!changed) return Res{R_UNCHANGED, 0, 0};
+  if (!changed) return Res{R_UNCHANGED, 0};
+  if (n <= 32u)
+    return warp_store(x, lane < n ? cd.to_p(cd.upd(cd.to_t(x.elem(e.d, lane)), e.u)) : 0u, lane < n, lane, n);
   unsigned long long off = 0;
-  if (!x.wa.alloc(n, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
+  if (!x.wa.alloc(n, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0};
   for (uint32_t q = lane; q < n; q += 32u)
-    if (CHECK_IDX(x.c, off + q, x.cap))
-      x.arena[off + q] = cd.to_p(cd.upd(cd.to_t(ld(x.arena, e.ow + q, x.cap, x.c)), e.u));
+    if (CHECK_IDX(x.c, off + q, x.cap)) x.arena[off + q] = cd.to_p(cd.upd(cd.to_t(x.elem(e.d, q)), e.u));
   x.bytes += 4ull * n;
-  return Res{R_CHANGED, off, n};
+  return Res{R_CHANGED, mkdesc(off, n)};
 }
 
 // Fold of up to 32 successors whose pairwise combinations stay <= 32: the
 // running antichain lives in one register per lane.
 template <class Cd>
-__device__ Res defend_small(const WarpCtx &x, const Cd &cd, unsigned long long e0, uint32_t d, uint32_t cv,
-                            unsigned long long ov, bool &fits) {
+__device__ Res defend_small(const WarpCtx &x, const Cd &cd, unsigned long long e0, uint32_t d,
+                            unsigned long long dv, bool &fits) {
   const uint32_t lane = x.lane;
   EdgeInfo ei{0, 0, 0};
   if (lane < d) ei = edge_info(x, e0 + lane);
   uint32_t s = __shfl_sync(FULL, ei.cw, 0);
   fits = false;
-  if (s > x.p.small_limit) return Res{R_UNCHANGED, 0, 0};
-  {
-    const unsigned long long ow0 = __shfl_sync(FULL, ei.ow, 0);
-    const uint32_t u0 = __shfl_sync(FULL, ei.u, 0);
-    uint32_t S = (lane < s) ? cd.upd(cd.to_t(ld(x.arena, ow0 + lane, x.cap, x.c)), u0) : 0u;
-    for (uint32_t k = 1; k < d; k++) {
-      const uint32_t cb = __shfl_sync(FULL, ei.cw, k);
-      const unsigned long long ob = __shfl_sync(FULL, ei.ow, k);
-      const uint32_t ub = __shfl_sync(FULL, ei.u, k);
-      const uint32_t combos = s * cb;
-      if (combos > x.p.small_limit) return Res{R_UNCHANGED, 0, 0};  // fits stays false
-      const uint32_t l = lane;
-      const bool valid = l < combos;
-      const uint32_t a = __shfl_sync(FULL, S, valid ? (l % s) : 0u);
-      uint32_t cc = 0;
-      if (valid) cc = a | cd.upd(cd.to_t(ld(x.arena, ob + l / s, x.cap, x.c)), ub);
-      bool killed = false;
-      for (uint32_t j = 0; j < combos; j++) {
-        uint32_t cj = __shfl_sync(FULL, cc, j);
-        if (valid && j != l) {
-          bool eq = cj == cc;
-          if ((eq && l > j) || (!eq && t_leq(cj, cc))) killed = true;
-        }
+  if (s > x.p.small_limit) return Res{R_UNCHANGED, 0};
+  const EdgeInfo e0i = shfl_edge(ei, 0);
+  uint32_t S = (lane < s) ? cd.upd(cd.to_t(x.elem(e0i.d, lane)), e0i.u) : 0u;
+  for (uint32_t k = 1; k < d; k++) {
+    const EdgeInfo b = shfl_edge(ei, k);
+    const uint32_t combos = s * b.cw;
+    if (combos > x.p.small_limit) return Res{R_UNCHANGED, 0};  // fits stays false
+    const uint32_t l = lane;
+    const bool valid = l < combos;
+    const uint32_t a = __shfl_sync(FULL, S, valid ? (l % s) : 0u);
+    uint32_t cc = 0;
+    if (valid) cc = a | cd.upd(cd.to_t(x.elem(b.d, l / s)), b.u);
+    bool killed = false;
+    for (uint32_t j = 0; j < combos; j++) {
+      const uint32_t cj = __shfl_sync(FULL, cc, j);
+      if (valid && j != l) {
+        const bool eq = cj == cc;
+        if ((eq && l > j) || (!eq && t_leq(cj, cc))) killed = true;
       }
-      const bool kept = valid && !killed;
-      const uint32_t bal = __ballot_sync(FULL, kept);
-      if (kept) x.sm[SM_TMP + __popc(bal & lanemask_lt())] = cc;
-      __syncwarp();
-      s = __popc(bal);
-      S = (lane < s) ? x.sm[SM_TMP + lane] : 0u;
-      __syncwarp();
     }
-    fits = true;
-    unsigned long long tot = 0;
-    if (lane < d) tot = ei.cw;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(FULL, tot, o);
-    x.bytes += 16ull * d + 4ull * tot;
-    const uint32_t np = (lane < s) ? cd.to_p(S) : 0u;
-    if (!differs_small(x, cd, np, s, cv, ov)) return Res{R_UNCHANGED, 0, 0};
-    unsigned long long off = 0;
-    if (!x.wa.alloc(s, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
-    if (lane < s && CHECK_IDX(x.c, off + lane, x.cap)) x.arena[off + lane] = np;
-    x.bytes += 4ull * s;
-    return Res{R_CHANGED, off, s};
+    const bool kept = valid && !killed;
+    const uint32_t bal = __ballot_sync(FULL, kept);
+    if (kept) x.sm[SM_TMP + __popc(bal & lanemask_lt())] = cc;
+    __syncwarp();
+    s = __popc(bal);
+    S = (lane < s) ? x.sm[SM_TMP + lane] : 0u;
+    __syncwarp();
   }
+  fits = true;
+  unsigned long long tot = (lane < d) ? ei.cw : 0ull;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(FULL, tot, o);
+  x.bytes += 16ull * d + 4ull * tot;
+  const uint32_t np = (lane < s) ? cd.to_p(S) : 0u;
+  if (!differs_small(x, np, s, dv)) return Res{R_UNCHANGED, 0};
+  return warp_store(x, np, lane < s, lane, s);
 }
 
 // STANDARD defender with large lists: intersect the up-closures of the
 // updated successor lists in a 4096-bit set, then take its minimal members.
-__device__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0,
-                             unsigned long long e1, uint32_t cv, unsigned long long ov) {
+__device__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0, unsigned long long e1,
+                             unsigned long long dv) {
   const uint32_t lane = x.lane;
+  const uint32_t cv = dcnt(dv);
   BM acc;
   acc.w0 = ~0ull;
   acc.w1 = ~0ull;
@@ -603,14 +651,11 @@ __device__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long
     if (k0 + lane < e1) ei = edge_info(x, k0 + lane);
     const uint32_t nk = (uint32_t)min(32ull, e1 - k0);
     for (uint32_t j = 0; j < nk; j++) {
-      const uint32_t cwj = __shfl_sync(FULL, ei.cw, j);
-      const unsigned long long owj = __shfl_sync(FULL, ei.ow, j);
-      const uint32_t uj = __shfl_sync(FULL, ei.u, j);
-      tot += cwj;
+      const EdgeInfo e = shfl_edge(ei, j);
+      tot += e.cw;
       for (uint32_t k = lane; k < 128u; k += 32u) x.sm[SM_BM + k] = 0u;
       __syncwarp();
-      for (uint32_t q = lane; q < cwj; q += 32u)
-        bm_set(x.sm + SM_BM, cd.to_p(cd.upd(cd.to_t(ld(x.arena, owj + q, x.cap, x.c)), uj)));
+      for (uint32_t q = lane; q < e.cw; q += 32u) bm_set(x.sm + SM_BM, cd.to_p(cd.upd(cd.to_t(x.elem(e.d, q)), e.u)));
       __syncwarp();
       const BM u = up_closure(bm_load(x.sm + SM_BM, lane), lane);
       __syncwarp();
@@ -625,60 +670,50 @@ __device__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long
   m.w1 = acc.w1 & ~st.w1;
   for (uint32_t k = lane; k < 128u; k += 32u) x.sm[SM_BM2 + k] = 0u;
   __syncwarp();
-  for (uint32_t q = lane; q < cv; q += 32u) bm_set(x.sm + SM_BM2, ld(x.arena, ov + q, x.cap, x.c));
+  for (uint32_t q = lane; q < cv; q += 32u) bm_set(x.sm + SM_BM2, x.elem(dv, q));
   __syncwarp();
   const BM old = bm_load(x.sm + SM_BM2, lane);
   __syncwarp();
-  const uint32_t c = (uint32_t)(__popcll(m.w0) + __popcll(m.w1));
-  const uint32_t incl = warp_incl_scan(c, lane);
-  const uint32_t total = __shfl_sync(FULL, incl, 31);
+  const uint32_t total = (uint32_t)__reduce_add_sync(FULL, (uint32_t)(__popcll(m.w0) + __popcll(m.w1)));
   const bool changed =
       total != cv || __ballot_sync(FULL, ((m.w0 & ~old.w0) | (m.w1 & ~old.w1)) != 0ull) != 0u;
-  if (!changed) return Res{R_UNCHANGED, 0, 0};
-  unsigned long long off = 0;
-  if (!x.wa.alloc(total, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
-  if (CHECK_IDX(x.c, off + total - 1, x.cap)) bm_emit(m, lane, x.arena, off, incl - c);
-  x.bytes += 4ull * total;
-  return Res{R_CHANGED, off, total};
+  if (!changed) return Res{R_UNCHANGED, 0};
+  return bm_store(x, m);
 }
 
 // Other confs with large lists: the fold of defend_iterative.wgsl with the
 // running list and the combinations in arena scratch.
 template <class Cd>
 __device__ Res defend_list(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
-                           uint32_t cv, unsigned long long ov) {
+                           unsigned long long dv) {
   const uint32_t lane = x.lane;
+  const uint32_t cv = dcnt(dv);
   EdgeInfo f{0, 0, 0};
   if (lane == 0) f = edge_info(x, e0);
-  f.cw = __shfl_sync(FULL, f.cw, 0);
-  f.ow = __shfl_sync(FULL, f.ow, 0);
-  f.u = __shfl_sync(FULL, f.u, 0);
+  f = shfl_edge(f, 0);
   unsigned long long S = 0;
   uint32_t s = f.cw;
-  if (!x.wa.alloc(s, x.c, x.cap, lane, S)) return Res{R_OVERFLOW, 0, 0};
+  if (!x.wa.alloc(s, x.c, x.cap, lane, S)) return Res{R_OVERFLOW, 0};
   for (uint32_t q = lane; q < s; q += 32u)
-    if (CHECK_IDX(x.c, S + q, x.cap)) x.arena[S + q] = cd.upd(cd.to_t(ld(x.arena, f.ow + q, x.cap, x.c)), f.u);
+    if (CHECK_IDX(x.c, S + q, x.cap)) x.arena[S + q] = cd.upd(cd.to_t(x.elem(f.d, q)), f.u);
   unsigned long long tot = s;
   __syncwarp();
   for (unsigned long long k = e0 + 1; k < e1; k++) {
     EdgeInfo b{0, 0, 0};
     if (lane == 0) b = edge_info(x, k);
-    b.cw = __shfl_sync(FULL, b.cw, 0);
-    b.ow = __shfl_sync(FULL, b.ow, 0);
-    b.u = __shfl_sync(FULL, b.u, 0);
+    b = shfl_edge(b, 0);
     tot += b.cw;
     const unsigned long long combos = (unsigned long long)s * b.cw;
     if (combos > (1ull << 22)) {
       if (lane == 0) { atomicOr(&x.c->error, DERR_SCRATCH); atomicExch(&x.c->halt, 1u); }
-      return Res{R_ERROR, 0, 0};
+      return Res{R_ERROR, 0};
     }
     unsigned long long C = 0, N = 0;
-    if (!x.wa.alloc((uint32_t)combos, x.c, x.cap, lane, C)) return Res{R_OVERFLOW, 0, 0};
-    if (!x.wa.alloc((uint32_t)combos, x.c, x.cap, lane, N)) return Res{R_OVERFLOW, 0, 0};
+    if (!x.wa.alloc((uint32_t)combos, x.c, x.cap, lane, C)) return Res{R_OVERFLOW, 0};
+    if (!x.wa.alloc((uint32_t)combos, x.c, x.cap, lane, N)) return Res{R_OVERFLOW, 0};
     for (unsigned long long l = lane; l < combos; l += 32)
       if (CHECK_IDX(x.c, C + l, x.cap))
-        x.arena[C + l] = ld(x.arena, S + l % s, x.cap, x.c) |
-                         cd.upd(cd.to_t(ld(x.arena, b.ow + l / s, x.cap, x.c)), b.u);
+        x.arena[C + l] = ld(x.arena, S + l % s, x.cap, x.c) | cd.upd(cd.to_t(x.elem(b.d, (uint32_t)(l / s))), b.u);
     __syncwarp();
     uint32_t cnt = 0;
     for (unsigned long long l0 = 0; l0 < combos; l0 += 32) {
@@ -690,14 +725,14 @@ __device__ Res defend_list(const WarpCtx &x, const Cd &cd, unsigned long long e0
         kept = true;
         for (unsigned long long j = 0; j < combos; j++) {
           if (j == l) continue;
-          uint32_t cj = ld(x.arena, C + j, x.cap, x.c);
-          bool eq = cj == cl;
+          const uint32_t cj = ld(x.arena, C + j, x.cap, x.c);
+          const bool eq = cj == cl;
           if ((eq && l > j) || (!eq && t_leq(cj, cl))) { kept = false; break; }
         }
       }
       const uint32_t bal = __ballot_sync(FULL, kept);
       if (kept) {
-        unsigned long long kk = N + cnt + __popc(bal & lanemask_lt());
+        const unsigned long long kk = N + cnt + __popc(bal & lanemask_lt());
         if (CHECK_IDX(x.c, kk, x.cap)) x.arena[kk] = cl;
       }
       cnt += __popc(bal);
@@ -707,25 +742,23 @@ __device__ Res defend_list(const WarpCtx &x, const Cd &cd, unsigned long long e0
     s = cnt;
   }
   x.bytes += 16ull * (e1 - e0) + 4ull * tot;
-  // changed test: same length and every new energy among the old ones
+  // packed copies for the comparison and the store
+  for (uint32_t q = lane; q < s; q += 32u)
+    if (CHECK_IDX(x.c, S + q, x.cap)) x.arena[S + q] = cd.to_p(ld(x.arena, S + q, x.cap, x.c));
+  __syncwarp();
   bool changed = s != cv;
   if (!changed) {
     bool miss = false;
     for (uint32_t q = lane; q < s; q += 32u) {
-      uint32_t np = cd.to_p(ld(x.arena, S + q, x.cap, x.c));
+      const uint32_t np = ld(x.arena, S + q, x.cap, x.c);
       bool found = false;
-      for (uint32_t j = 0; j < cv && !found; j++) found = ld(x.arena, ov + j, x.cap, x.c) == np;
+      for (uint32_t j = 0; j < cv && !found; j++) found = x.elem(dv, j) == np;
       miss |= !found;
     }
     changed = __ballot_sync(FULL, miss) != 0u;
   }
-  if (!changed) return Res{R_UNCHANGED, 0, 0};
-  unsigned long long off = 0;
-  if (!x.wa.alloc(s, x.c, x.cap, lane, off)) return Res{R_OVERFLOW, 0, 0};
-  for (uint32_t q = lane; q < s; q += 32u)
-    if (CHECK_IDX(x.c, off + q, x.cap)) x.arena[off + q] = cd.to_p(ld(x.arena, S + q, x.cap, x.c));
-  x.bytes += 4ull * s;
-  return Res{R_CHANGED, off, s};
+  if (!changed) return Res{R_UNCHANGED, 0};
+  return scratch_store(x, S, s);
 }
 
 template <class Cd>
@@ -735,60 +768,220 @@ __device__ Res solve_position(const WarpCtx &x, const Cd &cd, uint32_t v) {
   const unsigned long long e1 = ld(x.p.row, (unsigned long long)v + 1, x.p.n_nodes + 1, x.c);
   const uint32_t d = (uint32_t)(e1 - e0);
   const unsigned long long dv = ld(x.p.desc, v, x.p.n_nodes, x.c);
-  const uint32_t cv = dcnt(dv);
-  const unsigned long long ov = doff(dv);
   const bool attacker = ld(x.p.flags, v, x.p.n_nodes, x.c) & 1u;
-  if (d == 0) return Res{R_SKIPPED, 0, 0};
+  if (d == 0) return Res{R_SKIPPED, 0};
   if (attacker) {
     x.edges += d;
-    x.bytes += 12ull + 4ull * cv;
+    x.bytes += 12ull + 4ull * dcnt(dv);
     if (d <= 32u && x.p.small_limit > 0) {
       bool fits = false;
-      Res r = attack_small(x, cd, v, e0, d, cv, ov, fits);
+      const Res r = attack_small(x, cd, e0, d, dv, fits);
       if (fits) return r;
     }
-    if constexpr (Cd::kBitmap) return attack_bitmap(x, cd, v, e0, e1, cv, ov);
-    else return attack_list(x, cd, v, e0, e1, cv, ov);
+    if constexpr (Cd::kBitmap) return attack_bitmap(x, cd, e0, e1, dv);
+    else return attack_list(x, cd, e0, e1, dv);
   }
   // defender: skipped while a successor has no energies (energygame.rs:789-792)
   bool empty = false;
   for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
     bool e = false;
     if (k0 + lane < e1) {
-      uint32_t w = ld(x.p.col, k0 + lane, x.p.n_edges, x.c);
+      const uint32_t w = ld(x.p.col, k0 + lane, x.p.n_edges, x.c);
       e = dcnt(ld(x.p.desc, w, x.p.n_nodes, x.c)) == 0u;
     }
     if (__ballot_sync(FULL, e)) { empty = true; break; }
   }
-  if (empty) return Res{R_SKIPPED, 0, 0};
+  if (empty) return Res{R_SKIPPED, 0};
   x.edges += d;
   x.bytes += 12ull;
   if (d == 1u) {
     EdgeInfo e{0, 0, 0};
     if (lane == 0) e = edge_info(x, e0);
-    e.cw = __shfl_sync(FULL, e.cw, 0);
-    e.ow = __shfl_sync(FULL, e.ow, 0);
-    e.u = __shfl_sync(FULL, e.u, 0);
-    return defend_single(x, cd, e, cv, ov);
+    return defend_single(x, cd, shfl_edge(e, 0), dv);
   }
   if (d <= 32u && x.p.small_limit > 0) {
     bool fits = false;
-    Res r = defend_small(x, cd, e0, d, cv, ov, fits);
+    const Res r = defend_small(x, cd, e0, d, dv, fits);
     if (fits) return r;
   }
-  if constexpr (Cd::kBitmap) return defend_bitmap(x, cd, e0, e1, cv, ov);
-  else return defend_list(x, cd, e0, e1, cv, ov);
+  if constexpr (Cd::kBitmap) return defend_bitmap(x, cd, e0, e1, dv);
+  else return defend_list(x, cd, e0, e1, dv);
 }
 
-// Append the predecessors of v (reverse CSR) to the next frontier once.
-__device__ void push_preds(const KParams &p, Ctr *c, uint32_t v, uint32_t *NF, uint32_t *nf_size,
-                           uint32_t stamp, uint32_t lane) {
-  const unsigned long long b = ld(p.rrow, v, p.n_nodes + 1, c), e = ld(p.rrow, (unsigned long long)v + 1, p.n_nodes + 1, c);
-  for (unsigned long long k0 = b; k0 < e; k0 += 32) {
-    const unsigned long long k = k0 + lane;
+// ---- thread path: one lane per small position -----------------------------
+// Most positions have a handful of successors with one or two energies each.
+// Every lane of a warp solves its own such position with the same rules as
+// the warp routines above, keeping candidates in a lane-private column of
+// shared memory; positions beyond TD successors or TK candidates go to the
+// warp routines.
+constexpr uint32_t TK = 16;   // candidates (and combinations) per lane
+constexpr uint32_t TD = 16;   // successors per lane
+constexpr int TSCR = 2 * TK;  // scratch words per lane: [0,TK) work set, [TK,2TK) result
+enum : int { T_NONE = 0, T_UNCHANGED = 1, T_CHANGED = 2, T_SKIPPED = 3, T_BIG = 4, T_OVERFLOW = 5 };
+
+// scratch column of this lane: word i at scr[i * 32]
+#define SCR(i) scr[(uint32_t)(i) * 32u]
+
+template <class Cd>
+__device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32_t *arena, unsigned long long cap,
+                            uint32_t v, uint32_t *scr, uint32_t &out_cnt, unsigned long long &edges,
+                            unsigned long long &bytes) {
+  const uint32_t e0 = ld(p.row, v, p.n_nodes + 1, c), e1 = ld(p.row, (unsigned long long)v + 1, p.n_nodes + 1, c);
+  const uint32_t d = e1 - e0;
+  if (d == 0) return T_SKIPPED;
+  if (d > TD) return T_BIG;
+  const unsigned long long dv = ld(p.desc, v, p.n_nodes, c);
+  const uint32_t cv = dcnt(dv);
+  const bool attacker = ld(p.flags, v, p.n_nodes, c) & 1u;
+  if (attacker) {
+    // attack_update.wgsl + attack_minimize.wgsl, one lane
+    if (cv > TK) return T_BIG;
+    uint32_t k = 0;
+    for (uint32_t j0 = 0; j0 < d; j0 += 4) {
+      uint32_t w[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
+      unsigned long long dw[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+        if (j0 + t < d) {
+          w[t] = ld(p.col, (unsigned long long)e0 + j0 + t, p.n_edges, c);
+          u[t] = ld(p.wt, (unsigned long long)e0 + j0 + t, p.n_edges, c);
+        }
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+        if (j0 + t < d) dw[t] = ld(p.desc, w[t], p.n_nodes, c);
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+        if (j0 + t < d) {
+          const uint32_t cw = dcnt(dw[t]);
+          if (k + cw + cv > TK) return T_BIG;
+          for (uint32_t q = 0; q < cw; q++) SCR(k++) = cd.upd(cd.to_t(lelem(dw[t], q, arena, cap, c, p.ib, p.ibm)), u[t]);
+        }
+    }
+    const uint32_t tot = k;
+    for (uint32_t q = 0; q < cv; q++) SCR(k++) = cd.to_t(lelem(dv, q, arena, cap, c, p.ib, p.ibm));
+    const uint32_t K = k;
+    uint32_t keep = 0;
+    bool changed = false;
+    for (uint32_t i = 0; i < K; i++) {
+      const uint32_t ci = SCR(i);
+      bool kill = false;
+      for (uint32_t j = 0; j < K && !kill; j++) {
+        if (j == i) continue;
+        const uint32_t cj = SCR(j);
+        kill = (cj == ci) ? (i < j) : t_leq(cj, ci);
+      }
+      if (!kill) {
+        keep |= 1u << i;
+        if (i < tot) changed = true;
+      }
+    }
+    edges += d;
+    bytes += 12ull + 4ull * cv + 16ull * d + 4ull * tot;
+    if (!changed) return T_UNCHANGED;
+    uint32_t n = 0;
+    for (uint32_t i = 0; i < K; i++)
+      if (keep & (1u << i)) SCR(TK + n++) = cd.to_p(SCR(i));
+    out_cnt = n;
+    return T_CHANGED;
+  }
+  // defender: skipped while a successor has no energies (energygame.rs:789-792)
+  for (uint32_t j0 = 0; j0 < d; j0 += 4) {
+    uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int t = 0; t < 4; t++)
+      if (j0 + t < d) w[t] = ld(p.col, (unsigned long long)e0 + j0 + t, p.n_edges, c);
+#pragma unroll
+    for (int t = 0; t < 4; t++)
+      if (j0 + t < d && dcnt(ld(p.desc, w[t], p.n_nodes, c)) == 0u) return T_SKIPPED;
+  }
+  uint32_t n;
+  {
+    const uint32_t w0 = ld(p.col, e0, p.n_edges, c), u0 = ld(p.wt, e0, p.n_edges, c);
+    const unsigned long long d0 = ld(p.desc, w0, p.n_nodes, c);
+    uint32_t s = dcnt(d0);
+    if (s > TK) return T_BIG;
+    unsigned long long tot = s;
+    if (d == 1) {
+      // single successor: its updated list as is (defend_iterative.wgsl:301-313)
+      for (uint32_t q = 0; q < s; q++) SCR(TK + q) = cd.to_p(cd.upd(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), u0));
+      n = s;
+    } else {
+      for (uint32_t q = 0; q < s; q++) SCR(q) = cd.upd(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), u0);
+      for (uint32_t j = 1; j < d; j++) {
+        const uint32_t w = ld(p.col, (unsigned long long)e0 + j, p.n_edges, c);
+        const uint32_t u = ld(p.wt, (unsigned long long)e0 + j, p.n_edges, c);
+        const unsigned long long db = ld(p.desc, w, p.n_nodes, c);
+        const uint32_t cb = dcnt(db);
+        tot += cb;
+        const uint32_t combos = s * cb;
+        if (combos > TK) return T_BIG;
+        for (uint32_t l = 0; l < combos; l++)
+          SCR(TK + l) = SCR(l % s) | cd.upd(cd.to_t(lelem(db, l / s, arena, cap, c, p.ib, p.ibm)), u);
+        // minimise; equal combinations keep the lowest index (defend_iterative.wgsl:243-258)
+        uint32_t keep = 0;
+        for (uint32_t l = 0; l < combos; l++) {
+          const uint32_t cl = SCR(TK + l);
+          bool kill = false;
+          for (uint32_t m = 0; m < combos && !kill; m++) {
+            if (m == l) continue;
+            const uint32_t cm = SCR(TK + m);
+            kill = (cm == cl) ? (l > m) : t_leq(cm, cl);
+          }
+          if (!kill) keep |= 1u << l;
+        }
+        uint32_t ns = 0;
+        for (uint32_t l = 0; l < combos; l++)
+          if (keep & (1u << l)) SCR(ns++) = SCR(TK + l);
+        s = ns;
+      }
+      for (uint32_t q = 0; q < s; q++) SCR(TK + q) = cd.to_p(SCR(q));
+      n = s;
+    }
+    edges += d;
+    bytes += 12ull + 16ull * d + 4ull * tot;
+  }
+  // EnergyArray PartialEq (energy.rs:334-350) against the old list
+  bool changed = n != cv;
+  for (uint32_t i = 0; i < n && !changed; i++) {
+    const uint32_t x = SCR(TK + i);
+    bool found = false;
+    for (uint32_t j = 0; j < cv && !found; j++) found = lelem(dv, j, arena, cap, c, p.ib, p.ibm) == x;
+    changed = !found;
+  }
+  if (!changed) return T_UNCHANGED;
+  out_cnt = n;
+  return T_CHANGED;
+}
+
+// Append predecessors to the next frontier once.  The reverse-CSR ranges of
+// all flagged lanes are concatenated and walked 32 entries at a time, so a
+// position with many predecessors is spread over the whole warp.
+__device__ void push_preds_warp(const KParams &p, Ctr *c, uint32_t *sm, uint32_t v, bool flagged, uint32_t *NF,
+                                uint32_t *nf_size, uint32_t stamp, uint32_t lane) {
+  uint32_t b = 0, n = 0;
+  if (flagged) {
+    b = ld(p.rrow, v, p.n_nodes + 1, c);
+    n = ld(p.rrow, (unsigned long long)v + 1, p.n_nodes + 1, c) - b;
+  }
+  const uint32_t incl = warp_incl_scan(n, lane);
+  const uint32_t total = __shfl_sync(FULL, incl, 31);
+  if (total == 0u) return;
+  sm[SM_PINC + lane] = incl;
+  sm[SM_PBEG + lane] = b;
+  __syncwarp();
+  for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
+    const uint32_t t = t0 + lane;
     bool first = false;
     uint32_t u = 0;
-    if (k < e) {
+    if (t < total) {
+      // owner lane: the first whose inclusive end exceeds t
+      uint32_t lo = 0, hi = 31;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (sm[SM_PINC + mid] > t) hi = mid; else lo = mid + 1;
+      }
+      const uint32_t start = lo ? sm[SM_PINC + lo - 1] : 0u;
+      const unsigned long long k = (unsigned long long)sm[SM_PBEG + lo] + (t - start);
       u = ld(p.rcol, k, p.n_edges, c);
       if (CHECK_IDX(c, u, p.n_nodes)) first = atomicMax(&p.mark[u], stamp) < stamp;
     }
@@ -798,16 +991,28 @@ __device__ void push_preds(const KParams &p, Ctr *c, uint32_t v, uint32_t *NF, u
       if (lane == 0) base = atomicAdd(nf_size, (uint32_t)__popc(bal));
       base = __shfl_sync(FULL, base, 0);
       if (first) {
-        uint32_t slot = base + __popc(bal & lanemask_lt());
+        const uint32_t slot = base + __popc(bal & lanemask_lt());
         if (CHECK_IDX(c, slot, p.n_nodes)) NF[slot] = u;
       }
     }
   }
+  __syncwarp();
 }
 
-template <class Cd>
-__global__ void __launch_bounds__(BLOCK) k_round(KParams p) {
+__device__ __forceinline__ void requeue(const KParams &p, Ctr *c, uint32_t v, uint32_t *NF, uint32_t *nf_size,
+                                        uint32_t stamp) {
+  if (atomicMax(&p.mark[v], stamp) < stamp) {
+    const uint32_t s = atomicAdd(nf_size, 1u);
+    if (CHECK_IDX(c, s, p.n_nodes)) NF[s] = v;
+  }
+}
+
+// MINB = resident blocks per SM the register allocation is sized for (2, 3
+// or 4); the autotuner picks the variant (geq_tuning.blocks_per_sm).
+template <class Cd, int MINB>
+__global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
   __shared__ uint32_t smem[WARPS_PER_BLOCK * SM_WORDS];
+  __shared__ uint32_t tscr[WARPS_PER_BLOCK * TSCR * 32];
   Ctr *c = p.ctr;
   if (c->halt) return;
   const uint32_t cur = c->cur;
@@ -819,38 +1024,79 @@ __global__ void __launch_bounds__(BLOCK) k_round(KParams p) {
   const uint32_t stamp = c->stamp + 1u;
   const uint32_t lane = threadIdx.x & 31u;
   uint32_t *sm = smem + (threadIdx.x >> 5) * SM_WORDS;
+  uint32_t *scr = tscr + (threadIdx.x >> 5) * (TSCR * 32) + lane;
   const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-  Cd cd = make_codec<Cd>(p);
+  const Cd cd = make_codec<Cd>(p);
+  uint32_t *arena = c->arena;
+  const unsigned long long cap = c->arena_cap;
   WarpAlloc wa{0, 0};
-  unsigned long long edges = 0, bytes = 0, positions = 0;
-  WarpCtx x{p, c, c->arena, c->arena_cap, lane, sm, wa, edges, bytes};
-  for (uint32_t slot = gw; slot < fs; slot += nw) {
-    const uint32_t v = ld(F, slot, p.n_nodes, c);
-    Res r = solve_position(x, cd, v);
-    if (r.st != R_SKIPPED) positions++;
-    if (lane == 0 && CHECK_IDX(c, slot, p.n_nodes))
-      p.slot_new[slot] = (r.st == R_CHANGED) ? mkdesc(r.off, r.cnt) : NONE_DESC;
-    if (r.st == R_CHANGED) {
-      if (r.cnt > CNT_MASK && lane == 0) { atomicOr(&c->error, DERR_LIST); atomicExch(&c->halt, 1u); }
-      push_preds(p, c, v, NF, nf_size, stamp, lane);
-    } else if (r.st == R_OVERFLOW) {
-      // retry next round after the arena has been compacted
-      if (lane == 0 && atomicMax(&p.mark[v], stamp) < stamp) {
-        uint32_t s = atomicAdd(nf_size, 1u);
-        if (CHECK_IDX(c, s, p.n_nodes)) NF[s] = v;
+  unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0;  // warp routines (lane-uniform)
+  unsigned long long t_edges = 0, t_bytes = 0, t_pos = 0;  // thread path (per lane)
+  WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes};
+  for (uint32_t base = gw * 32u; base < fs; base += nw * 32u) {
+    const uint32_t slot = base + lane;
+    const bool active = slot < fs;
+    const uint32_t v = active ? ld(F, slot, p.n_nodes, c) : 0u;
+    int ts = T_NONE;
+    uint32_t cnt = 0;
+    if (active) ts = p.thread_path ? thread_solve(p, c, cd, arena, cap, v, scr, cnt, t_edges, t_bytes) : T_BIG;
+    if (ts != T_NONE && ts != T_BIG && ts != T_SKIPPED) t_pos++;
+    // inline results need no arena; one reservation for the others
+    unsigned long long nd = NONE_DESC;
+    if (ts == T_CHANGED && cnt <= p.inl) {
+      nd = inl_hdr(cnt);
+      for (uint32_t q = 0; q < cnt; q++) nd |= (unsigned long long)SCR(TK + q) << (q * p.ib);
+    }
+    const uint32_t need = (ts == T_CHANGED && cnt > p.inl) ? cnt : 0u;
+    const uint32_t incl = warp_incl_scan(need, lane);
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    unsigned long long obase = 0;
+    const bool ok = total == 0u || wa.alloc(total, c, cap, lane, obase);
+    if (need) {
+      if (!ok) {
+        ts = T_OVERFLOW;
+      } else {
+        const unsigned long long off = obase + incl - need;
+        for (uint32_t q = 0; q < need; q++)
+          if (CHECK_IDX(c, off + q, cap)) arena[off + q] = SCR(TK + q);
+        nd = mkdesc(off, need);
       }
     }
+    if (ts == T_CHANGED) t_bytes += 4ull * cnt;
+    if (active && ts != T_BIG && CHECK_IDX(c, slot, p.n_nodes)) p.slot_new[slot] = (ts == T_CHANGED) ? nd : NONE_DESC;
+    // large positions: the whole warp on one position at a time
+    uint32_t big = __ballot_sync(FULL, ts == T_BIG);
+    bool big_changed = false;
+    while (big) {
+      const uint32_t l = __ffs(big) - 1u;
+      big &= big - 1u;
+      const uint32_t vb = __shfl_sync(FULL, v, l);
+      const Res r = solve_position(x, cd, vb);
+      if (r.st != R_SKIPPED) w_pos++;
+      if (lane == 0 && CHECK_IDX(c, base + l, p.n_nodes))
+        p.slot_new[base + l] = (r.st == R_CHANGED) ? r.d : NONE_DESC;
+      if (lane == l) big_changed = r.st == R_CHANGED;
+      if (r.st == R_OVERFLOW && lane == 0) requeue(p, c, vb, NF, nf_size, stamp);  // retried after compaction
+    }
+    push_preds_warp(p, c, sm, v, ts == T_CHANGED || big_changed, NF, nf_size, stamp, lane);
+    if (ts == T_OVERFLOW) requeue(p, c, v, NF, nf_size, stamp);
   }
-  if (lane == 0 && positions) {
-    atomicAdd(&c->positions, positions);
-    atomicAdd(&c->edges, edges);
-    atomicAdd(&c->bytes, bytes);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    t_edges += __shfl_xor_sync(FULL, t_edges, o);
+    t_bytes += __shfl_xor_sync(FULL, t_bytes, o);
+    t_pos += __shfl_xor_sync(FULL, t_pos, o);
+  }
+  if (lane == 0 && (t_pos || w_pos)) {
+    atomicAdd(&c->positions, t_pos + w_pos);
+    atomicAdd(&c->edges, t_edges + w_edges);
+    atomicAdd(&c->bytes, t_bytes + w_bytes);
   }
 }
 
 // Publish the round's new descriptors and advance to the next frontier.
-__global__ void k_commit(KParams p) {
+__global__ void k_commit(const KParams p) {
   Ctr *c = p.ctr;
   // k_round only raises `overflow` (never `halt`) for arena exhaustion, so
   // the round that overflowed still commits its finished positions; the
@@ -1035,23 +1281,42 @@ __global__ void k_fix_cols(uint32_t *col, unsigned long long m, const unsigned l
   }
 }
 
-__global__ void k_init_reach(unsigned long long *desc, const uint32_t *reach, unsigned long long n_reach,
-                             unsigned long long zero_off) {
+// TryFrom checks on the device: every update code names an element and the
+// padding bits above the last element are clear (pack_upd, energy.rs:543-565).
+__global__ void k_check_weights(const uint32_t *wt, unsigned long long m, uint32_t elements, uint32_t ubits,
+                                uint32_t umask, uint32_t *err) {
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < m;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t u = wt[k];
+    bool bad = elements * ubits < 32u && (u >> (elements * ubits)) != 0u;
+    for (uint32_t i = 0; i < elements; i++)
+      if (((u >> (i * ubits)) & umask) > elements + 1u) bad = true;
+    if (bad) atomicOr(err, 2u);
+  }
+}
+
+// EnergyGame::with_reach (energygame.rs:355-365): {0} at every target.
+__global__ void k_init_reach(unsigned long long *desc, const uint32_t *reach, unsigned long long n_reach) {
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_reach;
        i += (unsigned long long)gridDim.x * blockDim.x)
-    desc[reach[i]] = mkdesc(zero_off, 1u);
+    desc[reach[i]] = inl_hdr(1u);  // one energy, all elements 0
 }
 
 // initialize_visit_lists (energygame.rs:1461-1465): predecessors of to_reach.
-__global__ void k_init_frontier(KParams p, const uint32_t *reach, unsigned long long n_reach) {
+__global__ void k_init_frontier(const KParams p, const uint32_t *reach, unsigned long long n_reach) {
+  __shared__ uint32_t smem[(256 / 32) * SM_WORDS];
   Ctr *c = p.ctr;
   const uint32_t lane = threadIdx.x & 31u;
+  uint32_t *sm = smem + (threadIdx.x >> 5) * SM_WORDS;
   const unsigned long long gw = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
-  for (unsigned long long i = gw; i < n_reach; i += nw)
-    push_preds(p, c, reach[i], p.front0, &c->fsize[0], c->stamp, lane);
+  for (unsigned long long i0 = gw * 32ull; i0 < n_reach; i0 += nw * 32ull) {
+    const unsigned long long i = i0 + lane;
+    push_preds_warp(p, c, sm, i < n_reach ? reach[i] : 0u, i < n_reach, p.front0, &c->fsize[0], c->stamp, lane);
+  }
 }
 
+// Arena compaction: live arena lists move to `dst`; inline lists stay.
 __global__ void k_compact(unsigned long long *desc, unsigned long long n, const unsigned long long *noff,
                           const uint32_t *src, uint32_t *dst) {
   const uint32_t lane = threadIdx.x & 31u;
@@ -1059,6 +1324,7 @@ __global__ void k_compact(unsigned long long *desc, unsigned long long n, const 
   const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   for (unsigned long long v = gw; v < n; v += nw) {
     const unsigned long long d = desc[v];
+    if (dinl(d)) continue;
     const uint32_t c = dcnt(d);
     const unsigned long long o = doff(d), no = noff[v];
     for (uint32_t q = lane; q < c; q += 32u) dst[no + q] = src[o + q];
@@ -1066,16 +1332,26 @@ __global__ void k_compact(unsigned long long *desc, unsigned long long n, const 
   }
 }
 
+// Arena words held by arena (non-inline) lists.
+__global__ void k_arena_counts(const unsigned long long *desc, unsigned long long n, uint32_t *cnt) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n;
+       v += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long d = desc[v];
+    cnt[v] = dinl(d) ? 0u : dcnt(d);
+  }
+}
+
 __global__ void k_gather(const unsigned long long *desc, unsigned long long n, const unsigned long long *goff,
-                         const uint32_t *arena, uint32_t *out) {
+                         const uint32_t *arena, uint32_t ib, uint32_t ibm, uint32_t *out) {
   const uint32_t lane = threadIdx.x & 31u;
   const unsigned long long gw = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   for (unsigned long long v = gw; v < n; v += nw) {
     const unsigned long long d = desc[v];
     const uint32_t c = dcnt(d);
-    const unsigned long long o = doff(d), go = goff[v];
-    for (uint32_t q = lane; q < c; q += 32u) out[go + q] = arena[o + q];
+    const unsigned long long go = goff[v];
+    for (uint32_t q = lane; q < c; q += 32u)
+      out[go + q] = dinl(d) ? ((uint32_t)(d >> (q * ib)) & ibm) : arena[doff(d) + q];
   }
 }
 
@@ -1103,15 +1379,17 @@ __global__ void k_sel_counts(const unsigned long long *desc, const uint32_t *sel
     cnt[i] = dcnt(desc[sel[i]]);
 }
 __global__ void k_sel_gather(const unsigned long long *desc, const uint32_t *sel, unsigned long long k,
-                             const unsigned long long *goff, const uint32_t *arena, uint32_t *out) {
+                             const unsigned long long *goff, const uint32_t *arena, uint32_t ib, uint32_t ibm,
+                             uint32_t *out) {
   const uint32_t lane = threadIdx.x & 31u;
   const unsigned long long gw = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   for (unsigned long long i = gw; i < k; i += nw) {
     const unsigned long long d = desc[sel[i]];
     const uint32_t c = dcnt(d);
-    const unsigned long long o = doff(d), go = goff[i];
-    for (uint32_t q = lane; q < c; q += 32u) out[go + q] = arena[o + q];
+    const unsigned long long go = goff[i];
+    for (uint32_t q = lane; q < c; q += 32u)
+      out[go + q] = dinl(d) ? ((uint32_t)(d >> (q * ib)) & ibm) : arena[doff(d) + q];
   }
 }
 
@@ -1134,36 +1412,88 @@ __global__ void k_set_arena(Ctr *c, uint32_t *arena, unsigned long long cap, uns
                   "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));        \
   } while (0)
 
-template <class T>
-static geq_status dalloc(T *&p, size_t n) {
-  p = nullptr;
-  if (n == 0) n = 1;
-  CU(cudaMalloc((void **)&p, n * sizeof(T)));
-  return GEQ_OK;
-}
-template <class T>
-static void dfree(T *&p) {
-  if (p) cudaFree(p);
-  p = nullptr;
-}
+// Device memory cache.  Solving one small game per call (the plain drop-in)
+// would otherwise pay a cudaMalloc/cudaFree pair per buffer and call; cached
+// blocks are reused by later uploads.
+class DevPool {
+ public:
+  static size_t round_size(size_t b) {
+    b = std::max<size_t>(b, 512);
+    if (b <= (8u << 20)) {
+      size_t r = 512;
+      while (r < b) r <<= 1;
+      return r;
+    }
+    return (b + (8u << 20) - 1) & ~size_t((8u << 20) - 1);
+  }
+  void *get(size_t bytes) {
+    const size_t r = round_size(bytes);
+    auto it = free_.find(r);
+    if (it != free_.end() && !it->second.empty()) {
+      void *p = it->second.back();
+      it->second.pop_back();
+      cached_ -= r;
+      return p;
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, r) != cudaSuccess) {
+      cudaGetLastError();
+      trim();
+      if (cudaMalloc(&p, r) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+      }
+    }
+    return p;
+  }
+  void put(void *p, size_t bytes) {
+    if (!p) return;
+    const size_t r = round_size(bytes);
+    if (cached_ + r > limit_) {
+      cudaFree(p);
+      return;
+    }
+    free_[r].push_back(p);
+    cached_ += r;
+  }
+  void trim() {
+    for (auto &kv : free_)
+      for (void *p : kv.second) cudaFree(p);
+    free_.clear();
+    cached_ = 0;
+  }
+  ~DevPool() { trim(); }
+
+ private:
+  std::map<size_t, std::vector<void *>> free_;
+  size_t cached_ = 0;
+  size_t limit_ = (size_t)16 << 30;
+};
 
 struct Engine::State {
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  Ctr *h_ctr = nullptr;  // pinned
-  // scan scratch
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, eva = nullptr, evb = nullptr;
+  Ctr *h_ctr = nullptr;     // pinned
+  // one captured graph of rounds per codec [CodecStd, CodecGen], shared by all
+  // uploads; its kernel nodes get the parameters of the games being solved
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  std::vector<cudaGraphNode_t> gnodes[2];
+  uint32_t g_rounds[2] = {0, 0}, g_bps[2] = {0, 0};
   unsigned long long *part = nullptr;
   size_t part_cap = 0;
   uint32_t *cnt = nullptr;
   size_t cnt_cap = 0;
-  // pinned staging
   char *stage = nullptr;
   size_t stage_cap = 0;
   uint32_t *d_err = nullptr;
-  int grid_blocks = 0;
+  DevPool pool;
+  std::set<DeviceGamesImpl *> live;
 };
 
 struct DeviceGamesImpl {
+  Engine::State *owner = nullptr;  // pool the buffers return to
+  std::vector<std::pair<void *, size_t>> bufs;
   Conf conf;
   bool generic = false;
   uint32_t n_games = 0;
@@ -1183,10 +1513,58 @@ struct DeviceGamesImpl {
   unsigned long long *d_node_base = nullptr;
   Ctr *ctr = nullptr;
   uint32_t next_stamp = 1;
-  cudaGraphExec_t gexec = nullptr;
-  uint32_t graph_rounds = 0;
   KParams kp{};
+
+  template <class T>
+  bool alloc(T *&p, size_t n) {
+    const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+    p = (T *)(owner ? owner->pool.get(bytes) : nullptr);
+    if (!p) return false;
+    bufs.emplace_back((void *)p, bytes);
+    return true;
+  }
+  template <class T>
+  void release(T *&p) {
+    for (size_t i = 0; i < bufs.size(); i++)
+      if (bufs[i].first == (void *)p) {
+        if (owner) owner->pool.put(p, bufs[i].second);
+        else cudaFree(p);
+        bufs.erase(bufs.begin() + i);
+        break;
+      }
+    p = nullptr;
+  }
+  void release_all() {
+    for (auto &b : bufs) {
+      if (owner) owner->pool.put(b.first, b.second);
+      else cudaFree(b.first);
+    }
+    bufs.clear();
+  }
 };
+
+void destroy_games(DeviceGamesImpl *p) {
+  if (!p) return;
+  if (p->owner) {
+    cudaStreamSynchronize(p->owner->stream);
+    p->owner->live.erase(p);
+  }
+  p->release_all();
+  delete p;
+}
+
+template <class T>
+static geq_status dalloc(T *&p, size_t n) {
+  p = nullptr;
+  if (n == 0) n = 1;
+  CU(cudaMalloc((void **)&p, n * sizeof(T)));
+  return GEQ_OK;
+}
+template <class T>
+static void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
 
 static geq_status scan_u32(Engine::State &s, const uint32_t *in, unsigned long long n, unsigned long long *out,
                            unsigned long long &launches) {
@@ -1228,6 +1606,40 @@ static geq_status ensure_stage(Engine::State &s, size_t bytes) {
   return GEQ_OK;
 }
 
+// memcpy jobs spread over host threads (large uploads only)
+struct CopyJob {
+  void *dst;
+  const void *src;
+  size_t bytes;
+};
+static void run_copies(std::vector<CopyJob> &jobs) {
+  size_t total = 0;
+  for (auto &j : jobs) total += j.bytes;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned T = total < (8u << 20) ? 1u : std::min(16u, hw);
+  if (T == 1) {
+    for (auto &j : jobs)
+      if (j.bytes) std::memcpy(j.dst, j.src, j.bytes);
+    return;
+  }
+  std::vector<CopyJob> split;
+  const size_t piece = 4u << 20;
+  for (auto &j : jobs)
+    for (size_t o = 0; o < j.bytes; o += piece)
+      split.push_back(CopyJob{(char *)j.dst + o, (const char *)j.src + o, std::min(piece, j.bytes - o)});
+  std::atomic<size_t> next{0};
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < T; t++)
+    pool.emplace_back([&]() {
+      for (;;) {
+        size_t i = next.fetch_add(1);
+        if (i >= split.size()) break;
+        std::memcpy(split[i].dst, split[i].src, split[i].bytes);
+      }
+    });
+  for (auto &th : pool) th.join();
+}
+
 geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
@@ -1246,11 +1658,13 @@ geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
   CU(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
   CU(cudaEventCreate(&s.ev0));
   CU(cudaEventCreate(&s.ev1));
+  CU(cudaEventCreate(&s.eva));
+  CU(cudaEventCreate(&s.evb));
   CU(cudaHostAlloc((void **)&s.h_ctr, sizeof(Ctr), cudaHostAllocDefault));
   CU(cudaMalloc((void **)&s.d_err, sizeof(uint32_t)));
   int bps = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_round<CodecStd>, BLOCK, 0));
-  eng->tuning.blocks_per_sm = (uint32_t)std::max(1, std::min(bps, 8));
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_round<CodecStd, 3>, BLOCK, 0));
+  eng->tuning.blocks_per_sm = (uint32_t)std::max(2, std::min(bps, 3));
   eng->tuning.rounds_per_graph = 8;
   eng->tuning.small_limit = 32;
   out = std::move(eng);
@@ -1261,37 +1675,38 @@ Engine::~Engine() {
   if (!st) return;
   State &s = *st;
   if (s.stream) cudaStreamSynchronize(s.stream);
+  // games still alive keep their memory but lose the pool
+  for (DeviceGamesImpl *g : s.live) {
+    g->release_all();
+    g->owner = nullptr;
+  }
+  s.live.clear();
+  for (auto &g : s.gexec)
+    if (g) cudaGraphExecDestroy(g);
+  for (auto &g : s.graph)
+    if (g) cudaGraphDestroy(g);
   dfree(s.part);
   dfree(s.cnt);
   dfree(s.d_err);
+  s.pool.trim();
   if (s.stage) cudaFreeHost(s.stage);
   if (s.h_ctr) cudaFreeHost(s.h_ctr);
   if (s.ev0) cudaEventDestroy(s.ev0);
   if (s.ev1) cudaEventDestroy(s.ev1);
+  if (s.eva) cudaEventDestroy(s.eva);
+  if (s.evb) cudaEventDestroy(s.evb);
   if (s.stream) cudaStreamDestroy(s.stream);
 }
 
-static void free_games(DeviceGamesImpl &dg) {
-  // cudaFree synchronises with outstanding work on the device
-  if (dg.gexec) cudaGraphExecDestroy(dg.gexec);
-  dg.gexec = nullptr;
-  dfree(dg.row); dfree(dg.col); dfree(dg.wt); dfree(dg.rrow); dfree(dg.rcol); dfree(dg.flags);
-  dfree(dg.desc); dfree(dg.desc_init); dfree(dg.slot_new); dfree(dg.mark); dfree(dg.front0);
-  dfree(dg.front1); dfree(dg.init_data); dfree(dg.arena[0]); dfree(dg.arena[1]); dfree(dg.reach);
-  dfree(dg.d_node_base); dfree(dg.ctr);
-}
-
-void destroy_games(DeviceGamesImpl *p) {
-  if (!p) return;
-  free_games(*p);
-  delete p;
-}
+uint64_t Engine::game_node_base(const DeviceGamesImpl &dg, uint32_t g) { return dg.node_base[g]; }
 
 // Pack the games into pinned staging and move them to the device.
 geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   State &s = *st;
   if (games.empty()) return fail(GEQ_ERR_INVALID_INPUT, "no games");
   GamesPtr dg(new DeviceGamesImpl());
+  dg->owner = &s;
+  s.live.insert(dg.get());
   dg->conf = Conf(games[0].g.conf);
   if (!dg->conf.supported())
     return fail(GEQ_ERR_UNSUPPORTED, "EnergyConf {%u, %u} is outside the device codecs", dg->conf.elements,
@@ -1308,7 +1723,6 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
     dg->node_base[g + 1] = dg->node_base[g] + gi.g.n_vertices;
     dg->edge_base[g + 1] = dg->edge_base[g] + gi.g.row_offsets[gi.g.n_vertices];
     if (gi.init) { any_init = true; init_total += gi.init->offsets[gi.init->n_vertices]; }
-    else init_total += 0;
     n_reach += gi.n_reach;
   }
   dg->N = dg->node_base.back();
@@ -1337,23 +1751,25 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   unsigned long long *h_nb = (unsigned long long *)(H + off_base);
   unsigned long long *h_eb = h_nb + (dg->n_games + 1);
   unsigned long long *h_gn = h_eb + (dg->n_games + 1);
+  std::vector<CopyJob> copies;
+  copies.reserve(4 * (size_t)dg->n_games);
   unsigned long long ri = 0, ii = 1;
   h_init[0] = 0;  // the zero energy of standard initialisation
   for (uint32_t g = 0; g < dg->n_games; g++) {
     const GameInput &gi = games[g];
     const uint32_t n = gi.g.n_vertices;
     const unsigned long long nb = dg->node_base[g], eb = dg->edge_base[g], m = dg->edge_base[g + 1] - eb;
-    std::memcpy(h_row + nb, gi.g.row_offsets, (size_t)n * 4);
+    copies.push_back(CopyJob{h_row + nb, gi.g.row_offsets, (size_t)n * 4});
     if (m) {
-      std::memcpy(h_col + eb, gi.g.column_indices, (size_t)m * 4);
-      std::memcpy(h_wt + eb, gi.g.weights, (size_t)m * 4);
+      copies.push_back(CopyJob{h_col + eb, gi.g.column_indices, (size_t)m * 4});
+      copies.push_back(CopyJob{h_wt + eb, gi.g.weights, (size_t)m * 4});
     }
-    std::memcpy(h_flags + nb, gi.g.attacker_pos, n);
+    copies.push_back(CopyJob{h_flags + nb, gi.g.attacker_pos, n});
     for (uint32_t i = 0; i < gi.n_reach; i++) h_reach[ri++] = gi.to_reach[i] + (uint32_t)nb;
     if (any_init) {
       if (gi.init) {
         const unsigned long long t = gi.init->offsets[n];
-        std::memcpy(h_init + ii, gi.init->data, (size_t)t * 4);
+        copies.push_back(CopyJob{h_init + ii, gi.init->data, (size_t)t * 4});
         for (uint32_t v = 0; v < n; v++) {
           unsigned long long o = gi.init->offsets[v], c = gi.init->offsets[v + 1] - o;
           h_desc[nb + v] = ((ii + o) << 24) | c;
@@ -1368,91 +1784,82 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
     h_eb[g] = eb;
     h_gn[g] = n;
   }
+  run_copies(copies);
   h_row[N] = (uint32_t)M;
   h_nb[dg->n_games] = N;
   h_eb[dg->n_games] = M;
   h_gn[dg->n_games] = 0;
 
-  // device allocations
-  geq_status a = GEQ_OK;
-  if ((a = dalloc(dg->row, N + 1)) || (a = dalloc(dg->col, M)) || (a = dalloc(dg->wt, M)) ||
-      (a = dalloc(dg->rrow, N + 1)) || (a = dalloc(dg->rcol, M)) || (a = dalloc(dg->flags, N)) ||
-      (a = dalloc(dg->desc, N)) || (a = dalloc(dg->desc_init, N)) || (a = dalloc(dg->slot_new, N)) ||
-      (a = dalloc(dg->mark, N)) || (a = dalloc(dg->front0, N)) || (a = dalloc(dg->front1, N)) ||
-      (a = dalloc(dg->init_data, dg->init_total)) || (a = dalloc(dg->reach, n_reach)) ||
-      (a = dalloc(dg->d_node_base, 3 * (dg->n_games + 1))) || (a = dalloc(dg->ctr, 1))) {
-    free_games(*dg);
-    return a;
-  }
-  unsigned long long cap = std::max<unsigned long long>(4ull * (dg->init_total + N) + (1ull << 20), 1ull << 22);
-  if ((a = dalloc(dg->arena[0], cap))) { free_games(*dg); return a; }
-  dg->arena_cap[0] = cap;
+  // device allocations (pooled)
+  DeviceGamesImpl &D = *dg;
+  if (!D.alloc(D.row, N + 1) || !D.alloc(D.col, M) || !D.alloc(D.wt, M) || !D.alloc(D.rrow, N + 1) ||
+      !D.alloc(D.rcol, M) || !D.alloc(D.flags, N) || !D.alloc(D.desc, N) || !D.alloc(D.desc_init, N) ||
+      !D.alloc(D.slot_new, N) || !D.alloc(D.mark, N) || !D.alloc(D.front0, N) || !D.alloc(D.front1, N) ||
+      !D.alloc(D.init_data, D.init_total) || !D.alloc(D.reach, n_reach) ||
+      !D.alloc(D.d_node_base, 3 * (D.n_games + 1)) || !D.alloc(D.ctr, 1))
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
+  unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
+  if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
+  D.arena_cap[0] = DevPool::round_size(cap * 4) / 4;
   cudaStream_t S = s.stream;
-#define CUF(call)                        \
-  do {                                   \
-    cudaError_t e_ = (call);             \
-    if (e_ != cudaSuccess) {             \
-      free_games(*dg);                   \
-      return fail(GEQ_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-    }                                    \
-  } while (0)
-  CUF(cudaMemcpyAsync(dg->row, h_row, (N + 1) * 4, cudaMemcpyHostToDevice, S));
+  CU(cudaMemcpyAsync(D.row, h_row, (N + 1) * 4, cudaMemcpyHostToDevice, S));
   if (M) {
-    CUF(cudaMemcpyAsync(dg->col, h_col, M * 4, cudaMemcpyHostToDevice, S));
-    CUF(cudaMemcpyAsync(dg->wt, h_wt, M * 4, cudaMemcpyHostToDevice, S));
+    CU(cudaMemcpyAsync(D.col, h_col, M * 4, cudaMemcpyHostToDevice, S));
+    CU(cudaMemcpyAsync(D.wt, h_wt, M * 4, cudaMemcpyHostToDevice, S));
   }
-  if (N) CUF(cudaMemcpyAsync(dg->flags, h_flags, N, cudaMemcpyHostToDevice, S));
-  if (n_reach) CUF(cudaMemcpyAsync(dg->reach, h_reach, n_reach * 4, cudaMemcpyHostToDevice, S));
-  CUF(cudaMemcpyAsync(dg->init_data, h_init, dg->init_total * 4, cudaMemcpyHostToDevice, S));
-  CUF(cudaMemcpyAsync(dg->d_node_base, h_nb, 3 * (dg->n_games + 1) * 8, cudaMemcpyHostToDevice, S));
+  if (N) CU(cudaMemcpyAsync(D.flags, h_flags, N, cudaMemcpyHostToDevice, S));
+  if (n_reach) CU(cudaMemcpyAsync(D.reach, h_reach, n_reach * 4, cudaMemcpyHostToDevice, S));
+  CU(cudaMemcpyAsync(D.init_data, h_init, D.init_total * 4, cudaMemcpyHostToDevice, S));
+  CU(cudaMemcpyAsync(D.d_node_base, h_nb, 3 * (D.n_games + 1) * 8, cudaMemcpyHostToDevice, S));
   if (any_init) {
-    if (N) CUF(cudaMemcpyAsync(dg->desc_init, h_desc, N * 8, cudaMemcpyHostToDevice, S));
+    if (N) CU(cudaMemcpyAsync(D.desc_init, h_desc, N * 8, cudaMemcpyHostToDevice, S));
   } else {
-    if (N) CUF(cudaMemsetAsync(dg->desc_init, 0, N * 8, S));
-    if (n_reach) k_init_reach<<<std::min<unsigned long long>((n_reach + 255) / 256, 4096), 256, 0, S>>>(dg->desc_init, dg->reach, n_reach, 0ull);
+    if (N) CU(cudaMemsetAsync(D.desc_init, 0, N * 8, S));
+    if (n_reach)
+      k_init_reach<<<(unsigned)std::min<unsigned long long>((n_reach + 255) / 256, 4096), 256, 0, S>>>(
+          D.desc_init, D.reach, n_reach);
   }
-  if (N) CUF(cudaMemsetAsync(dg->mark, 0, N * 4, S));
-  CUF(cudaMemsetAsync(s.d_err, 0, 4, S));
+  if (N) CU(cudaMemsetAsync(D.mark, 0, N * 4, S));
+  CU(cudaMemsetAsync(s.d_err, 0, 4, S));
   const unsigned grid = (unsigned)std::max(1, n_sms * 8);
-  if (dg->n_games > 1) {
-    k_fix_rows<<<grid, 256, 0, S>>>(dg->row, N, dg->d_node_base, dg->d_node_base + (dg->n_games + 1), dg->n_games);
-    k_fix_cols<<<grid, 256, 0, S>>>(dg->col, M, dg->d_node_base, dg->d_node_base + (dg->n_games + 1), dg->n_games,
-                                    dg->d_node_base + 2 * (dg->n_games + 1), s.d_err);
-  } else {
-    // single game: validate successor ids on the device as well
-    k_fix_cols<<<grid, 256, 0, S>>>(dg->col, M, dg->d_node_base, dg->d_node_base + (dg->n_games + 1), 1,
-                                    dg->d_node_base + 2 * (dg->n_games + 1), s.d_err);
-  }
+  if (D.n_games > 1)
+    k_fix_rows<<<grid, 256, 0, S>>>(D.row, N, D.d_node_base, D.d_node_base + (D.n_games + 1), D.n_games);
+  // successor ids into the global id space, checked against each game's size
+  k_fix_cols<<<grid, 256, 0, S>>>(D.col, M, D.d_node_base, D.d_node_base + (D.n_games + 1), D.n_games,
+                                  D.d_node_base + 2 * (D.n_games + 1), s.d_err);
+  k_check_weights<<<grid, 256, 0, S>>>(D.wt, M, D.conf.elements, D.conf.update_bits(), D.conf.update_mask(),
+                                       s.d_err);
   // reverse CSR
   geq_status es = ensure_cnt(s, N + 1);
-  if (es) { free_games(*dg); return es; }
-  CUF(cudaMemsetAsync(s.cnt, 0, (N + 1) * 4, S));
-  k_indegree<<<grid, 256, 0, S>>>(dg->col, M, N, s.cnt, s.d_err);
-  unsigned long long *roff = nullptr;
-  if ((a = dalloc(roff, N + 1))) { free_games(*dg); return a; }
+  if (es) return es;
+  CU(cudaMemsetAsync(s.cnt, 0, (N + 1) * 4, S));
+  k_indegree<<<grid, 256, 0, S>>>(D.col, M, N, s.cnt, s.d_err);
+  unsigned long long *roff = (unsigned long long *)s.pool.get((N + 1) * 8);
+  if (!roff) return fail(GEQ_ERR_OUT_OF_MEMORY, "reverse offsets");
   unsigned long long launches = 0;
-  if ((a = scan_u32(s, s.cnt, N, roff, launches))) { cudaFree(roff); free_games(*dg); return a; }
-  k_u64_to_u32<<<grid, 256, 0, S>>>(roff, N + 1, dg->rrow);
-  CUF(cudaMemcpyAsync(s.cnt, dg->rrow, N * 4, cudaMemcpyDeviceToDevice, S));
-  k_fill_reverse<<<grid, 256, 0, S>>>(dg->row, dg->col, N, s.cnt, dg->rcol);
-  uint32_t h_err = 0;
-  CUF(cudaMemcpyAsync(&s.h_ctr->pad, s.d_err, 4, cudaMemcpyDeviceToHost, S));
-  CUF(cudaStreamSynchronize(S));
-  h_err = s.h_ctr->pad;
-  cudaFree(roff);
-  CUF(cudaGetLastError());
-  if (h_err) {
-    free_games(*dg);
-    return fail(GEQ_ERR_INVALID_INPUT, "a successor index is out of range");
-  }
-#undef CUF
-  KParams &kp = dg->kp;
-  kp.row = dg->row; kp.col = dg->col; kp.wt = dg->wt; kp.rrow = dg->rrow; kp.rcol = dg->rcol;
-  kp.flags = dg->flags; kp.desc = dg->desc; kp.mark = dg->mark; kp.front0 = dg->front0; kp.front1 = dg->front1;
-  kp.slot_new = dg->slot_new; kp.ctr = dg->ctr; kp.n_nodes = N; kp.n_edges = M;
-  kp.el = dg->conf.elements; kp.mx = dg->conf.max; kp.eb = dg->conf.energy_bits(); kp.em = dg->conf.energy_mask();
-  kp.ub = dg->conf.update_bits(); kp.um = dg->conf.update_mask();
+  geq_status a = scan_u32(s, s.cnt, N, roff, launches);
+  if (a) { s.pool.put(roff, (N + 1) * 8); return a; }
+  k_u64_to_u32<<<grid, 256, 0, S>>>(roff, N + 1, D.rrow);
+  CU(cudaMemcpyAsync(s.cnt, D.rrow, N * 4, cudaMemcpyDeviceToDevice, S));
+  k_fill_reverse<<<grid, 256, 0, S>>>(D.row, D.col, N, s.cnt, D.rcol);
+  CU(cudaMemcpyAsync(&s.h_ctr->pad, s.d_err, 4, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  s.pool.put(roff, (N + 1) * 8);
+  CU(cudaGetLastError());
+  const uint32_t h_err = s.h_ctr->pad;
+  if (h_err & 1u) return fail(GEQ_ERR_INVALID_INPUT, "Node index too high: a successor index is out of range");
+  if (h_err & 2u) return fail(GEQ_ERR_INVALID_INPUT, "an edge update names no element or sets padding bits");
+  KParams &kp = D.kp;
+  kp.row = D.row; kp.col = D.col; kp.wt = D.wt; kp.rrow = D.rrow; kp.rcol = D.rcol;
+  kp.flags = D.flags; kp.desc = D.desc; kp.mark = D.mark; kp.front0 = D.front0; kp.front1 = D.front1;
+  kp.slot_new = D.slot_new; kp.ctr = D.ctr; kp.n_nodes = N; kp.n_edges = M;
+  kp.el = D.conf.elements; kp.mx = D.conf.max; kp.eb = D.conf.energy_bits(); kp.em = D.conf.energy_mask();
+  kp.ub = D.conf.update_bits(); kp.um = D.conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
+  kp.thread_path = (tuning.flags & (GEQ_TUNE_FORCE_LARGE | GEQ_TUNE_NO_THREAD_PATH)) ? 0u : 1u;
+  kp.ib = D.conf.elements * D.conf.energy_bits();
+  kp.ibm = kp.ib >= 32 ? 0xFFFFFFFFu : ((1u << kp.ib) - 1u);
+  kp.inl = std::min<uint32_t>(7u, 60u / kp.ib);
   out = std::move(dg);
   return GEQ_OK;
 }
@@ -1463,38 +1870,89 @@ static geq_status compact(Engine &E, DeviceGamesImpl &dg, unsigned long long &la
   const unsigned long long N = dg.N;
   geq_status a = ensure_cnt(s, N + 1);
   if (a) return a;
-  unsigned long long *noff = nullptr;
-  if ((a = dalloc(noff, N + 1))) return a;
+  unsigned long long *noff = (unsigned long long *)s.pool.get((N + 1) * 8);
+  if (!noff) return fail(GEQ_ERR_OUT_OF_MEMORY, "compaction offsets");
   const unsigned grid = (unsigned)std::max(1, E.n_sms * 8);
-  k_desc_counts<<<grid, 256, 0, S>>>(dg.desc, N, s.cnt);
+  k_arena_counts<<<grid, 256, 0, S>>>(dg.desc, N, s.cnt);
   launches++;
-  if ((a = scan_u32(s, s.cnt, N, noff, launches))) { cudaFree(noff); return a; }
+  if ((a = scan_u32(s, s.cnt, N, noff, launches))) { s.pool.put(noff, (N + 1) * 8); return a; }
   unsigned long long total = 0;
-  CU(cudaMemcpyAsync(&total, noff + N, 8, cudaMemcpyDeviceToHost, S));
+  CU(cudaMemcpyAsync(&s.h_ctr->positions, noff + N, 8, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
+  total = s.h_ctr->positions;
   const int alt = dg.arena_cur ^ 1;
   unsigned long long need = std::max<unsigned long long>(dg.arena_cap[dg.arena_cur], 4 * total + (1ull << 20));
   if (dg.arena_cap[alt] < need) {
-    dfree(dg.arena[alt]);
+    if (dg.arena[alt]) dg.release(dg.arena[alt]);
     dg.arena_cap[alt] = 0;
-    if ((a = dalloc(dg.arena[alt], need))) { cudaFree(noff); return a; }
-    dg.arena_cap[alt] = need;
+    if (!dg.alloc(dg.arena[alt], need)) { s.pool.put(noff, (N + 1) * 8); return fail(GEQ_ERR_OUT_OF_MEMORY, "arena"); }
+    dg.arena_cap[alt] = DevPool::round_size(need * 4) / 4;
   }
   k_compact<<<grid, 256, 0, S>>>(dg.desc, N, noff, dg.arena[dg.arena_cur], dg.arena[alt]);
   k_set_arena<<<1, 1, 0, S>>>(dg.ctr, dg.arena[alt], dg.arena_cap[alt], total);
   launches += 2;
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(S));
-  cudaFree(noff);
+  s.pool.put(noff, (N + 1) * 8);
   dg.arena_cur = alt;
   return GEQ_OK;
 }
 
 template <class Cd>
-static void launch_round(Engine &E, DeviceGamesImpl &dg, cudaStream_t S) {
-  const unsigned grid = (unsigned)std::max<uint32_t>(1, E.n_sms * E.tuning.blocks_per_sm);
-  k_round<Cd><<<grid, BLOCK, 0, S>>>(dg.kp);
-  k_commit<<<(unsigned)std::max(1, E.n_sms * 2), 256, 0, S>>>(dg.kp);
+static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent_t ea = nullptr,
+                         cudaEvent_t eb = nullptr) {
+  const uint32_t bps = std::min<uint32_t>(std::max<uint32_t>(E.tuning.blocks_per_sm, 2), 4);
+  const unsigned grid = (unsigned)std::max<uint32_t>(1, E.n_sms * bps);
+  if (ea) cudaEventRecord(ea, S);
+  if (bps == 2) k_round<Cd, 2><<<grid, BLOCK, 0, S>>>(kp);
+  else if (bps == 3) k_round<Cd, 3><<<grid, BLOCK, 0, S>>>(kp);
+  else k_round<Cd, 4><<<grid, BLOCK, 0, S>>>(kp);
+  if (eb) cudaEventRecord(eb, S);
+  k_commit<<<(unsigned)std::max(1, E.n_sms * 2), 256, 0, S>>>(kp);
+}
+
+// One captured graph of R rounds per codec, shared by every upload: before a
+// solve its kernel nodes are pointed at the parameters of that upload.
+static geq_status round_graph(Engine &E, const KParams &kp, bool generic, uint32_t R, cudaGraphExec_t &out) {
+  Engine::State &s = *E.st;
+  const int k = generic ? 1 : 0;
+  if (!(s.gexec[k] && s.g_rounds[k] == R && s.g_bps[k] == E.tuning.blocks_per_sm)) {
+    if (s.gexec[k]) { cudaGraphExecDestroy(s.gexec[k]); s.gexec[k] = nullptr; }
+    if (s.graph[k]) { cudaGraphDestroy(s.graph[k]); s.graph[k] = nullptr; }
+    cudaStream_t cs;
+    CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+      for (uint32_t r = 0; r < R; r++) {
+        if (generic) launch_round<CodecGen>(E, kp, cs);
+        else launch_round<CodecStd>(E, kp, cs);
+      }
+      ce = cudaStreamEndCapture(cs, &s.graph[k]);
+    }
+    cudaStreamDestroy(cs);
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&s.gexec[k], s.graph[k], 0);
+    size_t n = 0;
+    if (ce == cudaSuccess) ce = cudaGraphGetNodes(s.graph[k], nullptr, &n);
+    s.gnodes[k].assign(n, nullptr);
+    if (ce == cudaSuccess && n) ce = cudaGraphGetNodes(s.graph[k], s.gnodes[k].data(), &n);
+    if (ce != cudaSuccess) return fail(GEQ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+    s.g_rounds[k] = R;
+    s.g_bps[k] = E.tuning.blocks_per_sm;
+  } else {
+    for (cudaGraphNode_t node : s.gnodes[k]) {
+      cudaGraphNodeType t;
+      CU(cudaGraphNodeGetType(node, &t));
+      if (t != cudaGraphNodeTypeKernel) continue;
+      cudaKernelNodeParams np;
+      CU(cudaGraphKernelNodeGetParams(node, &np));
+      void *args[1] = {(void *)&kp};
+      np.kernelParams = args;
+      np.extra = nullptr;
+      CU(cudaGraphExecKernelNodeSetParams(s.gexec[k], node, &np));
+    }
+  }
+  out = s.gexec[k];
+  return GEQ_OK;
 }
 
 geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
@@ -1518,33 +1976,21 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
   *s.h_ctr = h;
   CU(cudaMemcpyAsync(dg.ctr, s.h_ctr, sizeof(Ctr), cudaMemcpyHostToDevice, S));
   if (dg.n_reach) {
-    const unsigned grid = (unsigned)std::max<unsigned long long>(1, std::min<unsigned long long>((dg.n_reach + 7) / 8, (unsigned long long)n_sms * 16));
+    const unsigned grid = (unsigned)std::max<unsigned long long>(
+        1, std::min<unsigned long long>((dg.n_reach + 7) / 8, (unsigned long long)n_sms * 16));
     k_init_frontier<<<grid, 256, 0, S>>>(dg.kp, dg.reach, dg.n_reach);
     launches++;
   }
   CU(cudaGetLastError());
-  const bool use_graph = !(tuning.flags & GEQ_TUNE_NO_GRAPH);
+  const bool profile = (tuning.flags & GEQ_TUNE_PROFILE) != 0;
+  double round_ms = 0.0;
+  unsigned long long round_launches = 0;
+  const bool use_graph = !(tuning.flags & (GEQ_TUNE_NO_GRAPH | GEQ_TUNE_PROFILE));
   const uint32_t R = use_graph ? std::max<uint32_t>(1, tuning.rounds_per_graph) : 1;
-  if (use_graph && (!dg.gexec || dg.graph_rounds != R)) {
-    if (dg.gexec) { cudaGraphExecDestroy(dg.gexec); dg.gexec = nullptr; }
-    cudaStream_t cs;
-    CU(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    cudaGraph_t graph;
-    cudaError_t ce = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-    if (ce == cudaSuccess) {
-      for (uint32_t r = 0; r < R; r++) {
-        if (dg.generic) launch_round<CodecGen>(*this, dg, cs);
-        else launch_round<CodecStd>(*this, dg, cs);
-      }
-      ce = cudaStreamEndCapture(cs, &graph);
-    }
-    if (ce == cudaSuccess) {
-      ce = cudaGraphInstantiate(&dg.gexec, graph, 0);
-      cudaGraphDestroy(graph);
-    }
-    cudaStreamDestroy(cs);
-    if (ce != cudaSuccess) return fail(GEQ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
-    dg.graph_rounds = R;
+  cudaGraphExec_t gexec = nullptr;
+  if (use_graph) {
+    geq_status g = round_graph(*this, dg.kp, dg.generic, R, gexec);
+    if (g) return g;
   }
   // The device work of every launch is bounded; this bounds the host loop in
   // case the frontier never empties (GEQ_SOLVE_TIMEOUT_S seconds, default 600).
@@ -1553,15 +1999,22 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
   const auto t_start = std::chrono::steady_clock::now();
   for (unsigned long long iter = 0;; iter++) {
     if (use_graph) {
-      CU(cudaGraphLaunch(dg.gexec, S));
+      CU(cudaGraphLaunch(gexec, S));
     } else {
-      if (dg.generic) launch_round<CodecGen>(*this, dg, S);
-      else launch_round<CodecStd>(*this, dg, S);
+      cudaEvent_t ea = profile ? s.eva : nullptr, eb = profile ? s.evb : nullptr;
+      if (dg.generic) launch_round<CodecGen>(*this, dg.kp, S, ea, eb);
+      else launch_round<CodecStd>(*this, dg.kp, S, ea, eb);
     }
     launches += 2ull * R;
     CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
     CU(cudaStreamSynchronize(S));
     const Ctr c = *s.h_ctr;
+    if (profile) {
+      float ms = 0.f;
+      CU(cudaEventElapsedTime(&ms, s.eva, s.evb));
+      round_ms += ms;
+      round_launches++;
+    }
     if (c.error) {
       const char *what = (c.error & DERR_BOUNDS) ? "index out of range" :
                          (c.error & DERR_LIST) ? "energy list too long" : "combination too large";
@@ -1593,6 +2046,8 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
     stats->arena_compactions = compactions;
     stats->kernel_launches = launches;
     stats->device_ms = ms;
+    stats->round_kernel_ms = round_ms;
+    stats->round_kernel_launches = round_launches;
   }
   return GEQ_OK;
 }
@@ -1604,18 +2059,22 @@ geq_status Engine::download(DeviceGamesImpl &dg, geq_solution &sol) {
   unsigned long long launches = 0;
   geq_status a = ensure_cnt(s, N + 1);
   if (a) return a;
-  unsigned long long *goff = nullptr, *rel = nullptr;
-  uint32_t *out = nullptr;
-  if ((a = dalloc(goff, N + 1))) return a;
-  if ((a = dalloc(rel, N + dg.n_games))) { cudaFree(goff); return a; }
+  unsigned long long *goff = (unsigned long long *)s.pool.get((N + 1) * 8);
+  unsigned long long *rel = (unsigned long long *)s.pool.get((N + dg.n_games) * 8);
+  if (!goff || !rel) {
+    s.pool.put(goff, (N + 1) * 8);
+    s.pool.put(rel, (N + dg.n_games) * 8);
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "download offsets");
+  }
   const unsigned grid = (unsigned)std::max(1, n_sms * 8);
   k_desc_counts<<<grid, 256, 0, S>>>(dg.desc, N, s.cnt);
-  if ((a = scan_u32(s, s.cnt, N, goff, launches))) { cudaFree(goff); cudaFree(rel); return a; }
-  unsigned long long total = 0;
-  CU(cudaMemcpyAsync(&total, goff + N, 8, cudaMemcpyDeviceToHost, S));
+  if ((a = scan_u32(s, s.cnt, N, goff, launches))) return a;
+  CU(cudaMemcpyAsync(&s.h_ctr->positions, goff + N, 8, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
-  if ((a = dalloc(out, total))) { cudaFree(goff); cudaFree(rel); return a; }
-  k_gather<<<grid, 256, 0, S>>>(dg.desc, N, goff, dg.arena[dg.arena_cur], out);
+  const unsigned long long total = s.h_ctr->positions;
+  uint32_t *out = (uint32_t *)s.pool.get(std::max<unsigned long long>(total, 1) * 4);
+  if (!out) return fail(GEQ_ERR_OUT_OF_MEMORY, "download data");
+  k_gather<<<grid, 256, 0, S>>>(dg.desc, N, goff, dg.arena[dg.arena_cur], dg.kp.ib, dg.kp.ibm, out);
   k_rel_offsets<<<grid, 256, 0, S>>>(goff, N, dg.d_node_base, dg.n_games, rel);
   sol.energy_size = 1;
   sol.offsets.resize(N + dg.n_games);
@@ -1624,20 +2083,16 @@ geq_status Engine::download(DeviceGamesImpl &dg, geq_solution &sol) {
   if (total) CU(cudaMemcpyAsync(sol.data.data(), out, total * 4, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   CU(cudaGetLastError());
-  cudaFree(goff);
-  cudaFree(rel);
-  cudaFree(out);
+  s.pool.put(goff, (N + 1) * 8);
+  s.pool.put(rel, (N + dg.n_games) * 8);
+  s.pool.put(out, std::max<unsigned long long>(total, 1) * 4);
   sol.n_vertices.resize(dg.n_games);
   sol.offsets_base.resize(dg.n_games);
   sol.data_base.resize(dg.n_games);
+  unsigned long long db = 0;
   for (uint32_t g = 0; g < dg.n_games; g++) {
     sol.n_vertices[g] = (uint32_t)(dg.node_base[g + 1] - dg.node_base[g]);
     sol.offsets_base[g] = dg.node_base[g] + g;
-  }
-  // data base of each game = global offset of its first position; recover it
-  // from the relative offsets by accumulating the game totals.
-  unsigned long long db = 0;
-  for (uint32_t g = 0; g < dg.n_games; g++) {
     sol.data_base[g] = db;
     db += sol.offsets[sol.offsets_base[g] + sol.n_vertices[g]];
   }
@@ -1656,28 +2111,28 @@ geq_status Engine::download_selected(DeviceGamesImpl &dg, const std::vector<uint
   unsigned long long launches = 0;
   geq_status a = ensure_cnt(s, K + 1);
   if (a) return a;
-  uint32_t *d_sel = nullptr, *out = nullptr;
-  unsigned long long *goff = nullptr;
-  if ((a = dalloc(d_sel, K))) return a;
-  if ((a = dalloc(goff, K + 1))) { cudaFree(d_sel); return a; }
+  uint32_t *d_sel = (uint32_t *)s.pool.get(std::max<unsigned long long>(K, 1) * 4);
+  unsigned long long *goff = (unsigned long long *)s.pool.get((K + 1) * 8);
+  if (!d_sel || !goff) return fail(GEQ_ERR_OUT_OF_MEMORY, "selection");
   if (K) CU(cudaMemcpyAsync(d_sel, sel.data(), K * 4, cudaMemcpyHostToDevice, S));
   const unsigned grid = (unsigned)std::max(1, n_sms * 8);
   k_sel_counts<<<grid, 256, 0, S>>>(dg.desc, d_sel, K, s.cnt);
-  if ((a = scan_u32(s, s.cnt, K, goff, launches))) { cudaFree(d_sel); cudaFree(goff); return a; }
+  if ((a = scan_u32(s, s.cnt, K, goff, launches))) return a;
   std::vector<unsigned long long> off(K + 1);
   CU(cudaMemcpyAsync(off.data(), goff, (K + 1) * 8, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   const unsigned long long total = off[K];
-  if ((a = dalloc(out, total))) { cudaFree(d_sel); cudaFree(goff); return a; }
-  k_sel_gather<<<grid, 256, 0, S>>>(dg.desc, d_sel, K, goff, dg.arena[dg.arena_cur], out);
+  uint32_t *out = (uint32_t *)s.pool.get(std::max<unsigned long long>(total, 1) * 4);
+  if (!out) return fail(GEQ_ERR_OUT_OF_MEMORY, "selection data");
+  k_sel_gather<<<grid, 256, 0, S>>>(dg.desc, d_sel, K, goff, dg.arena[dg.arena_cur], dg.kp.ib, dg.kp.ibm, out);
   sol.energy_size = 1;
   sol.data.resize(total);
   if (total) CU(cudaMemcpyAsync(sol.data.data(), out, total * 4, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   CU(cudaGetLastError());
-  cudaFree(d_sel);
-  cudaFree(goff);
-  cudaFree(out);
+  s.pool.put(d_sel, std::max<unsigned long long>(K, 1) * 4);
+  s.pool.put(goff, (K + 1) * 8);
+  s.pool.put(out, std::max<unsigned long long>(total, 1) * 4);
   sol.n_vertices.assign(count.begin(), count.end());
   sol.offsets_base.resize(G);
   sol.data_base.resize(G);

@@ -154,6 +154,10 @@ void GameBuilder::build(const Lts &l) {
   col.clear();
   wt.clear();
   for (size_t idx = 0; idx < nodes.size(); idx++) {
+    if (max_positions && nodes.size() > max_positions) {
+      truncated = true;
+      break;
+    }
     const PosKey x = nodes[idx];
     succ.clear();
     sw.clear();

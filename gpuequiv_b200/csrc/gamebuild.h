@@ -38,6 +38,8 @@ struct GameBuilder {
   std::vector<PosKey> nodes;
   std::vector<uint32_t> table;  // node id + 1, 0 = free
   uint32_t n_starting = 0;
+  uint64_t max_positions = 0;  // 0 = unbounded; build() stops once exceeded
+  bool truncated = false;
   std::vector<uint32_t> row, col, wt;
   std::vector<uint8_t> attacker;
 

@@ -100,6 +100,8 @@ class Engine {
   // become game g of the solution.
   geq_status download_selected(DeviceGamesImpl &dg, const std::vector<uint32_t> &first,
                                const std::vector<uint32_t> &count, geq_solution &sol);
+  // Node id of game g's first position inside the uploaded batch.
+  static uint64_t game_node_base(const DeviceGamesImpl &dg, uint32_t g);
   geq_tuning tuning{};
   int n_sms = 0;
   uint64_t total_mem = 0;

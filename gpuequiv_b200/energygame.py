@@ -272,6 +272,37 @@ def run_batch(graphs: Sequence[GameGraph], context: Context | None = None):
     return out, stats
 
 
+def run_batch_raw(graphs: Sequence[GameGraph], context: Context | None = None, views=None):
+    """geq_energy_game_run_batch with flat results: returns (offsets, data,
+    stats) where offsets[g] is game g's (n+1) offset array and data[g] its
+    packed energies.  No per-position objects are created."""
+    ctx = context or default_context()
+    n = len(graphs)
+    if views is None:
+        views = (geq_game_graph * n)(*[g.c_view() for g in graphs])
+    sol = C.c_void_p()
+    check(lib.geq_energy_game_run_batch(ctx.h, n, views, None, None, None, C.byref(sol)))
+    try:
+        view = geq_energy_lists()
+        offs, data = [], []
+        for i in range(n):
+            check(lib.geq_solution_lists(sol, i, C.byref(view)))
+            nv = view.n_vertices
+            o = np.ctypeslib.as_array(view.offsets, shape=(nv + 1,))
+            t = int(o[-1])
+            offs.append(o.copy())
+            data.append(np.ctypeslib.as_array(view.data, shape=(t,)).copy() if t else np.zeros(0, np.uint32))
+        stats = _stats_of(sol)
+    finally:
+        lib.geq_solution_free(sol)
+    return offs, data, stats
+
+
+def c_views(graphs: Sequence[GameGraph]):
+    """geq_game_graph array of the graphs (keep the graphs alive)."""
+    return (geq_game_graph * len(graphs))(*[g.c_view() for g in graphs])
+
+
 class DeviceGames:
     """Games resident on the device (upload once, solve repeatedly)."""
 
@@ -309,4 +340,5 @@ class DeviceGames:
             pass
 
 
-__all__ = ["Context", "default_context", "GameGraph", "EnergyGame", "run_batch", "DeviceGames", "GeqError"]
+__all__ = ["Context", "default_context", "GameGraph", "EnergyGame", "run_batch", "run_batch_raw", "c_views",
+           "DeviceGames", "GeqError"]

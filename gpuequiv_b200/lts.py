@@ -220,6 +220,13 @@ class GameBuild:
         return cls(h)
 
     @classmethod
+    def compare_bounded(cls, lts: TransitionSystem, p: int, q: int, max_positions: int) -> "GameBuild":
+        """compare() that raises GeqError(OUT_OF_MEMORY) beyond max_positions."""
+        h = C.c_void_p()
+        check(lib.geq_game_build_compare_bounded(lts.h, p, q, int(max_positions), C.byref(h)))
+        return cls(h)
+
+    @classmethod
     def compare_all(cls, lts: TransitionSystem) -> tuple["GameBuild", StartInfo]:
         h = C.c_void_p()
         check(lib.geq_game_build_compare_all(lts.h, C.byref(h)))

@@ -149,3 +149,65 @@ def stress_game(seed: int = 2, n: int = 2_000_000, m: int = 10_000_000, p_att: f
 def scaled_stress_game(seed: int, n: int, m: int):
     """The stress generator at another size (parity tests)."""
     return stress_game(seed=seed, n=n, m=m)
+
+
+def select_batched_jobs(n_jobs: int, max_positions: int = 200_000, first_seed: int = 0, threads: int | None = None):
+    """Jobs of the batched configuration, in seed order, keeping those whose
+    pair is not bisimilar and whose game has at most ``max_positions``
+    positions (the spectroscopy game is exponential in the nondeterminism of
+    the LTS; about a quarter of the specified jobs exceed a million
+    positions).  Returns a list of dicts with the LTS arrays, the pair, the
+    minimised LTS, the built game and its seed."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+
+    from gpuequiv_b200 import GameBuild, GeqError, TransitionSystem
+
+    threads = threads or min(32, os.cpu_count() or 4)
+
+    def one(seed):
+        src, dst, lab, p, q = batched_lts(seed)
+        lts = TransitionSystem.from_arrays(src, dst, lab)
+        red, mapping = lts.bisimilar_minimize()
+        pm, qm = int(mapping[p]), int(mapping[q])
+        if pm == qm:
+            return None
+        try:
+            b = GameBuild.compare_bounded(red, pm, qm, max_positions)
+        except GeqError:
+            return None
+        return dict(seed=seed, src=src, dst=dst, lab=lab, p=p, q=q, lts=lts, red=red, pm=pm, qm=qm, build=b)
+
+    out = []
+    seed = first_seed
+    chunk = max(64, threads * 8)
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while len(out) < n_jobs:
+            res = list(ex.map(one, range(seed, seed + chunk)))
+            seed += chunk
+            out.extend(r for r in res if r is not None)
+    return out[:n_jobs]
+
+
+MANIFEST = __import__("os").path.join(__import__("os").path.dirname(__file__), "data", "batched_seeds.json")
+
+
+def write_batched_manifest(n_jobs: int = 4096, max_positions: int = 200_000, path: str = MANIFEST) -> None:
+    """Record the accepted seeds of the batched configuration (with their game
+    sizes) so that every consumer solves exactly the same jobs."""
+    import json
+    jobs = select_batched_jobs(n_jobs, max_positions)
+    rows = [[j["seed"], int(j["build"].game.n_vertices()), int(j["build"].game.n_edges())] for j in jobs]
+    with open(path, "w") as f:
+        json.dump({"generator": "synth.batched_lts", "max_positions": max_positions,
+                   "fields": ["seed", "positions", "edges"], "jobs": rows}, f, separators=(",", ":"))
+
+
+def batched_manifest(path: str = MANIFEST) -> dict:
+    import json
+    with open(path) as f:
+        return json.load(f)
+
+
+if __name__ == "__main__":
+    write_batched_manifest()

@@ -141,6 +141,9 @@ typedef struct geq_solve_stats {
   uint64_t arena_compactions;   /* energy-arena garbage collections */
   uint64_t kernel_launches;     /* kernels launched by the solve */
   double device_ms;             /* device time of the solve (CUDA events) */
+  double round_kernel_ms;       /* GEQ_TUNE_PROFILE only: summed duration of the
+                                   round kernel launches (CUDA events around each) */
+  uint64_t round_kernel_launches;
 } geq_solve_stats;
 
 /* Result of a solve: one or more games, each with its per-position lists. */
@@ -187,7 +190,8 @@ void geq_device_games_free(geq_device_games *dg);
 
 /* Solver tuning (autotuner output).  Zero fields keep the current value. */
 typedef struct geq_tuning {
-  uint32_t blocks_per_sm;     /* resident 256-thread blocks per SM of the round kernel */
+  uint32_t blocks_per_sm;     /* resident 256-thread blocks per SM of the round kernel
+                                 (2, 3 or 4: selects the register budget) */
   uint32_t rounds_per_graph;  /* worklist rounds captured per CUDA graph launch */
   uint32_t small_limit;       /* candidates handled in registers per position (1..32) */
   uint32_t flags;             /* GEQ_TUNE_* bits */
@@ -195,6 +199,8 @@ typedef struct geq_tuning {
 #define GEQ_TUNE_FORCE_GENERIC 1u /* generic codec even for STANDARD (cross-check) */
 #define GEQ_TUNE_FORCE_LARGE 2u   /* bypass the register paths (cross-check) */
 #define GEQ_TUNE_NO_GRAPH 4u      /* launch rounds one by one instead of graphs */
+#define GEQ_TUNE_PROFILE 8u       /* time every round-kernel launch (implies no graphs) */
+#define GEQ_TUNE_NO_THREAD_PATH 16u /* no lane-per-position path (cross-check) */
 geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t);
 void geq_context_get_tuning(const geq_context *ctx, geq_tuning *t);
 
@@ -228,6 +234,11 @@ geq_status geq_game_build_compare_all(const geq_lts *l, geq_game_build **out);
 /* GameBuild::compare_multiple (gamebuild.rs:176-194) */
 geq_status geq_game_build_compare_multiple(const geq_lts *l, const uint32_t *processes,
                                            uint32_t n_processes, geq_game_build **out);
+/* GameBuild::compare with a bound: GEQ_ERR_OUT_OF_MEMORY if the game would
+ * have more than max_positions positions (the game is exponential in the
+ * nondeterminism of the LTS; the reference has no such guard). */
+geq_status geq_game_build_compare_bounded(const geq_lts *l, uint32_t p, uint32_t q,
+                                          uint64_t max_positions, geq_game_build **out);
 /* The generated GameGraph (borrowed view). */
 void geq_game_build_graph(const geq_game_build *b, geq_game_graph *out);
 uint32_t geq_game_build_n_starting_points(const geq_game_build *b);

@@ -1,8 +1,10 @@
 """CUDA path vs the oracle and the reference's known answers (EnergyGame::run).
 
-Every case runs under four solver modes so that each kernel path is checked:
-the default (register paths + 4096-bit bitmap paths, CUDA graphs), the
-bitmap/list paths only, the generic codec, and round-by-round launches.
+Every case runs under several solver modes so that each kernel path is
+checked: the default (lane-per-position path, warp register paths, 4096-bit
+bitmap paths, CUDA graphs), the warp paths only, the bitmap/list paths only,
+the generic codec (with and without the register paths), and round-by-round
+launches.
 Bit-exact: per-position energy lists are compared as sorted multisets.
 """
 import numpy as np
@@ -16,6 +18,7 @@ pytestmark = pytest.mark.gpu
 
 MODES = {
     "default": dict(),
+    "warp": dict(flags=16),
     "large": dict(flags=2),
     "generic": dict(flags=1),
     "generic_large": dict(flags=3),
