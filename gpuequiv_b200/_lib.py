@@ -98,6 +98,8 @@ _SIGS = {
     "geq_context_get_tuning": ([vp, C.POINTER(geq_tuning)], None),
     "geq_solution_n_games": ([vp], C.c_uint32),
     "geq_solution_lists": ([vp, C.c_uint32, C.POINTER(geq_energy_lists)], C.c_int),
+    "geq_solution_flat": ([vp, C.POINTER(u64p), C.POINTER(C.c_uint64), C.POINTER(u32p), C.POINTER(C.c_uint64)],
+                          C.c_int),
     "geq_solution_stats": ([vp, C.POINTER(geq_solve_stats)], None),
     "geq_solution_free": ([vp], None),
     "geq_energy_game_run": ([vp, C.POINTER(geq_game_graph), C.POINTER(geq_energy_lists), u32p, C.c_uint32,
@@ -141,6 +143,10 @@ _SIGS = {
 
 
 def library_path() -> str:
+    """$GEQ_LIBRARY if set (another build of the same ABI), else the in-tree
+    libgeq.so, or libgeq_checked.so when GEQ_CHECKED=1."""
+    if os.environ.get("GEQ_LIBRARY"):
+        return os.path.abspath(os.environ["GEQ_LIBRARY"])
     name = "libgeq_checked.so" if os.environ.get("GEQ_CHECKED") == "1" else "libgeq.so"
     return os.path.join(HERE, name)
 

@@ -276,8 +276,26 @@ geq_status geq_solution_lists(const geq_solution *s, uint32_t game, geq_energy_l
   if (!s || !out || game >= s->n_vertices.size()) return fail(GEQ_ERR_INVALID_INPUT, "no such game");
   out->n_vertices = s->n_vertices[game];
   out->energy_size = s->energy_size;
-  out->offsets = s->offsets.data() + s->offsets_base[game];
-  out->data = s->data.data() + s->data_base[game] * s->energy_size;
+  out->offsets = s->off_ptr() + s->offsets_base[game];
+  out->data = s->data_ptr() + s->data_base[game] * s->energy_size;
+  return GEQ_OK;
+}
+
+geq_status geq_solution_flat(const geq_solution *s, const uint64_t **offsets, uint64_t *n_offsets,
+                             const uint32_t **data, uint64_t *n_words) {
+  if (!s || !offsets || !n_offsets || !data || !n_words) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  // the flat layout holds when each game's offsets and words follow the previous game's
+  uint64_t ob = 0, db = 0;
+  for (size_t g = 0; g < s->n_vertices.size(); g++) {
+    if (s->offsets_base[g] != ob || s->data_base[g] != db)
+      return fail(GEQ_ERR_UNSUPPORTED, "solution is not laid out flat");
+    db += s->off_ptr()[ob + s->n_vertices[g]];
+    ob += (uint64_t)s->n_vertices[g] + 1;
+  }
+  *offsets = s->off_ptr();
+  *n_offsets = s->offsets_len();
+  *data = s->data_ptr();
+  *n_words = s->data_len() / (s->energy_size ? s->energy_size : 1);
   return GEQ_OK;
 }
 

@@ -56,6 +56,11 @@ namespace geq {
 #ifndef GEQ_CHECKED
 #define GEQ_CHECKED 0
 #endif
+// GEQ_PATH_PROFILE=1: k_round counts positions and SM cycles per code path
+// into Ctr::prof and solve() prints them to stderr (diagnostic builds only).
+#ifndef GEQ_PATH_PROFILE
+#define GEQ_PATH_PROFILE 0
+#endif
 
 constexpr uint32_t FULL = 0xffffffffu;
 constexpr unsigned long long NONE_DESC = ~0ull;
@@ -92,7 +97,19 @@ struct Ctr {
   uint32_t done_blocks;
   uint32_t pad;
   unsigned long long positions, edges, bytes, rounds;
+#if GEQ_PATH_PROFILE
+  unsigned long long prof[16];
+#endif
 };
+#if GEQ_PATH_PROFILE
+enum : int {
+  PF_CYC_THREAD, PF_CYC_BIG, PF_CYC_PUSH, PF_T_ATT, PF_T_DEF, PF_B_ATT, PF_B_DEF, PF_T_CAND, PF_T_DEG,
+  PF_SKIP, PF_SLOTS, PF_CYC_ALL, PF_ITERS, PF_T_UNCH, PF_B_DEG, PF_PUSHED
+};
+#define PROF_ADD(i, v) prof_acc[i] += (v)
+#else
+#define PROF_ADD(i, v) ((void)0)
+#endif
 
 struct KParams {
   const uint32_t *row, *col, *wt, *rrow, *rcol;
@@ -1034,7 +1051,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
   unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0;  // warp routines (lane-uniform)
   unsigned long long t_edges = 0, t_bytes = 0, t_pos = 0;  // thread path (per lane)
   WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes};
+#if GEQ_PATH_PROFILE
+  unsigned long long prof_acc[16] = {};
+  const long long t_all0 = clock64();
+#endif
   for (uint32_t base = gw * 32u; base < fs; base += nw * 32u) {
+#if GEQ_PATH_PROFILE
+    const long long tq0 = clock64();
+#endif
     const uint32_t slot = base + lane;
     const bool active = slot < fs;
     const uint32_t v = active ? ld(F, slot, p.n_nodes, c) : 0u;
@@ -1067,11 +1091,30 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
     if (active && ts != T_BIG && CHECK_IDX(c, slot, p.n_nodes)) p.slot_new[slot] = (ts == T_CHANGED) ? nd : NONE_DESC;
     // large positions: the whole warp on one position at a time
     uint32_t big = __ballot_sync(FULL, ts == T_BIG);
+#if GEQ_PATH_PROFILE
+    const long long tq1 = clock64();
+    if (lane == 0) { PROF_ADD(PF_CYC_THREAD, tq1 - tq0); PROF_ADD(PF_ITERS, 1); }
+    if (active) {
+      PROF_ADD(PF_SLOTS, 1);
+      if (ts == T_SKIPPED) PROF_ADD(PF_SKIP, 1);
+      if (ts == T_CHANGED || ts == T_UNCHANGED) {
+        PROF_ADD((p.flags[v] & 1u) ? PF_T_ATT : PF_T_DEF, 1);
+        PROF_ADD(PF_T_DEG, p.row[v + 1] - p.row[v]);
+        if (ts == T_UNCHANGED) PROF_ADD(PF_T_UNCH, 1);
+      }
+    }
+#endif
     bool big_changed = false;
     while (big) {
       const uint32_t l = __ffs(big) - 1u;
       big &= big - 1u;
       const uint32_t vb = __shfl_sync(FULL, v, l);
+#if GEQ_PATH_PROFILE
+      if (lane == 0) {
+        PROF_ADD((p.flags[vb] & 1u) ? PF_B_ATT : PF_B_DEF, 1);
+        PROF_ADD(PF_B_DEG, p.row[vb + 1] - p.row[vb]);
+      }
+#endif
       const Res r = solve_position(x, cd, vb);
       if (r.st != R_SKIPPED) w_pos++;
       if (lane == 0 && CHECK_IDX(c, base + l, p.n_nodes))
@@ -1079,9 +1122,27 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
       if (lane == l) big_changed = r.st == R_CHANGED;
       if (r.st == R_OVERFLOW && lane == 0) requeue(p, c, vb, NF, nf_size, stamp);  // retried after compaction
     }
+#if GEQ_PATH_PROFILE
+    const long long tq2 = clock64();
+    if (lane == 0) PROF_ADD(PF_CYC_BIG, tq2 - tq1);
+#endif
     push_preds_warp(p, c, sm, v, ts == T_CHANGED || big_changed, NF, nf_size, stamp, lane);
     if (ts == T_OVERFLOW) requeue(p, c, v, NF, nf_size, stamp);
+#if GEQ_PATH_PROFILE
+    if (lane == 0) PROF_ADD(PF_CYC_PUSH, clock64() - tq2);
+    if ((ts == T_CHANGED || big_changed)) PROF_ADD(PF_PUSHED, p.rrow[v + 1] - p.rrow[v]);
+#endif
   }
+#if GEQ_PATH_PROFILE
+  if (lane == 0) PROF_ADD(PF_CYC_ALL, clock64() - t_all0);
+#pragma unroll
+  for (int i = 0; i < 16; i++) {
+    unsigned long long a = prof_acc[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(FULL, a, o);
+    if (lane == 0 && a) atomicAdd(&c->prof[i], a);
+  }
+#endif
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     t_edges += __shfl_xor_sync(FULL, t_edges, o);
@@ -1470,6 +1531,71 @@ class DevPool {
   size_t limit_ = (size_t)16 << 30;
 };
 
+size_t HostPool::round_size(size_t b) {
+  b = std::max<size_t>(b, 4096);
+  if (b <= (64u << 20)) {
+    size_t r = 4096;
+    while (r < b) r <<= 1;
+    return r;
+  }
+  return (b + (64u << 20) - 1) & ~size_t((64u << 20) - 1);
+}
+void *HostPool::get(size_t bytes, size_t &cap) {
+  cap = round_size(bytes);
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = free_.find(cap);
+    if (it != free_.end() && !it->second.empty()) {
+      void *p = it->second.back();
+      it->second.pop_back();
+      cached_ -= cap;
+      return p;
+    }
+  }
+  void *p = nullptr;
+  if (cudaHostAlloc(&p, cap, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+void HostPool::put(void *p, size_t cap) {
+  if (!p) return;
+  {
+    std::lock_guard<std::mutex> g(mu_);
+    if (cached_ + cap <= limit_) {
+      free_[cap].push_back(p);
+      cached_ += cap;
+      return;
+    }
+  }
+  cudaFreeHost(p);
+}
+HostPool::~HostPool() {
+  for (auto &kv : free_)
+    for (void *p : kv.second) cudaFreeHost(p);
+}
+bool HostBuf::alloc(const std::shared_ptr<HostPool> &hp, size_t bytes) {
+  reset();
+  bytes = std::max<size_t>(bytes, 8);
+  if (hp && (p = hp->get(bytes, cap)) != nullptr) {
+    pool = hp;
+    return true;
+  }
+  p = std::malloc(bytes);
+  cap = bytes;
+  return p != nullptr;
+}
+void HostBuf::reset() {
+  if (p) {
+    if (pool) pool->put(p, cap);
+    else std::free(p);
+  }
+  p = nullptr;
+  cap = 0;
+  pool.reset();
+}
+
 struct Engine::State {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, eva = nullptr, evb = nullptr;
@@ -1488,6 +1614,7 @@ struct Engine::State {
   size_t stage_cap = 0;
   uint32_t *d_err = nullptr;
   DevPool pool;
+  std::shared_ptr<HostPool> hpool = std::make_shared<HostPool>();
   std::set<DeviceGamesImpl *> live;
 };
 
@@ -1505,6 +1632,7 @@ struct DeviceGamesImpl {
   uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr;
   uint32_t *init_data = nullptr;
   unsigned long long init_total = 0;
+  char *inbuf = nullptr;  // row, col, wt, flags, reach, init_data, [desc_init], node bases
   uint32_t *arena[2] = {nullptr, nullptr};
   unsigned long long arena_cap[2] = {0, 0};
   int arena_cur = 0;
@@ -1606,38 +1734,72 @@ static geq_status ensure_stage(Engine::State &s, size_t bytes) {
   return GEQ_OK;
 }
 
-// memcpy jobs spread over host threads (large uploads only)
+// Host-to-device upload of the staging buffer.  Small uploads are packed
+// serially and sent with one copy.  Large ones are split into windows of the
+// staging buffer: host threads pack the pieces in address order and each
+// window is sent as soon as all its pieces are in, so packing overlaps the
+// link transfer.
 struct CopyJob {
   void *dst;
   const void *src;
   size_t bytes;
 };
-static void run_copies(std::vector<CopyJob> &jobs) {
-  size_t total = 0;
-  for (auto &j : jobs) total += j.bytes;
+static geq_status staged_upload(std::vector<CopyJob> &jobs, const char *stage, char *dev, size_t total,
+                                cudaStream_t S) {
+  size_t payload = 0;
+  for (auto &j : jobs) payload += j.bytes;
   const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const unsigned T = total < (8u << 20) ? 1u : std::min(16u, hw);
-  if (T == 1) {
+  if (payload < (16u << 20) || hw < 2) {
     for (auto &j : jobs)
       if (j.bytes) std::memcpy(j.dst, j.src, j.bytes);
-    return;
+    if (total) CU(cudaMemcpyAsync(dev, stage, total, cudaMemcpyHostToDevice, S));
+    return GEQ_OK;
   }
-  std::vector<CopyJob> split;
-  const size_t piece = 4u << 20;
-  for (auto &j : jobs)
-    for (size_t o = 0; o < j.bytes; o += piece)
-      split.push_back(CopyJob{(char *)j.dst + o, (const char *)j.src + o, std::min(piece, j.bytes - o)});
+  constexpr size_t WIN = 32u << 20, PIECE = 2u << 20;
+  const size_t n_win = (total + WIN - 1) / WIN;
+  struct Piece {
+    size_t off;  // offset in the staging buffer
+    const char *src;
+    size_t bytes;
+  };
+  std::vector<Piece> pieces;
+  pieces.reserve(jobs.size() + payload / PIECE + n_win);
+  for (auto &j : jobs) {
+    size_t o = (size_t)((const char *)j.dst - stage), left = j.bytes;
+    const char *src = (const char *)j.src;
+    while (left) {
+      const size_t win_end = (o / WIN + 1) * WIN;
+      const size_t b = std::min({left, PIECE, win_end - o});
+      pieces.push_back(Piece{o, src, b});
+      o += b; src += b; left -= b;
+    }
+  }
+  std::sort(pieces.begin(), pieces.end(), [](const Piece &a, const Piece &b) { return a.off < b.off; });
+  std::unique_ptr<std::atomic<size_t>[]> pending(new std::atomic<size_t>[n_win]);
+  for (size_t w = 0; w < n_win; w++) pending[w].store(0, std::memory_order_relaxed);
+  for (auto &pc : pieces) pending[pc.off / WIN].fetch_add(1, std::memory_order_relaxed);
   std::atomic<size_t> next{0};
+  const unsigned T = std::min(16u, hw);
   std::vector<std::thread> pool;
+  pool.reserve(T);
   for (unsigned t = 0; t < T; t++)
     pool.emplace_back([&]() {
       for (;;) {
-        size_t i = next.fetch_add(1);
-        if (i >= split.size()) break;
-        std::memcpy(split[i].dst, split[i].src, split[i].bytes);
+        const size_t i = next.fetch_add(1, std::memory_order_relaxed);
+        if (i >= pieces.size()) break;
+        std::memcpy((char *)stage + pieces[i].off, pieces[i].src, pieces[i].bytes);
+        pending[pieces[i].off / WIN].fetch_sub(1, std::memory_order_release);
       }
     });
+  cudaError_t ce = cudaSuccess;
+  for (size_t w = 0; w < n_win; w++) {
+    while (pending[w].load(std::memory_order_acquire) != 0) std::this_thread::yield();
+    const size_t o = w * WIN, b = std::min(WIN, total - o);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(dev + o, stage + o, b, cudaMemcpyHostToDevice, S);
+  }
   for (auto &th : pool) th.join();
+  if (ce != cudaSuccess) return fail(GEQ_ERR_CUDA, "upload copy: %s", cudaGetErrorString(ce));
+  return GEQ_OK;
 }
 
 geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
@@ -1784,36 +1946,35 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
     h_eb[g] = eb;
     h_gn[g] = n;
   }
-  run_copies(copies);
   h_row[N] = (uint32_t)M;
   h_nb[dg->n_games] = N;
   h_eb[dg->n_games] = M;
   h_gn[dg->n_games] = 0;
 
-  // device allocations (pooled)
+  // device allocations (pooled); the uploaded inputs share one block laid
+  // out like the staging buffer, so any window of it is one copy
   DeviceGamesImpl &D = *dg;
-  if (!D.alloc(D.row, N + 1) || !D.alloc(D.col, M) || !D.alloc(D.wt, M) || !D.alloc(D.rrow, N + 1) ||
-      !D.alloc(D.rcol, M) || !D.alloc(D.flags, N) || !D.alloc(D.desc, N) || !D.alloc(D.desc_init, N) ||
-      !D.alloc(D.slot_new, N) || !D.alloc(D.mark, N) || !D.alloc(D.front0, N) || !D.alloc(D.front1, N) ||
-      !D.alloc(D.init_data, D.init_total) || !D.alloc(D.reach, n_reach) ||
-      !D.alloc(D.d_node_base, 3 * (D.n_games + 1)) || !D.alloc(D.ctr, 1))
+  if (!D.alloc(D.inbuf, total_bytes))
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation of %zu input bytes failed", total_bytes);
+  D.row = (uint32_t *)(D.inbuf + off_row);
+  D.col = (uint32_t *)(D.inbuf + off_col);
+  D.wt = (uint32_t *)(D.inbuf + off_wt);
+  D.flags = (uint8_t *)(D.inbuf + off_flags);
+  D.reach = (uint32_t *)(D.inbuf + off_reach);
+  D.init_data = (uint32_t *)(D.inbuf + off_init);
+  D.d_node_base = (unsigned long long *)(D.inbuf + off_base);
+  if (any_init) D.desc_init = (unsigned long long *)(D.inbuf + off_desc);
+  if (!D.alloc(D.rrow, N + 1) || !D.alloc(D.rcol, M) || !D.alloc(D.desc, N) ||
+      (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, N) ||
+      !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1))
     return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
   D.arena_cap[0] = DevPool::round_size(cap * 4) / 4;
   cudaStream_t S = s.stream;
-  CU(cudaMemcpyAsync(D.row, h_row, (N + 1) * 4, cudaMemcpyHostToDevice, S));
-  if (M) {
-    CU(cudaMemcpyAsync(D.col, h_col, M * 4, cudaMemcpyHostToDevice, S));
-    CU(cudaMemcpyAsync(D.wt, h_wt, M * 4, cudaMemcpyHostToDevice, S));
-  }
-  if (N) CU(cudaMemcpyAsync(D.flags, h_flags, N, cudaMemcpyHostToDevice, S));
-  if (n_reach) CU(cudaMemcpyAsync(D.reach, h_reach, n_reach * 4, cudaMemcpyHostToDevice, S));
-  CU(cudaMemcpyAsync(D.init_data, h_init, D.init_total * 4, cudaMemcpyHostToDevice, S));
-  CU(cudaMemcpyAsync(D.d_node_base, h_nb, 3 * (D.n_games + 1) * 8, cudaMemcpyHostToDevice, S));
-  if (any_init) {
-    if (N) CU(cudaMemcpyAsync(D.desc_init, h_desc, N * 8, cudaMemcpyHostToDevice, S));
-  } else {
+  geq_status ust = staged_upload(copies, H, D.inbuf, total_bytes, S);
+  if (ust) return ust;
+  if (!any_init) {
     if (N) CU(cudaMemsetAsync(D.desc_init, 0, N * 8, S));
     if (n_reach)
       k_init_reach<<<(unsigned)std::min<unsigned long long>((n_reach + 255) / 256, 4096), 256, 0, S>>>(
@@ -2036,6 +2197,11 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
   CU(cudaStreamSynchronize(S));
   const Ctr c = *s.h_ctr;
   dg.next_stamp = c.stamp + 2u;
+#if GEQ_PATH_PROFILE
+  std::fprintf(stderr, "GEQ_PROF");
+  for (int i = 0; i < 16; i++) std::fprintf(stderr, " %llu", c.prof[i]);
+  std::fprintf(stderr, "\n");
+#endif
   if (stats) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, s.ev0, s.ev1);
@@ -2077,10 +2243,13 @@ geq_status Engine::download(DeviceGamesImpl &dg, geq_solution &sol) {
   k_gather<<<grid, 256, 0, S>>>(dg.desc, N, goff, dg.arena[dg.arena_cur], dg.kp.ib, dg.kp.ibm, out);
   k_rel_offsets<<<grid, 256, 0, S>>>(goff, N, dg.d_node_base, dg.n_games, rel);
   sol.energy_size = 1;
-  sol.offsets.resize(N + dg.n_games);
-  sol.data.resize(total);
-  CU(cudaMemcpyAsync(sol.offsets.data(), rel, (N + dg.n_games) * 8, cudaMemcpyDeviceToHost, S));
-  if (total) CU(cudaMemcpyAsync(sol.data.data(), out, total * 4, cudaMemcpyDeviceToHost, S));
+  // straight into page-locked host memory (no staging copy, no zero fill)
+  sol.n_offsets = N + dg.n_games;
+  sol.n_words = total;
+  if (!sol.off_buf.alloc(s.hpool, sol.n_offsets * 8) || !sol.data_buf.alloc(s.hpool, total * 4))
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu result words", total);
+  CU(cudaMemcpyAsync(sol.off_buf.p, rel, sol.n_offsets * 8, cudaMemcpyDeviceToHost, S));
+  if (total) CU(cudaMemcpyAsync(sol.data_buf.p, out, total * 4, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   CU(cudaGetLastError());
   s.pool.put(goff, (N + 1) * 8);
@@ -2089,12 +2258,13 @@ geq_status Engine::download(DeviceGamesImpl &dg, geq_solution &sol) {
   sol.n_vertices.resize(dg.n_games);
   sol.offsets_base.resize(dg.n_games);
   sol.data_base.resize(dg.n_games);
+  const uint64_t *offs = sol.off_ptr();
   unsigned long long db = 0;
   for (uint32_t g = 0; g < dg.n_games; g++) {
     sol.n_vertices[g] = (uint32_t)(dg.node_base[g + 1] - dg.node_base[g]);
     sol.offsets_base[g] = dg.node_base[g] + g;
     sol.data_base[g] = db;
-    db += sol.offsets[sol.offsets_base[g] + sol.n_vertices[g]];
+    db += offs[sol.offsets_base[g] + sol.n_vertices[g]];
   }
   return GEQ_OK;
 }

@@ -1,8 +1,11 @@
 // geq_internal.h - declarations shared by the sources of libgeq.so.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -52,17 +55,59 @@ struct GameInput {
 geq_status validate_graph(const geq_game_graph &g);
 geq_status validate_lists(const geq_game_graph &g, const geq_energy_lists *l);
 
+// ---- page-locked host memory for results -------------------------------------
+// Blocks are cached by size class so that downloads copy straight into
+// page-locked memory at full link speed without paying for the page locking
+// on every call.  A block lent to a solution returns to the cache when the
+// solution is freed; the cache lives as long as its engine or its last
+// lent block, whichever is later.
+class HostPool {
+ public:
+  static size_t round_size(size_t bytes);
+  void *get(size_t bytes, size_t &cap);  // nullptr when page-locked memory is unavailable
+  void put(void *p, size_t cap);
+  ~HostPool();
+
+ private:
+  std::mutex mu_;
+  std::map<size_t, std::vector<void *>> free_;
+  size_t cached_ = 0;
+  size_t limit_ = (size_t)4 << 30;
+};
+
+// One host array: a HostPool block, or heap memory when none could be had.
+// The contents start uninitialised.
+struct HostBuf {
+  std::shared_ptr<HostPool> pool;
+  void *p = nullptr;
+  size_t cap = 0;
+  bool alloc(const std::shared_ptr<HostPool> &hp, size_t bytes);
+  void reset();
+  HostBuf() = default;
+  HostBuf(const HostBuf &) = delete;
+  HostBuf &operator=(const HostBuf &) = delete;
+  ~HostBuf() { reset(); }
+};
+
 }  // namespace geq
 
 // ---- opaque objects of the C ABI ------------------------------------------
+// A solution's lists live either in the vectors (results assembled on the
+// host) or in the HostBufs (a whole batch copied back from the device).
 struct geq_solution {
   uint32_t energy_size = 1;
   std::vector<uint32_t> n_vertices;     // per game
-  std::vector<uint64_t> offsets_base;   // per game: index into `offsets`
-  std::vector<uint64_t> data_base;      // per game: first word in `data`
+  std::vector<uint64_t> offsets_base;   // per game: index into the offsets
+  std::vector<uint64_t> data_base;      // per game: first word in the data
   std::vector<uint64_t> offsets;        // per game n+1 entries, relative
   std::vector<uint32_t> data;
+  geq::HostBuf off_buf, data_buf;
+  uint64_t n_offsets = 0, n_words = 0;  // sizes when the HostBufs are used
   geq_solve_stats stats{};
+  const uint64_t *off_ptr() const { return off_buf.p ? (const uint64_t *)off_buf.p : offsets.data(); }
+  const uint32_t *data_ptr() const { return data_buf.p ? (const uint32_t *)data_buf.p : data.data(); }
+  uint64_t offsets_len() const { return off_buf.p ? n_offsets : offsets.size(); }
+  uint64_t data_len() const { return data_buf.p ? n_words : data.size(); }
 };
 
 namespace geq {

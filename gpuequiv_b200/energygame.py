@@ -272,29 +272,55 @@ def run_batch(graphs: Sequence[GameGraph], context: Context | None = None):
     return out, stats
 
 
+class _SolutionOwner:
+    """Frees a geq_solution once the last array viewing its memory is gone."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self):
+        if self.h is not None and self.h.value:
+            lib.geq_solution_free(self.h)
+            self.h = None
+
+
+def _borrow(ptr, n: int, ctype, dtype, owner: _SolutionOwner) -> np.ndarray:
+    """numpy view of n elements at ptr that keeps `owner` alive."""
+    if n == 0:
+        return np.zeros(0, dtype)
+    buf = (ctype * n).from_address(C.cast(ptr, C.c_void_p).value)
+    buf._owner = owner
+    return np.frombuffer(buf, dtype=dtype)
+
+
 def run_batch_raw(graphs: Sequence[GameGraph], context: Context | None = None, views=None):
     """geq_energy_game_run_batch with flat results: returns (offsets, data,
     stats) where offsets[g] is game g's (n+1) offset array and data[g] its
-    packed energies.  No per-position objects are created."""
+    packed energies.  The arrays are views of the solution's page-locked
+    memory (no copy, no per-position objects); it is released when the last
+    of them is gone."""
     ctx = context or default_context()
     n = len(graphs)
     if views is None:
         views = (geq_game_graph * n)(*[g.c_view() for g in graphs])
     sol = C.c_void_p()
     check(lib.geq_energy_game_run_batch(ctx.h, n, views, None, None, None, C.byref(sol)))
-    try:
-        view = geq_energy_lists()
-        offs, data = [], []
-        for i in range(n):
-            check(lib.geq_solution_lists(sol, i, C.byref(view)))
-            nv = view.n_vertices
-            o = np.ctypeslib.as_array(view.offsets, shape=(nv + 1,))
-            t = int(o[-1])
-            offs.append(o.copy())
-            data.append(np.ctypeslib.as_array(view.data, shape=(t,)).copy() if t else np.zeros(0, np.uint32))
-        stats = _stats_of(sol)
-    finally:
-        lib.geq_solution_free(sol)
+    owner = _SolutionOwner(sol)
+    stats = _stats_of(sol)
+    po, pd = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+    no, nw = C.c_uint64(), C.c_uint64()
+    check(lib.geq_solution_flat(sol, C.byref(po), C.byref(no), C.byref(pd), C.byref(nw)))
+    flat_o = _borrow(po, no.value, C.c_uint64, np.uint64, owner)
+    flat_d = _borrow(pd, nw.value, C.c_uint32, np.uint32, owner)
+    nv = np.fromiter((g.n_vertices() for g in graphs), dtype=np.int64, count=n)
+    ob = np.zeros(n + 1, np.int64)
+    np.cumsum(nv + 1, out=ob[1:])
+    tot = flat_o[ob[1:] - 1].astype(np.int64) if n else np.zeros(0, np.int64)
+    db = np.zeros(n + 1, np.int64)
+    np.cumsum(tot, out=db[1:])
+    obl, dbl = ob.tolist(), db.tolist()
+    offs = [flat_o[obl[i]:obl[i + 1]] for i in range(n)]
+    data = [flat_d[dbl[i]:dbl[i + 1]] for i in range(n)]
     return offs, data, stats
 
 

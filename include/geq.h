@@ -151,6 +151,14 @@ typedef struct geq_solution geq_solution;
 uint32_t geq_solution_n_games(const geq_solution *s);
 /* Lists of game `game` (borrowed from the solution). */
 geq_status geq_solution_lists(const geq_solution *s, uint32_t game, geq_energy_lists *out);
+/* All games' lists at once (borrowed): game g's n_vertices(g)+1 offsets start
+ * at offsets[first_offset(g)] where first_offset(g) = sum over h < g of
+ * (n_vertices(h) + 1); they are relative to game g's first word, and game g's
+ * words follow game g-1's in `data`.  Lets a binding hand the whole batch to
+ * its caller without per-game calls.  No counterpart in the crate, whose
+ * results are per EnergyGame. */
+geq_status geq_solution_flat(const geq_solution *s, const uint64_t **offsets, uint64_t *n_offsets,
+                             const uint32_t **data, uint64_t *n_words);
 void geq_solution_stats(const geq_solution *s, geq_solve_stats *out);
 void geq_solution_free(geq_solution *s);
 
