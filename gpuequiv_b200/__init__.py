@@ -9,13 +9,13 @@ from ._lib import GeqError, library_path
 from .energy import (Energy, EnergyArray, EnergyConf, Upd, Update, UpdateArray, std_equivalences,
                      update)
 from .energygame import (Context, DeviceGames, EnergyGame, GameGraph, c_views, default_context, run_batch,
-                         run_batch_raw)
+                         run_batch_raw, run_static)
 from .lts import (Equivalence, EquivalenceRelation, GameBuild, Position, StartInfo, TransitionSystem,
                   compare_batch)
 
 __all__ = [
     "GeqError", "library_path", "Energy", "EnergyArray", "EnergyConf", "Upd", "Update", "UpdateArray",
     "std_equivalences", "update", "Context", "DeviceGames", "EnergyGame", "GameGraph", "default_context",
-    "run_batch", "run_batch_raw", "c_views", "Equivalence", "EquivalenceRelation", "GameBuild", "Position", "StartInfo",
+    "run_batch", "run_batch_raw", "run_static", "c_views", "Equivalence", "EquivalenceRelation", "GameBuild", "Position", "StartInfo",
     "TransitionSystem", "compare_batch",
 ]

@@ -104,6 +104,8 @@ _SIGS = {
     "geq_solution_free": ([vp], None),
     "geq_energy_game_run": ([vp, C.POINTER(geq_game_graph), C.POINTER(geq_energy_lists), u32p, C.c_uint32,
                              C.POINTER(vp)], C.c_int),
+    "geq_energy_game_run_static": ([vp, C.POINTER(geq_game_graph), u32p, C.c_uint32, u64p, u32p, C.c_uint64, u64p,
+                                    C.POINTER(geq_solve_stats)], C.c_int),
     "geq_energy_game_run_batch": ([vp, C.c_uint32, C.POINTER(geq_game_graph),
                                    C.POINTER(C.POINTER(geq_energy_lists)), C.POINTER(u32p), u32p,
                                    C.POINTER(vp)], C.c_int),

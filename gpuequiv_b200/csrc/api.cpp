@@ -377,6 +377,21 @@ geq_status geq_energy_game_run(geq_context *ctx, const geq_game_graph *graph, co
   return geq_energy_game_run_batch(ctx, 1, graph, initial ? init : nullptr, reach, nr, out);
 }
 
+geq_status geq_energy_game_run_static(geq_context *ctx, const geq_game_graph *graph, const uint32_t *to_reach,
+                                      uint32_t n_to_reach, uint64_t *offsets, uint32_t *data,
+                                      uint64_t data_cap, uint64_t *n_words, geq_solve_stats *stats) {
+  Engine *e;
+  geq_status st = ctx_engine(ctx, e);
+  if (st) return st;
+  if (!graph || !offsets || !n_words) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  if (data_cap && !data) return fail(GEQ_ERR_INVALID_INPUT, "data is NULL with a non-zero data_cap");
+  if ((st = validate_graph(*graph))) return st;
+  if (!to_reach && n_to_reach) return fail(GEQ_ERR_INVALID_INPUT, "to_reach is NULL with a non-zero count");
+  for (uint32_t i = 0; to_reach && i < n_to_reach; i++)
+    if (to_reach[i] >= graph->n_vertices) return fail(GEQ_ERR_INVALID_INPUT, "to_reach index out of range");
+  return e->run_static(ctx->device, *graph, to_reach, n_to_reach, offsets, data, data_cap, n_words, stats);
+}
+
 // ---- TransitionSystem -------------------------------------------------------
 geq_status geq_lts_from_edges(uint64_t n_edges, const uint32_t *src, const uint32_t *dst, const int32_t *label,
                               geq_lts **out) {

@@ -44,6 +44,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <set>
 #include <thread>
 #include <vector>
@@ -2314,6 +2315,377 @@ geq_status Engine::download_selected(DeviceGamesImpl &dg, const std::vector<uint
     sol.data_base[g] = off[k];
     for (uint32_t i = 0; i <= count[g]; i++) sol.offsets.push_back(off[k + i] - off[k]);
     k += count[g];
+  }
+  return GEQ_OK;
+}
+
+// ---- allocation-free solve of one game (geq_energy_game_run_static) -------
+// All device memory of this solve is one file-scope array: the game, its
+// reverse CSR, descriptors, frontiers, control block and energy arena.  One
+// block of BLOCK threads runs the whole solve in one launch -- validation,
+// reverse CSR, initialisation, the rounds (the position routines of k_round,
+// with block barriers between a round and its commit) and the gather of the
+// result lists -- so the call allocates nothing and launches one kernel.
+static __device__ __align__(256) unsigned char g_static_scratch[GEQ_STATIC_SCRATCH_BYTES];
+
+struct StaticArgs {
+  const uint32_t *reach;        // explicit to_reach list, or null: standard reach
+  uint32_t n_reach;
+  uint32_t max_rounds;
+  uint32_t *arena;
+  unsigned long long arena_cap;  // words
+  unsigned long long *out_off;   // n_nodes + 1 result offsets
+};
+// Ctr::pad bits of the static solve
+constexpr uint32_t SERR_COL = 1u, SERR_WEIGHT = 2u, SERR_ARENA = 4u, SERR_ROUNDS = 8u;
+
+// out[v] = sum of cnt(u) for u < v, out[n] = the total; one block.
+template <class T, class F>
+__device__ void block_excl_scan_n(unsigned long long n, F cnt, T *out, unsigned long long *ws) {
+  const uint32_t t = threadIdx.x;
+  const unsigned long long chunk = (n + BLOCK - 1) / BLOCK;
+  const unsigned long long b = min(n, (unsigned long long)t * chunk), e = min(n, b + chunk);
+  unsigned long long sum = 0;
+  for (unsigned long long v = b; v < e; v++) sum += cnt(v);
+  ws[t] = sum;
+  __syncthreads();
+  if (t == 0) {
+    unsigned long long acc = 0;
+    for (int i = 0; i < BLOCK; i++) {
+      const unsigned long long x = ws[i];
+      ws[i] = acc;
+      acc += x;
+    }
+    out[n] = (T)acc;
+  }
+  __syncthreads();
+  unsigned long long acc = ws[t];
+  for (unsigned long long v = b; v < e; v++) {
+    out[v] = (T)acc;
+    acc += cnt(v);
+  }
+  __syncthreads();
+}
+
+template <class Cd>
+__global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, const StaticArgs a) {
+  __shared__ uint32_t smem[WARPS_PER_BLOCK * SM_WORDS];
+  __shared__ uint32_t tscr[WARPS_PER_BLOCK * TSCR * 32];
+  __shared__ unsigned long long ws[BLOCK];
+  __shared__ uint32_t s_err;
+  Ctr *c = p.ctr;
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+  const unsigned long long N = p.n_nodes, M = p.n_edges;
+  uint32_t *rrow = const_cast<uint32_t *>(p.rrow), *rcol = const_cast<uint32_t *>(p.rcol);
+  // -- everything that must start at zero, and the control block
+  if (tid == 0) {
+    Ctr h{};
+    h.arena = a.arena;
+    h.arena_cap = a.arena_cap;
+    h.arena_top = 1;  // word 0: the zero energy
+    h.stamp = 1;
+    *c = h;
+    a.arena[0] = 0u;
+    s_err = 0u;
+  }
+  for (unsigned long long v = tid; v < N; v += BLOCK) {
+    p.desc[v] = 0ull;
+    p.mark[v] = 0u;
+  }
+  __syncthreads();
+  // -- successor ids and update codes (k_indegree, k_check_weights); in-degrees into mark
+  uint32_t bad = 0;
+  for (unsigned long long k = tid; k < M; k += BLOCK) {
+    const uint32_t w = p.col[k];
+    if (w < N) atomicAdd(&p.mark[w], 1u);
+    else bad |= SERR_COL;
+    const uint32_t u = p.wt[k];
+    if (p.el * p.ub < 32u && (u >> (p.el * p.ub)) != 0u) bad |= SERR_WEIGHT;
+    for (uint32_t i = 0; i < p.el; i++)
+      if (((u >> (i * p.ub)) & p.um) > p.el + 1u) bad |= SERR_WEIGHT;
+  }
+  if (bad) atomicOr(&s_err, bad);
+  __syncthreads();
+  if (s_err) {
+    if (tid == 0) c->pad = s_err;
+    return;
+  }
+  // -- reverse CSR: offsets, then predecessors through a cursor kept in mark
+  block_excl_scan_n<uint32_t>(N, [&](unsigned long long v) { return (unsigned long long)p.mark[v]; }, rrow, ws);
+  for (unsigned long long v = tid; v < N; v += BLOCK) p.mark[v] = rrow[v];
+  __syncthreads();
+  for (unsigned long long v = tid; v < N; v += BLOCK)
+    for (uint32_t k = p.row[v]; k < p.row[v + 1]; k++) rcol[atomicAdd(&p.mark[p.col[k]], 1u)] = (uint32_t)v;
+  __syncthreads();
+  for (unsigned long long v = tid; v < N; v += BLOCK) p.mark[v] = 0u;
+  __syncthreads();
+  // -- standard initialisation: {0} at the positions to reach (EnergyGame::with_reach)
+  auto is_reach = [&](unsigned long long v) { return !(p.flags[v] & 1u) && p.row[v + 1] == p.row[v]; };
+  const unsigned long long n_src = a.reach ? a.n_reach : N;
+  for (unsigned long long i = tid; i < n_src; i += BLOCK) {
+    if (a.reach) p.desc[a.reach[i]] = inl_hdr(1u);
+    else if (is_reach(i)) p.desc[i] = inl_hdr(1u);
+  }
+  __syncthreads();
+  uint32_t *sm = smem + warp * SM_WORDS;
+  for (unsigned long long b0 = (unsigned long long)warp * 32u; b0 < n_src; b0 += BLOCK) {
+    const unsigned long long i = b0 + lane;
+    bool f = false;
+    uint32_t v = 0;
+    if (i < n_src) {
+      v = a.reach ? a.reach[i] : (uint32_t)i;
+      f = a.reach ? true : is_reach(i);
+    }
+    push_preds_warp(p, c, sm, v, f, p.front0, &c->fsize[0], c->stamp, lane);
+  }
+  __syncthreads();
+  // -- rounds (k_round + k_commit in one block)
+  uint32_t *scr = tscr + warp * (TSCR * 32) + lane;
+  const Cd cd = make_codec<Cd>(p);
+  uint32_t *arena = a.arena;
+  const unsigned long long cap = a.arena_cap;
+  WarpAlloc wa{0, 0};
+  unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0, t_edges = 0, t_bytes = 0, t_pos = 0;
+  WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes};
+  __shared__ uint32_t s_cur, s_fs, s_stop;
+  for (uint32_t r = 0;; r++) {
+    // one thread decides, so that every warp leaves the loop in the same round
+    if (tid == 0) {
+      s_cur = c->cur;
+      s_fs = c->fsize[s_cur];
+      s_stop = (s_fs == 0u || c->overflow || c->error) ? 1u : (r >= a.max_rounds ? 2u : 0u);
+      if (s_stop == 2u) c->pad = SERR_ROUNDS;
+    }
+    __syncthreads();
+    if (s_stop) break;
+    const uint32_t cur = s_cur, fs = s_fs;
+    const uint32_t *F = cur ? p.front1 : p.front0;
+    uint32_t *NF = cur ? p.front0 : p.front1;
+    uint32_t *nf_size = &c->fsize[cur ^ 1u];
+    const uint32_t stamp = c->stamp + 1u;
+    for (uint32_t base = warp * 32u; base < fs; base += BLOCK) {
+      const uint32_t slot = base + lane;
+      const bool active = slot < fs;
+      const uint32_t v = active ? ld(F, slot, p.n_nodes, c) : 0u;
+      int ts = T_NONE;
+      uint32_t cnt = 0;
+      if (active) ts = p.thread_path ? thread_solve(p, c, cd, arena, cap, v, scr, cnt, t_edges, t_bytes) : T_BIG;
+      if (ts != T_NONE && ts != T_BIG && ts != T_SKIPPED) t_pos++;
+      unsigned long long nd = NONE_DESC;
+      if (ts == T_CHANGED && cnt <= p.inl) {
+        nd = inl_hdr(cnt);
+        for (uint32_t q = 0; q < cnt; q++) nd |= (unsigned long long)SCR(TK + q) << (q * p.ib);
+      }
+      const uint32_t need = (ts == T_CHANGED && cnt > p.inl) ? cnt : 0u;
+      const uint32_t incl = warp_incl_scan(need, lane);
+      const uint32_t total = __shfl_sync(FULL, incl, 31);
+      unsigned long long obase = 0;
+      const bool ok = total == 0u || wa.alloc(total, c, cap, lane, obase);
+      if (need) {
+        if (!ok) {
+          ts = T_OVERFLOW;
+        } else {
+          const unsigned long long off = obase + incl - need;
+          for (uint32_t q = 0; q < need; q++)
+            if (CHECK_IDX(c, off + q, cap)) arena[off + q] = SCR(TK + q);
+          nd = mkdesc(off, need);
+        }
+      }
+      if (ts == T_CHANGED) t_bytes += 4ull * cnt;
+      if (active && ts != T_BIG && CHECK_IDX(c, slot, p.n_nodes)) p.slot_new[slot] = (ts == T_CHANGED) ? nd : NONE_DESC;
+      uint32_t big = __ballot_sync(FULL, ts == T_BIG);
+      bool big_changed = false;
+      while (big) {
+        const uint32_t l = __ffs(big) - 1u;
+        big &= big - 1u;
+        const uint32_t vb = __shfl_sync(FULL, v, l);
+        const Res rs = solve_position(x, cd, vb);
+        if (rs.st != R_SKIPPED) w_pos++;
+        if (lane == 0 && CHECK_IDX(c, base + l, p.n_nodes))
+          p.slot_new[base + l] = (rs.st == R_CHANGED) ? rs.d : NONE_DESC;
+        if (lane == l) big_changed = rs.st == R_CHANGED;
+      }
+      push_preds_warp(p, c, sm, v, ts == T_CHANGED || big_changed, NF, nf_size, stamp, lane);
+    }
+    __syncthreads();
+    for (uint32_t s2 = tid; s2 < fs; s2 += BLOCK) {
+      const unsigned long long d = p.slot_new[s2];
+      if (d != NONE_DESC) {
+        const uint32_t v = F[s2];
+        if (CHECK_IDX(c, v, p.n_nodes)) p.desc[v] = d;
+      }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      c->fsize[cur] = 0u;
+      c->cur = cur ^ 1u;
+      c->stamp = c->stamp + 1u;
+      c->rounds = c->rounds + 1ull;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    t_edges += __shfl_xor_sync(FULL, t_edges, o);
+    t_bytes += __shfl_xor_sync(FULL, t_bytes, o);
+    t_pos += __shfl_xor_sync(FULL, t_pos, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&c->positions, t_pos + w_pos);
+    atomicAdd(&c->edges, t_edges + w_edges);
+    atomicAdd(&c->bytes, t_bytes + w_bytes);
+  }
+  __syncthreads();
+  if (c->overflow) {
+    if (tid == 0) c->pad |= SERR_ARENA;
+    return;
+  }
+  if (c->pad || c->error) return;
+  // -- result lists (k_desc_counts + scan + k_gather) behind the arena's used part
+  block_excl_scan_n<unsigned long long>(N, [&](unsigned long long v) { return (unsigned long long)dcnt(p.desc[v]); },
+                                        a.out_off, ws);
+  const unsigned long long top = c->arena_top, total = a.out_off[N];
+  if (top + total > cap) {
+    if (tid == 0) c->pad = SERR_ARENA;
+    return;
+  }
+  uint32_t *out = arena + top;
+  for (unsigned long long v = warp; v < N; v += WARPS_PER_BLOCK) {
+    const unsigned long long d = p.desc[v];
+    const uint32_t n = dcnt(d);
+    const unsigned long long go = a.out_off[v];
+    for (uint32_t q = lane; q < n; q += 32u)
+      out[go + q] = dinl(d) ? ((uint32_t)(d >> (q * p.ib)) & p.ibm) : arena[doff(d) + q];
+  }
+}
+
+namespace {
+std::mutex g_static_mu;
+void *g_static_ptr[64] = {};
+}  // namespace
+
+// Address of the scratch on `device` (current), looked up once per device.
+static geq_status static_scratch(int device, unsigned char *&out) {
+  if (device < 0 || device >= 64) return fail(GEQ_ERR_NO_DEVICE, "device %d out of range", device);
+  std::lock_guard<std::mutex> g(g_static_mu);
+  if (!g_static_ptr[device]) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(GEQ_ERR_CUDA, "cudaGetSymbolAddress of the static scratch: %s", cudaGetErrorString(e));
+    g_static_ptr[device] = ptr;
+  }
+  out = (unsigned char *)g_static_ptr[device];
+  return GEQ_OK;
+}
+
+geq_status Engine::run_static(int device, const geq_game_graph &g, const uint32_t *to_reach, uint32_t n_reach,
+                              uint64_t *offsets, uint32_t *data, uint64_t data_cap, uint64_t *n_words,
+                              geq_solve_stats *stats) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  int prev = -1;
+  CU(cudaGetDevice(&prev));
+  if (prev != device) CU(cudaSetDevice(device));
+  struct Restore {
+    int prev, dev;
+    ~Restore() { if (prev != dev && prev >= 0) cudaSetDevice(prev); }
+  } restore{prev, device};
+  const Conf conf(g.conf);
+  if (!conf.supported())
+    return fail(GEQ_ERR_UNSUPPORTED, "EnergyConf {%u, %u} is outside the device codecs", conf.elements, conf.max);
+  const unsigned long long N = g.n_vertices, M = g.row_offsets[g.n_vertices];
+  // scratch layout, 256-byte aligned pieces
+  size_t top = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = top;
+    top = (top + std::max<size_t>(bytes, 1) + 255) & ~size_t(255);
+    return o;
+  };
+  const size_t o_ctr = take(sizeof(Ctr)), o_row = take((N + 1) * 4), o_col = take(M * 4), o_wt = take(M * 4),
+               o_flags = take(N), o_reach = take((size_t)n_reach * 4), o_rrow = take((N + 1) * 4),
+               o_rcol = take(M * 4), o_desc = take(N * 8), o_slot = take(N * 8), o_mark = take(N * 4),
+               o_f0 = take(N * 4), o_f1 = take(N * 4), o_out = take((N + 1) * 8);
+  const size_t min_arena = 4096 * 4;
+  if (N >= 0xFFFFFFF0ull || M >= 0xFFFFFFF0ull || top + min_arena > GEQ_STATIC_SCRATCH_BYTES)
+    return fail(GEQ_ERR_UNSUPPORTED,
+                "game of %llu positions / %llu edges needs %zu bytes of the %u-byte static scratch",
+                N, M, top + min_arena, (unsigned)GEQ_STATIC_SCRATCH_BYTES);
+  unsigned char *base = nullptr;
+  geq_status rc = static_scratch(device, base);
+  if (rc) return rc;
+  KParams kp{};
+  kp.row = (const uint32_t *)(base + o_row);
+  kp.col = (const uint32_t *)(base + o_col);
+  kp.wt = (const uint32_t *)(base + o_wt);
+  kp.rrow = (const uint32_t *)(base + o_rrow);
+  kp.rcol = (const uint32_t *)(base + o_rcol);
+  kp.flags = (const uint8_t *)(base + o_flags);
+  kp.desc = (unsigned long long *)(base + o_desc);
+  kp.mark = (uint32_t *)(base + o_mark);
+  kp.front0 = (uint32_t *)(base + o_f0);
+  kp.front1 = (uint32_t *)(base + o_f1);
+  kp.slot_new = (unsigned long long *)(base + o_slot);
+  kp.ctr = (Ctr *)(base + o_ctr);
+  kp.n_nodes = N;
+  kp.n_edges = M;
+  kp.el = conf.elements; kp.mx = conf.max; kp.eb = conf.energy_bits(); kp.em = conf.energy_mask();
+  kp.ub = conf.update_bits(); kp.um = conf.update_mask();
+  kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
+  kp.thread_path = (tuning.flags & (GEQ_TUNE_FORCE_LARGE | GEQ_TUNE_NO_THREAD_PATH)) ? 0u : 1u;
+  kp.ib = conf.elements * conf.energy_bits();
+  kp.ibm = kp.ib >= 32 ? 0xFFFFFFFFu : ((1u << kp.ib) - 1u);
+  kp.inl = std::min<uint32_t>(7u, 60u / kp.ib);
+  StaticArgs sa{};
+  sa.reach = to_reach ? (const uint32_t *)(base + o_reach) : nullptr;
+  sa.n_reach = to_reach ? n_reach : 0u;
+  sa.max_rounds = 1u << 20;
+  sa.arena = (uint32_t *)(base + top);
+  sa.arena_cap = (GEQ_STATIC_SCRATCH_BYTES - top) / 4;
+  sa.out_off = (unsigned long long *)(base + o_out);
+  // the game, straight from the caller's buffers
+  CU(cudaEventRecord(s.ev0, S));
+  CU(cudaMemcpyAsync(base + o_row, g.row_offsets, (N + 1) * 4, cudaMemcpyHostToDevice, S));
+  if (M) {
+    CU(cudaMemcpyAsync(base + o_col, g.column_indices, M * 4, cudaMemcpyHostToDevice, S));
+    CU(cudaMemcpyAsync(base + o_wt, g.weights, M * 4, cudaMemcpyHostToDevice, S));
+  }
+  if (N) CU(cudaMemcpyAsync(base + o_flags, g.attacker_pos, N, cudaMemcpyHostToDevice, S));
+  if (to_reach && n_reach) CU(cudaMemcpyAsync(base + o_reach, to_reach, (size_t)n_reach * 4, cudaMemcpyHostToDevice, S));
+  const bool generic = !conf.standard() || (tuning.flags & GEQ_TUNE_FORCE_GENERIC);
+  if (generic) k_solve_static<CodecGen><<<1, BLOCK, 0, S>>>(kp, sa);
+  else k_solve_static<CodecStd><<<1, BLOCK, 0, S>>>(kp, sa);
+  CU(cudaGetLastError());
+  Ctr h{};
+  CU(cudaMemcpyAsync(&h, kp.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
+  CU(cudaMemcpyAsync(offsets, sa.out_off, (N + 1) * 8, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  if (h.pad & SERR_COL) return fail(GEQ_ERR_INVALID_INPUT, "Node index too high: a successor index is out of range");
+  if (h.pad & SERR_WEIGHT) return fail(GEQ_ERR_INVALID_INPUT, "an edge update names no element or sets padding bits");
+  if (h.error)
+    return fail((h.error & DERR_BOUNDS) ? GEQ_ERR_INTERNAL : GEQ_ERR_OUT_OF_MEMORY, "device error %u (line %u)",
+                h.error, h.err_line);
+  if (h.pad & SERR_ARENA)
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "the energy lists outgrew the static scratch (%llu words)", sa.arena_cap);
+  if (h.pad & SERR_ROUNDS) return fail(GEQ_ERR_TIMEOUT, "no fixpoint after %u rounds", sa.max_rounds);
+  const unsigned long long total = offsets[N];
+  if (n_words) *n_words = total;
+  if (total > data_cap)
+    return fail(GEQ_ERR_INVALID_INPUT, "data_cap %llu is below the %llu result words", (unsigned long long)data_cap,
+                total);
+  if (total) CU(cudaMemcpyAsync(data, sa.arena + h.arena_top, total * 4, cudaMemcpyDeviceToHost, S));
+  CU(cudaEventRecord(s.ev1, S));
+  CU(cudaStreamSynchronize(S));
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s.ev0, s.ev1);
+    *stats = geq_solve_stats{};
+    stats->rounds = h.rounds;
+    stats->positions_computed = h.positions;
+    stats->edges_relaxed = h.edges;
+    stats->algorithmic_bytes = h.bytes;
+    stats->kernel_launches = 1;
+    stats->device_ms = ms;
   }
   return GEQ_OK;
 }

@@ -145,6 +145,10 @@ class Engine {
   // become game g of the solution.
   geq_status download_selected(DeviceGamesImpl &dg, const std::vector<uint32_t> &first,
                                const std::vector<uint32_t> &count, geq_solution &sol);
+  // geq_energy_game_run_static: one game in the file-scope scratch, no allocation.
+  geq_status run_static(int device, const geq_game_graph &g, const uint32_t *to_reach, uint32_t n_reach,
+                        uint64_t *offsets, uint32_t *data, uint64_t data_cap, uint64_t *n_words,
+                        geq_solve_stats *stats);
   // Node id of game g's first position inside the uploaded batch.
   static uint64_t game_node_base(const DeviceGamesImpl &dg, uint32_t g);
   geq_tuning tuning{};

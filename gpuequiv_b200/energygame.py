@@ -324,6 +324,36 @@ def run_batch_raw(graphs: Sequence[GameGraph], context: Context | None = None, v
     return offs, data, stats
 
 
+def run_static(graph: GameGraph, context: Context | None = None, to_reach=None, data_cap: int | None = None):
+    """geq_energy_game_run_static: one game solved inside the library's
+    file-scope device scratch, with no allocation in the call.  Returns
+    (offsets, data, stats) like one game of run_batch_raw; to_reach None means
+    standard reach.  If the result outgrows data_cap the call is repeated
+    with the size it reported."""
+    ctx = context or default_context()
+    n = graph.n_vertices()
+    view = graph.c_view()
+    reach = None if to_reach is None else np.ascontiguousarray(to_reach, dtype=np.uint32)
+    rp = None if reach is None else reach.ctypes.data_as(C.POINTER(C.c_uint32))
+    nr = 0 if reach is None else len(reach)
+    offs = np.zeros(n + 1, np.uint64)
+    cap = 4 * n + 64 if data_cap is None else int(data_cap)
+    for _ in range(2):
+        data = np.zeros(max(cap, 1), np.uint32)
+        nw = C.c_uint64(0)
+        st = geq_solve_stats()
+        status = lib.geq_energy_game_run_static(ctx.h, C.byref(view), rp, nr,
+                                                offs.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                                data.ctypes.data_as(C.POINTER(C.c_uint32)), cap, C.byref(nw),
+                                                C.byref(st))
+        if status == 3 and nw.value > cap and data_cap is None:  # INVALID_INPUT: data_cap too small
+            cap = int(nw.value)
+            continue
+        check(status)
+        return offs, data[:nw.value], st.as_dict()
+    check(status)
+
+
 def c_views(graphs: Sequence[GameGraph]):
     """geq_game_graph array of the graphs (keep the graphs alive)."""
     return (geq_game_graph * len(graphs))(*[g.c_view() for g in graphs])

@@ -170,6 +170,39 @@ geq_status geq_energy_game_run(geq_context *ctx, const geq_game_graph *graph,
                                const geq_energy_lists *initial, const uint32_t *to_reach,
                                uint32_t n_to_reach, geq_solution **out);
 
+/* geq_energy_game_run_static: geq_energy_game_run for one game with no initial
+ * lists, computed without allocating any memory -- no cudaMalloc/cudaFree, no
+ * page-locked or heap buffers, no CUDA graph.  The game, its reverse CSR, the
+ * energy lists and the frontiers live in one file-scope device array of
+ * GEQ_STATIC_SCRATCH_BYTES per device, and one single-block kernel runs the
+ * whole solve.  For callers that cannot allocate device memory when they
+ * solve: a process whose own allocator has reserved the device's memory (a
+ * serving framework or caching allocator that preallocates HBM, where a
+ * cudaMalloc fails), and latency-bound callers whose other streams would be
+ * stalled by the implicit device-wide synchronisation of cudaFree.
+ *
+ * to_reach: NULL = standard reach (EnergyGame::standard_reach), else the
+ *   n_to_reach positions that start with {0}.
+ * offsets (n_vertices + 1 entries) and data (data_cap words) receive the
+ *   lists in the layout of geq_energy_lists; *n_words = result words, set
+ *   also when data_cap is too small (then GEQ_ERR_INVALID_INPUT and data is
+ *   not written).  After any other error offsets and data are unspecified.
+ * Limit: 45 bytes per position + 12 per edge of the scratch hold the game;
+ *   the rest (at least 16 KiB) holds the energy lists.  A larger game gives
+ *   GEQ_ERR_UNSUPPORTED, lists that outgrow the rest GEQ_ERR_OUT_OF_MEMORY.
+ * The scratch address is looked up (cudaGetSymbolAddress) by the first call
+ * per device, with the context's device current: make that first call
+ * before any stream capture.  All contexts of a device share the scratch:
+ * calls that overlap in time on one device race on it, so the caller must
+ * serialise them.
+ * No counterpart in the reference, whose runs create their buffers per run
+ * (GPURunner::with_game and the shader constructors, energygame.rs:1442,
+ * :507-540). */
+#define GEQ_STATIC_SCRATCH_BYTES (16u << 20)
+geq_status geq_energy_game_run_static(geq_context *ctx, const geq_game_graph *graph, const uint32_t *to_reach,
+                                      uint32_t n_to_reach, uint64_t *offsets, uint32_t *data,
+                                      uint64_t data_cap, uint64_t *n_words, geq_solve_stats *stats);
+
 /* Many independent games solved together in one set of device rounds (the
  * batched form; no reference counterpart beyond calling EnergyGame::run once
  * per game).  initial / to_reach / n_to_reach are arrays of n_games entries;
