@@ -41,26 +41,51 @@ struct CodecStd {
     return (p0 ^ p1 ^ p2) | (p1 << 1);
   }
   // Inverse of the edge update u (4-bit codes: 0 Zero, 1 Decrement, k+2 =
-  // Min into element k).  All decrements first, then the merges in index
-  // order, exactly as UPDATE1 followed by UPDATE_MIN.
-  __host__ __device__ __forceinline__ uint32_t upd(uint32_t t, uint32_t u) const {
-    if (u == 0) return t;
-    uint32_t lod = 0;
-#pragma unroll
-    for (int i = 0; i < 6; i++)
-      if (((u >> (4 * i)) & 15u) == 1u) lod |= 1u << (2 * i);
-    // v -> min(v+1, 3): plane 0 becomes 1, plane 1 takes plane 0, plane 2 takes plane 1.
-    t = t | lod | ((t & lod) << 1) | ((t & (lod << 1)) << 11);
-#pragma unroll
-    for (int i = 0; i < 6; i++) {
-      uint32_t c = (u >> (4 * i)) & 15u;
-      if (c >= 2u) {
-        uint32_t tg = c - 2u;
-        if (tg < 6u) t |= ((t >> (2 * i)) & 0x1003u) << (2 * tg);
+  // Min into element k): all decrements first, then the merges in index
+  // order, exactly as UPDATE1 followed by UPDATE_MIN.  An update is decoded
+  // once per edge (prep) and applied to each energy of the successor's list
+  // (apply): `lod` = plane-0 bits of the decremented fields, `mg` = the
+  // merges as (2*source, 2*target) nibble pairs in index order.
+  struct Upd {
+    uint32_t lod, nm;
+    unsigned long long mg;
+  };
+  __host__ __device__ __forceinline__ Upd prep(uint32_t u) const {
+    Upd q{0u, 0u, 0ull};
+    // fields whose code is 1: bit 4i of z, then moved to bit 2i
+    const uint32_t x = u ^ 0x111111u;
+    uint32_t z = ~(x | (x >> 1) | (x >> 2) | (x >> 3)) & 0x111111u;
+    z = (z & ~0x101010u) | ((z & 0x101010u) >> 2);
+    z = (z & ~0x000500u) | ((z & 0x000500u) >> 4);
+    z = (z & ~0x050000u) | ((z & 0x050000u) >> 8);
+    q.lod = z;
+    // fields whose code is >= 2
+    uint32_t m = ((u >> 1) | (u >> 2) | (u >> 3)) & 0x111111u;
+    while (m) {
+#ifdef __CUDA_ARCH__
+      const uint32_t b = (uint32_t)__ffs((int)m) - 1u;
+#else
+      const uint32_t b = (uint32_t)__builtin_ctz(m);
+#endif
+      m &= m - 1u;
+      const uint32_t i = b >> 2, tg = ((u >> b) & 15u) - 2u;
+      if (tg < 6u) {
+        q.mg |= (unsigned long long)((2u * i) | ((2u * tg) << 4)) << (8u * q.nm);
+        q.nm++;
       }
+    }
+    return q;
+  }
+  __host__ __device__ __forceinline__ uint32_t apply(uint32_t t, const Upd &q) const {
+    // v -> min(v+1, 3): plane 0 becomes 1, plane 1 takes plane 0, plane 2 takes plane 1.
+    t = t | q.lod | ((t & q.lod) << 1) | ((t & (q.lod << 1)) << 11);
+    for (uint32_t k = 0; k < q.nm; k++) {
+      const uint32_t e = (uint32_t)(q.mg >> (8u * k));
+      t |= ((t >> (e & 15u)) & 0x1003u) << ((e >> 4) & 15u);
     }
     return t;
   }
+  __host__ __device__ __forceinline__ uint32_t upd(uint32_t t, uint32_t u) const { return apply(t, prep(u)); }
 };
 
 struct CodecGen {
@@ -92,6 +117,9 @@ struct CodecGen {
     }
     return p;
   }
+  using Upd = uint32_t;
+  __host__ __device__ __forceinline__ Upd prep(uint32_t u) const { return u; }
+  __host__ __device__ __forceinline__ uint32_t apply(uint32_t t, Upd u) const { return upd(t, u); }
   __host__ __device__ __forceinline__ uint32_t upd(uint32_t t, uint32_t u) const {
     if (u == 0) return t;
     for (uint32_t i = 0; i < el; i++) {

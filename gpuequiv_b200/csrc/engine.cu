@@ -99,17 +99,28 @@ struct Ctr {
   uint32_t pad;
   unsigned long long positions, edges, bytes, rounds;
 #if GEQ_PATH_PROFILE
-  unsigned long long prof[16];
+  unsigned long long prof[32];
 #endif
 };
 #if GEQ_PATH_PROFILE
 enum : int {
   PF_CYC_THREAD, PF_CYC_BIG, PF_CYC_PUSH, PF_T_ATT, PF_T_DEF, PF_B_ATT, PF_B_DEF, PF_T_CAND, PF_T_DEG,
-  PF_SKIP, PF_SLOTS, PF_CYC_ALL, PF_ITERS, PF_T_UNCH, PF_B_DEG, PF_PUSHED
+  PF_SKIP, PF_SLOTS, PF_CYC_ALL, PF_ITERS, PF_T_UNCH, PF_B_DEG, PF_PUSHED,
+  // warp routines: calls and cycles (lane 0, straight into Ctr::prof)
+  PF_AS_N, PF_AS_C, PF_AB_N, PF_AB_C, PF_D1_N, PF_D1_C, PF_DS_N, PF_DS_C, PF_DB_N, PF_DB_C, PF_DK_N, PF_DK_C,
+  PF_DT_N, PF_DT_C
 };
+#define PROF_WARP(c, n_idx, t0)                                           \
+  do {                                                                    \
+    if ((threadIdx.x & 31u) == 0) {                                       \
+      atomicAdd(&(c)->prof[n_idx], 1ull);                                 \
+      atomicAdd(&(c)->prof[(n_idx) + 1], (unsigned long long)(clock64() - (t0))); \
+    }                                                                     \
+  } while (0)
 #define PROF_ADD(i, v) prof_acc[i] += (v)
 #else
 #define PROF_ADD(i, v) ((void)0)
+#define PROF_WARP(c, n_idx, t0) ((void)0)
 #endif
 
 struct KParams {
@@ -301,12 +312,50 @@ struct WarpCtx {
   uint32_t *sm;
   WarpAlloc &wa;
   unsigned long long &edges, &bytes;
+  uint32_t *scr;  // this lane's scratch column (free while the warp routines run)
   __device__ __forceinline__ uint32_t elem(unsigned long long d, uint32_t q) const {
     return lelem(d, q, arena, cap, c, p.ib, p.ibm);
   }
 };
 
 // Successor of edge k: its update and list descriptor (lane-local).
+// ---- antichains in lane-private shared-memory columns ----------------------
+constexpr uint32_t TK = 16;   // antichain members per column
+constexpr uint32_t TD = 16;   // successors per lane
+constexpr uint32_t TW = 64;   // candidates (attacker) / combinations per step (defender)
+constexpr int TSCR = 2 * TK;  // scratch words per lane: two antichain columns
+enum : int { T_NONE = 0, T_UNCHANGED = 1, T_CHANGED = 2, T_SKIPPED = 3, T_BIG = 4, T_OVERFLOW = 5 };
+
+// scratch column of this lane: word i at scr[i * 32]
+#define SCR(i) scr[(uint32_t)(i) * 32u]
+
+// Insert thermometer code x into the antichain at column words [b, b+n).
+// om bit k: member k equals an own energy (the attacker's tie rule keeps the
+// own copy, the later one).  false if the antichain would exceed TK members.
+__device__ __forceinline__ bool ac_insert(uint32_t *scr, uint32_t b, uint32_t &n, uint32_t &om, uint32_t x,
+                                          bool own) {
+  uint32_t j = 0, om2 = 0;
+  for (uint32_t k = 0; k < n; k++) {
+    const uint32_t a = SCR(b + k);
+    if ((a & ~x) == 0u) {
+      // a <= x: x is not minimal.  No member was removed before this one:
+      // a member above x would be above a, and members form an antichain.
+      if (own && a == x) om |= 1u << k;
+      return true;
+    }
+    if ((x & ~a) != 0u) {  // a is not above x: keep it
+      if (j != k) SCR(b + j) = a;
+      om2 |= ((om >> k) & 1u) << j;
+      j++;
+    }
+  }
+  if (j >= TK) return false;
+  SCR(b + j) = x;
+  om = om2 | ((own ? 1u : 0u) << j);
+  n = j + 1;
+  return true;
+}
+
 struct EdgeInfo {
   uint32_t u, cw;
   unsigned long long d;
@@ -654,6 +703,70 @@ __device__ Res defend_small(const WarpCtx &x, const Cd &cd, unsigned long long e
   return warp_store(x, np, lane < s, lane, s);
 }
 
+// Defender fold across the warp: lane l folds the updated lists of
+// successors l, l+32, ... into an antichain in its scratch column, then the
+// lanes' antichains are combined pairwise in five steps.  The suprema fold
+// is associative and commutative once minimised, so the result is the set of
+// minimal suprema of the reference's sequential fold.  fits = false when an
+// antichain outgrows TK members or one combination step TW pairs.
+template <class Cd>
+__device__ Res defend_tree(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
+                           unsigned long long dv, bool &fits) {
+  const uint32_t lane = x.lane;
+  uint32_t *scr = x.scr;
+  uint32_t n = 0, om = 0, tot = 0;
+  bool ok = true, first = true;
+  for (unsigned long long k = e0 + lane; k < e1; k += 32) {
+    const EdgeInfo e = edge_info(x, k);
+    tot += e.cw;
+    if (!ok) continue;
+    const auto pu = cd.prep(e.u);
+    if (first) {
+      for (uint32_t q = 0; q < e.cw && ok; q++) ok = ac_insert(scr, 0, n, om, cd.apply(cd.to_t(x.elem(e.d, q)), pu), false);
+      first = false;
+    } else if (n * e.cw > TW) {
+      ok = false;
+    } else {
+      uint32_t nn = 0;
+      for (uint32_t q = 0; q < e.cw && ok; q++) {
+        const uint32_t bq = cd.apply(cd.to_t(x.elem(e.d, q)), pu);
+        for (uint32_t i = 0; i < n && ok; i++) ok = ac_insert(scr, TK, nn, om, SCR(i) | bq, false);
+      }
+      for (uint32_t q = 0; q < nn && ok; q++) SCR(q) = SCR(TK + q);
+      n = nn;
+    }
+  }
+  fits = false;
+  if (__any_sync(FULL, !ok)) return Res{R_UNCHANGED, 0};
+  const uint32_t dl = (uint32_t)min(32ull, e1 - e0);
+  for (uint32_t st = 1; st < dl; st <<= 1) {
+    __syncwarp();
+    const uint32_t np = __shfl_down_sync(FULL, n, st);
+    if ((lane & (2u * st - 1u)) == 0u && lane + st < dl) {
+      if (n * np > TW) {
+        ok = false;
+      } else {
+        uint32_t nn = 0;
+        for (uint32_t j = 0; j < np && ok; j++) {
+          const uint32_t b = scr[st + j * 32u];  // partner lane's column
+          for (uint32_t i = 0; i < n && ok; i++) ok = ac_insert(scr, TK, nn, om, SCR(i) | b, false);
+        }
+        for (uint32_t q = 0; q < nn && ok; q++) SCR(q) = SCR(TK + q);
+        n = nn;
+      }
+    }
+    if (__any_sync(FULL, !ok)) return Res{R_UNCHANGED, 0};
+  }
+  __syncwarp();
+  fits = true;
+  x.bytes += 16ull * (e1 - e0) + 4ull * __reduce_add_sync(FULL, tot);
+  const uint32_t r = __shfl_sync(FULL, n, 0);
+  const uint32_t np = lane < r ? cd.to_p((scr - lane)[lane * 32u]) : 0u;  // word `lane` of lane 0's column
+  __syncwarp();
+  if (!differs_small(x, np, r, dv)) return Res{R_UNCHANGED, 0};
+  return warp_store(x, np, lane < r, lane, r);
+}
+
 // STANDARD defender with large lists: intersect the up-closures of the
 // updated successor lists in a 4096-bit set, then take its minimal members.
 __device__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0, unsigned long long e1,
@@ -788,15 +901,18 @@ __device__ Res solve_position(const WarpCtx &x, const Cd &cd, uint32_t v) {
   const unsigned long long dv = ld(x.p.desc, v, x.p.n_nodes, x.c);
   const bool attacker = ld(x.p.flags, v, x.p.n_nodes, x.c) & 1u;
   if (d == 0) return Res{R_SKIPPED, 0};
+#if GEQ_PATH_PROFILE
+  const long long t0 = clock64();
+#endif
   if (attacker) {
     x.edges += d;
     x.bytes += 12ull + 4ull * dcnt(dv);
     if (d <= 32u && x.p.small_limit > 0) {
       bool fits = false;
       const Res r = attack_small(x, cd, e0, d, dv, fits);
-      if (fits) return r;
+      if (fits) { PROF_WARP(x.c, PF_AS_N, t0); return r; }
     }
-    if constexpr (Cd::kBitmap) return attack_bitmap(x, cd, e0, e1, dv);
+    if constexpr (Cd::kBitmap) { const Res r = attack_bitmap(x, cd, e0, e1, dv); PROF_WARP(x.c, PF_AB_N, t0); return r; }
     else return attack_list(x, cd, e0, e1, dv);
   }
   // defender: skipped while a successor has no energies (energygame.rs:789-792)
@@ -809,37 +925,40 @@ __device__ Res solve_position(const WarpCtx &x, const Cd &cd, uint32_t v) {
     }
     if (__ballot_sync(FULL, e)) { empty = true; break; }
   }
-  if (empty) return Res{R_SKIPPED, 0};
+  if (empty) { PROF_WARP(x.c, PF_DK_N, t0); return Res{R_SKIPPED, 0}; }
   x.edges += d;
   x.bytes += 12ull;
   if (d == 1u) {
     EdgeInfo e{0, 0, 0};
     if (lane == 0) e = edge_info(x, e0);
-    return defend_single(x, cd, shfl_edge(e, 0), dv);
+    const Res r = defend_single(x, cd, shfl_edge(e, 0), dv);
+    PROF_WARP(x.c, PF_D1_N, t0);
+    return r;
+  }
+  if (x.p.small_limit > 0) {
+    bool fits = false;
+    const Res r = defend_tree(x, cd, e0, e1, dv, fits);
+    if (fits) { PROF_WARP(x.c, PF_DT_N, t0); return r; }
   }
   if (d <= 32u && x.p.small_limit > 0) {
     bool fits = false;
     const Res r = defend_small(x, cd, e0, d, dv, fits);
-    if (fits) return r;
+    if (fits) { PROF_WARP(x.c, PF_DS_N, t0); return r; }
   }
-  if constexpr (Cd::kBitmap) return defend_bitmap(x, cd, e0, e1, dv);
+  if constexpr (Cd::kBitmap) { const Res r = defend_bitmap(x, cd, e0, e1, dv); PROF_WARP(x.c, PF_DB_N, t0); return r; }
   else return defend_list(x, cd, e0, e1, dv);
 }
 
 // ---- thread path: one lane per small position -----------------------------
 // Most positions have a handful of successors with one or two energies each.
-// Every lane of a warp solves its own such position with the same rules as
-// the warp routines above, keeping candidates in a lane-private column of
-// shared memory; positions beyond TD successors or TK candidates go to the
-// warp routines.
-constexpr uint32_t TK = 16;   // candidates (and combinations) per lane
-constexpr uint32_t TD = 16;   // successors per lane
-constexpr int TSCR = 2 * TK;  // scratch words per lane: [0,TK) work set, [TK,2TK) result
-enum : int { T_NONE = 0, T_UNCHANGED = 1, T_CHANGED = 2, T_SKIPPED = 3, T_BIG = 4, T_OVERFLOW = 5 };
-
-// scratch column of this lane: word i at scr[i * 32]
-#define SCR(i) scr[(uint32_t)(i) * 32u]
-
+// Every lane of a warp solves its own such position.  Candidates stream into
+// an antichain held in a lane-private column of shared memory (bank = lane):
+// a candidate is dropped when a member lies below or equals it, and removes
+// the members above it.  What remains is the set of minimal candidates
+// whatever the insertion order, so the lists equal the reference's as sets
+// (the order inside a list may differ).  Positions beyond TD successors, TK
+// members or TW candidates (per defender step: combinations) go to the warp
+// routines.
 template <class Cd>
 __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32_t *arena, unsigned long long cap,
                             uint32_t v, uint32_t *scr, uint32_t &out_cnt, unsigned long long &edges,
@@ -852,9 +971,10 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
   const uint32_t cv = dcnt(dv);
   const bool attacker = ld(p.flags, v, p.n_nodes, c) & 1u;
   if (attacker) {
-    // attack_update.wgsl + attack_minimize.wgsl, one lane
+    // attack_update.wgsl + attack_minimize.wgsl: successor candidates, then
+    // the own energies; changed iff a minimal value has no own copy
     if (cv > TK) return T_BIG;
-    uint32_t k = 0;
+    uint32_t n = 0, om = 0, tot = 0;
     for (uint32_t j0 = 0; j0 < d; j0 += 4) {
       uint32_t w[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
       unsigned long long dw[4] = {0, 0, 0, 0};
@@ -871,34 +991,20 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
       for (int t = 0; t < 4; t++)
         if (j0 + t < d) {
           const uint32_t cw = dcnt(dw[t]);
-          if (k + cw + cv > TK) return T_BIG;
-          for (uint32_t q = 0; q < cw; q++) SCR(k++) = cd.upd(cd.to_t(lelem(dw[t], q, arena, cap, c, p.ib, p.ibm)), u[t]);
+          tot += cw;
+          if (tot > TW) return T_BIG;
+          const auto pu = cd.prep(u[t]);
+          for (uint32_t q = 0; q < cw; q++)
+            if (!ac_insert(scr, 0, n, om, cd.apply(cd.to_t(lelem(dw[t], q, arena, cap, c, p.ib, p.ibm)), pu), false))
+              return T_BIG;
         }
     }
-    const uint32_t tot = k;
-    for (uint32_t q = 0; q < cv; q++) SCR(k++) = cd.to_t(lelem(dv, q, arena, cap, c, p.ib, p.ibm));
-    const uint32_t K = k;
-    uint32_t keep = 0;
-    bool changed = false;
-    for (uint32_t i = 0; i < K; i++) {
-      const uint32_t ci = SCR(i);
-      bool kill = false;
-      for (uint32_t j = 0; j < K && !kill; j++) {
-        if (j == i) continue;
-        const uint32_t cj = SCR(j);
-        kill = (cj == ci) ? (i < j) : t_leq(cj, ci);
-      }
-      if (!kill) {
-        keep |= 1u << i;
-        if (i < tot) changed = true;
-      }
-    }
+    for (uint32_t q = 0; q < cv; q++)
+      if (!ac_insert(scr, 0, n, om, cd.to_t(lelem(dv, q, arena, cap, c, p.ib, p.ibm)), true)) return T_BIG;
     edges += d;
     bytes += 12ull + 4ull * cv + 16ull * d + 4ull * tot;
-    if (!changed) return T_UNCHANGED;
-    uint32_t n = 0;
-    for (uint32_t i = 0; i < K; i++)
-      if (keep & (1u << i)) SCR(TK + n++) = cd.to_p(SCR(i));
+    if (om == (1u << n) - 1u) return T_UNCHANGED;
+    for (uint32_t q = 0; q < n; q++) SCR(TK + q) = cd.to_p(SCR(q));
     out_cnt = n;
     return T_CHANGED;
   }
@@ -916,44 +1022,45 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
   {
     const uint32_t w0 = ld(p.col, e0, p.n_edges, c), u0 = ld(p.wt, e0, p.n_edges, c);
     const unsigned long long d0 = ld(p.desc, w0, p.n_nodes, c);
-    uint32_t s = dcnt(d0);
-    if (s > TK) return T_BIG;
+    const uint32_t s = dcnt(d0);
+    const auto pu0 = cd.prep(u0);
     unsigned long long tot = s;
     if (d == 1) {
       // single successor: its updated list as is (defend_iterative.wgsl:301-313)
-      for (uint32_t q = 0; q < s; q++) SCR(TK + q) = cd.to_p(cd.upd(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), u0));
+      if (s > TK) return T_BIG;
+      for (uint32_t q = 0; q < s; q++)
+        SCR(TK + q) = cd.to_p(cd.apply(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), pu0));
       n = s;
     } else {
-      for (uint32_t q = 0; q < s; q++) SCR(q) = cd.upd(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), u0);
+      // fold of pairwise suprema, minimised after every step
+      // (defend_iterative.wgsl:243-258, 283-368); the first list minimised
+      // too, which leaves the minimal suprema unchanged
+      if (s > TW) return T_BIG;
+      uint32_t sb = 0, nb = TK, ns = 0, om = 0;
+      for (uint32_t q = 0; q < s; q++)
+        if (!ac_insert(scr, sb, ns, om, cd.apply(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), pu0), false))
+          return T_BIG;
       for (uint32_t j = 1; j < d; j++) {
         const uint32_t w = ld(p.col, (unsigned long long)e0 + j, p.n_edges, c);
         const uint32_t u = ld(p.wt, (unsigned long long)e0 + j, p.n_edges, c);
         const unsigned long long db = ld(p.desc, w, p.n_nodes, c);
         const uint32_t cb = dcnt(db);
         tot += cb;
-        const uint32_t combos = s * cb;
-        if (combos > TK) return T_BIG;
-        for (uint32_t l = 0; l < combos; l++)
-          SCR(TK + l) = SCR(l % s) | cd.upd(cd.to_t(lelem(db, l / s, arena, cap, c, p.ib, p.ibm)), u);
-        // minimise; equal combinations keep the lowest index (defend_iterative.wgsl:243-258)
-        uint32_t keep = 0;
-        for (uint32_t l = 0; l < combos; l++) {
-          const uint32_t cl = SCR(TK + l);
-          bool kill = false;
-          for (uint32_t m = 0; m < combos && !kill; m++) {
-            if (m == l) continue;
-            const uint32_t cm = SCR(TK + m);
-            kill = (cm == cl) ? (l > m) : t_leq(cm, cl);
-          }
-          if (!kill) keep |= 1u << l;
+        if (ns * cb > TW) return T_BIG;
+        const auto pu = cd.prep(u);
+        uint32_t nn = 0;
+        for (uint32_t q = 0; q < cb; q++) {
+          const uint32_t bq = cd.apply(cd.to_t(lelem(db, q, arena, cap, c, p.ib, p.ibm)), pu);
+          for (uint32_t k = 0; k < ns; k++)
+            if (!ac_insert(scr, nb, nn, om, SCR(sb + k) | bq, false)) return T_BIG;
         }
-        uint32_t ns = 0;
-        for (uint32_t l = 0; l < combos; l++)
-          if (keep & (1u << l)) SCR(ns++) = SCR(TK + l);
-        s = ns;
+        const uint32_t t = sb;
+        sb = nb;
+        nb = t;
+        ns = nn;
       }
-      for (uint32_t q = 0; q < s; q++) SCR(TK + q) = cd.to_p(SCR(q));
-      n = s;
+      for (uint32_t q = 0; q < ns; q++) SCR(TK + q) = cd.to_p(SCR(sb + q));
+      n = ns;
     }
     edges += d;
     bytes += 12ull + 16ull * d + 4ull * tot;
@@ -1051,7 +1158,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
   WarpAlloc wa{0, 0};
   unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0;  // warp routines (lane-uniform)
   unsigned long long t_edges = 0, t_bytes = 0, t_pos = 0;  // thread path (per lane)
-  WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes};
+  WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes, scr};
 #if GEQ_PATH_PROFILE
   unsigned long long prof_acc[16] = {};
   const long long t_all0 = clock64();
@@ -2200,7 +2307,7 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
   dg.next_stamp = c.stamp + 2u;
 #if GEQ_PATH_PROFILE
   std::fprintf(stderr, "GEQ_PROF");
-  for (int i = 0; i < 16; i++) std::fprintf(stderr, " %llu", c.prof[i]);
+  for (int i = 0; i < 32; i++) std::fprintf(stderr, " %llu", c.prof[i]);
   std::fprintf(stderr, "\n");
 #endif
   if (stats) {
@@ -2446,7 +2553,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
   const unsigned long long cap = a.arena_cap;
   WarpAlloc wa{0, 0};
   unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0, t_edges = 0, t_bytes = 0, t_pos = 0;
-  WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes};
+  WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes, scr};
   __shared__ uint32_t s_cur, s_fs, s_stop;
   for (uint32_t r = 0;; r++) {
     // one thread decides, so that every warp leaves the loop in the same round

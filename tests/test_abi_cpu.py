@@ -216,6 +216,18 @@ int main() {
   for (uint32_t u : ups)
     for (uint32_t p = 0; p < 4096; p++)
       std::printf("%u %u %u %u\n", u, p, s.to_p(s.upd(s.to_t(p), u)), g.to_p(g.upd(g.to_t(p), u)));
+  // pseudo-random valid STANDARD updates (every field code 0..7)
+  uint32_t r = 12345u;
+  for (int k = 0; k < 48; k++) {
+    uint32_t u = 0;
+    for (int i = 0; i < 6; i++) {
+      r = r * 1664525u + 1013904223u;
+      const uint32_t c = (r >> 24) % 10u;
+      u |= (c < 8u ? c : 0u) << (4 * i);
+    }
+    for (uint32_t p = 0; p < 4096; p++)
+      std::printf("%u %u %u %u\n", u, p, s.to_p(s.upd(s.to_t(p), u)), g.to_p(g.upd(g.to_t(p), u)));
+  }
   // order: (a & ~b) == 0 iff field-wise <=
   for (uint32_t a = 0; a < 4096; a += 7)
     for (uint32_t b = 0; b < 4096; b += 5) {
