@@ -97,6 +97,8 @@ struct Ctr {
   uint32_t err_line;
   uint32_t done_blocks;
   uint32_t pad;
+  uint32_t next_slot;  // k_round: next frontier slot to hand out (32 per grab)
+  uint32_t pad2;
   unsigned long long positions, edges, bytes, rounds;
 #if GEQ_PATH_PROFILE
   unsigned long long prof[32];
@@ -136,6 +138,9 @@ struct KParams {
   uint32_t small_limit;
   uint32_t thread_path;  // 1: lane-per-position path for small positions
   uint32_t ib, ibm, inl; // inline descriptors: bits per energy, its mask, capacity
+  uint32_t mwords;       // words of one half of the frontier bitmap `mark`
+  uint32_t *fpart;       // per-block set-bit counts of the bitmap (k_fcount)
+  uint32_t fblocks;      // blocks of k_fcount / k_ffill
 };
 
 // Energy-list descriptors (one u64 per position):
@@ -487,7 +492,7 @@ __device__ Res attack_small(const WarpCtx &x, const Cd &cd, unsigned long long e
 
 // Large attacker positions on STANDARD: candidates go into a 4096-bit set;
 // minimal members = set minus the strict up-closure of the set.
-__device__ Res attack_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0, unsigned long long e1,
+__device__ __noinline__ Res attack_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0, unsigned long long e1,
                              unsigned long long dv) {
   const uint32_t lane = x.lane;
   const uint32_t cv = dcnt(dv);
@@ -526,7 +531,7 @@ __device__ Res attack_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long
 // Large attacker positions on other confs: candidates in arena scratch,
 // pairwise minimisation (same tie rule).
 template <class Cd>
-__device__ Res attack_list(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
+__device__ __noinline__ Res attack_list(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
                            unsigned long long dv) {
   const uint32_t lane = x.lane;
   const uint32_t cv = dcnt(dv);
@@ -658,7 +663,7 @@ __device__ Res defend_single(const WarpCtx &x, const Cd &cd, const EdgeInfo &e, 
 // Fold of up to 32 successors whose pairwise combinations stay <= 32: the
 // running antichain lives in one register per lane.
 template <class Cd>
-__device__ Res defend_small(const WarpCtx &x, const Cd &cd, unsigned long long e0, uint32_t d,
+__device__ __noinline__ Res defend_small(const WarpCtx &x, const Cd &cd, unsigned long long e0, uint32_t d,
                             unsigned long long dv, bool &fits) {
   const uint32_t lane = x.lane;
   EdgeInfo ei{0, 0, 0};
@@ -769,7 +774,7 @@ __device__ Res defend_tree(const WarpCtx &x, const Cd &cd, unsigned long long e0
 
 // STANDARD defender with large lists: intersect the up-closures of the
 // updated successor lists in a 4096-bit set, then take its minimal members.
-__device__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0, unsigned long long e1,
+__device__ __noinline__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long long e0, unsigned long long e1,
                              unsigned long long dv) {
   const uint32_t lane = x.lane;
   const uint32_t cv = dcnt(dv);
@@ -815,7 +820,7 @@ __device__ Res defend_bitmap(const WarpCtx &x, const CodecStd &cd, unsigned long
 // Other confs with large lists: the fold of defend_iterative.wgsl with the
 // running list and the combinations in arena scratch.
 template <class Cd>
-__device__ Res defend_list(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
+__device__ __noinline__ Res defend_list(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
                            unsigned long long dv) {
   const uint32_t lane = x.lane;
   const uint32_t cv = dcnt(dv);
@@ -1078,11 +1083,21 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
   return T_CHANGED;
 }
 
-// Append predecessors to the next frontier once.  The reverse-CSR ranges of
-// all flagged lanes are concatenated and walked 32 entries at a time, so a
-// position with many predecessors is spread over the whole warp.
-__device__ void push_preds_warp(const KParams &p, Ctr *c, uint32_t *sm, uint32_t v, bool flagged, uint32_t *NF,
-                                uint32_t *nf_size, uint32_t stamp, uint32_t lane) {
+// The next frontier is a bitmap: one bit per position in each of two halves
+// of `mark`, chosen by the parity of the stamp of the round that pushes.
+// k_fcount / k_ffill turn the half into the frontier list in position order
+// after the round, and k_commit clears the half that the round after next
+// uses.  The bitmap (N/16 bytes) stays in L2.
+__device__ __forceinline__ void mark_push(const KParams &p, uint32_t u, uint32_t stamp) {
+  atomicOr(p.mark + (stamp & 1u) * p.mwords + (u >> 5), 1u << (u & 31u));
+}
+
+// Put the predecessors of the flagged lanes' positions into the next
+// frontier.  The reverse-CSR ranges of all flagged lanes are concatenated and
+// walked 32 entries at a time, so a position with many predecessors is spread
+// over the whole warp.
+__device__ void push_preds_warp(const KParams &p, Ctr *c, uint32_t *sm, uint32_t v, bool flagged, uint32_t stamp,
+                                uint32_t lane) {
   uint32_t b = 0, n = 0;
   if (flagged) {
     b = ld(p.rrow, v, p.n_nodes + 1, c);
@@ -1096,8 +1111,6 @@ __device__ void push_preds_warp(const KParams &p, Ctr *c, uint32_t *sm, uint32_t
   __syncwarp();
   for (uint32_t t0 = 0; t0 < total; t0 += 32u) {
     const uint32_t t = t0 + lane;
-    bool first = false;
-    uint32_t u = 0;
     if (t < total) {
       // owner lane: the first whose inclusive end exceeds t
       uint32_t lo = 0, hi = 31;
@@ -1107,33 +1120,13 @@ __device__ void push_preds_warp(const KParams &p, Ctr *c, uint32_t *sm, uint32_t
       }
       const uint32_t start = lo ? sm[SM_PINC + lo - 1] : 0u;
       const unsigned long long k = (unsigned long long)sm[SM_PBEG + lo] + (t - start);
-      u = ld(p.rcol, k, p.n_edges, c);
-      if (CHECK_IDX(c, u, p.n_nodes)) first = atomicMax(&p.mark[u], stamp) < stamp;
-    }
-    const uint32_t bal = __ballot_sync(FULL, first);
-    if (bal) {
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(nf_size, (uint32_t)__popc(bal));
-      base = __shfl_sync(FULL, base, 0);
-      if (first) {
-        const uint32_t slot = base + __popc(bal & lanemask_lt());
-        if (CHECK_IDX(c, slot, p.n_nodes)) NF[slot] = u;
-      }
+      const uint32_t u = ld(p.rcol, k, p.n_edges, c);
+      if (CHECK_IDX(c, u, p.n_nodes)) mark_push(p, u, stamp);
     }
   }
   __syncwarp();
 }
 
-__device__ __forceinline__ void requeue(const KParams &p, Ctr *c, uint32_t v, uint32_t *NF, uint32_t *nf_size,
-                                        uint32_t stamp) {
-  if (atomicMax(&p.mark[v], stamp) < stamp) {
-    const uint32_t s = atomicAdd(nf_size, 1u);
-    if (CHECK_IDX(c, s, p.n_nodes)) NF[s] = v;
-  }
-}
-
-// MINB = resident blocks per SM the register allocation is sized for (2, 3
-// or 4); the autotuner picks the variant (geq_tuning.blocks_per_sm).
 template <class Cd, int MINB>
 __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
   __shared__ uint32_t smem[WARPS_PER_BLOCK * SM_WORDS];
@@ -1144,14 +1137,10 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
   const uint32_t fs = c->fsize[cur];
   if (fs == 0) return;
   const uint32_t *F = cur ? p.front1 : p.front0;
-  uint32_t *NF = cur ? p.front0 : p.front1;
-  uint32_t *nf_size = &c->fsize[cur ^ 1u];
   const uint32_t stamp = c->stamp + 1u;
   const uint32_t lane = threadIdx.x & 31u;
   uint32_t *sm = smem + (threadIdx.x >> 5) * SM_WORDS;
   uint32_t *scr = tscr + (threadIdx.x >> 5) * (TSCR * 32) + lane;
-  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   const Cd cd = make_codec<Cd>(p);
   uint32_t *arena = c->arena;
   const unsigned long long cap = c->arena_cap;
@@ -1163,7 +1152,13 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
   unsigned long long prof_acc[16] = {};
   const long long t_all0 = clock64();
 #endif
-  for (uint32_t base = gw * 32u; base < fs; base += nw * 32u) {
+  for (;;) {
+    // 32 slots at a time from a shared counter: warps that drew heavy
+    // positions take fewer slots
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&c->next_slot, 32u);
+    base = __shfl_sync(FULL, base, 0);
+    if (base >= fs) break;
 #if GEQ_PATH_PROFILE
     const long long tq0 = clock64();
 #endif
@@ -1228,14 +1223,14 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
       if (lane == 0 && CHECK_IDX(c, base + l, p.n_nodes))
         p.slot_new[base + l] = (r.st == R_CHANGED) ? r.d : NONE_DESC;
       if (lane == l) big_changed = r.st == R_CHANGED;
-      if (r.st == R_OVERFLOW && lane == 0) requeue(p, c, vb, NF, nf_size, stamp);  // retried after compaction
+      if (r.st == R_OVERFLOW && lane == 0) mark_push(p, vb, stamp);  // retried after compaction
     }
 #if GEQ_PATH_PROFILE
     const long long tq2 = clock64();
     if (lane == 0) PROF_ADD(PF_CYC_BIG, tq2 - tq1);
 #endif
-    push_preds_warp(p, c, sm, v, ts == T_CHANGED || big_changed, NF, nf_size, stamp, lane);
-    if (ts == T_OVERFLOW) requeue(p, c, v, NF, nf_size, stamp);
+    push_preds_warp(p, c, sm, v, ts == T_CHANGED || big_changed, stamp, lane);
+    if (ts == T_OVERFLOW) mark_push(p, v, stamp);
 #if GEQ_PATH_PROFILE
     if (lane == 0) PROF_ADD(PF_CYC_PUSH, clock64() - tq2);
     if ((ts == T_CHANGED || big_changed)) PROF_ADD(PF_PUSHED, p.rrow[v + 1] - p.rrow[v]);
@@ -1276,6 +1271,9 @@ __global__ void k_commit(const KParams p) {
   const uint32_t fs = c->fsize[cur];
   if (fs == 0) return;
   const uint32_t *F = cur ? p.front1 : p.front0;
+  // the next round pushes with stamp + 2: clear that half of the bitmap
+  uint32_t *mh = p.mark + (c->stamp & 1u) * p.mwords;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.mwords; i += gridDim.x * blockDim.x) mh[i] = 0u;
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < fs; s += gridDim.x * blockDim.x) {
     const unsigned long long d = p.slot_new[s];
     if (d != NONE_DESC) {
@@ -1297,8 +1295,85 @@ __global__ void k_commit(const KParams p) {
     c->stamp = c->stamp + 1u;
     c->rounds = c->rounds + 1ull;
     c->done_blocks = 0u;
-    if (c->overflow) c->halt = 1u;
     __threadfence();
+  }
+}
+
+// Ids of the set bits of words [b, e) of `mh`, in order, to F[base ...];
+// every thread of the block calls it.  Returns the count.  wsum: 33 words of
+// shared memory.
+__device__ uint32_t block_fill_bits(const uint32_t *mh, uint32_t b, uint32_t e, uint32_t base, uint32_t *F,
+                                    uint32_t nmax, Ctr *c, uint32_t *wsum) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  uint32_t total = 0;
+  for (uint32_t t0 = b; t0 < e; t0 += blockDim.x) {
+    const uint32_t i = t0 + tid;
+    const uint32_t w = i < e ? mh[i] : 0u;
+    const uint32_t cnt = (uint32_t)__popc(w);
+    const uint32_t incl = warp_incl_scan(cnt, lane);
+    if (lane == 31u) wsum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const uint32_t x = lane < nwarps ? wsum[lane] : 0u;
+      const uint32_t xi = warp_incl_scan(x, lane);
+      if (lane < nwarps) wsum[lane] = xi - x;
+      if (lane == 31u) wsum[32] = xi;
+    }
+    __syncthreads();
+    uint32_t off = base + total + wsum[warp] + incl - cnt;
+    for (uint32_t x = w; x; x &= x - 1u, off++)
+      if (CHECK_IDX(c, off, nmax)) F[off] = i * 32u + (uint32_t)__ffs((int)x) - 1u;
+    total += wsum[32];
+    __syncthreads();
+  }
+  return total;
+}
+
+// k_fcount + k_ffill: the next frontier (stamp parity half of the bitmap)
+// as a list in position order.  The last k_ffill block publishes its size,
+// resets the slot counter and, after an arena overflow, halts the remaining
+// rounds of the graph until the host has compacted the arena.
+__global__ void k_fcount(const KParams p) {
+  Ctr *c = p.ctr;
+  if (c->halt) return;
+  __shared__ uint32_t wsum[WARPS_PER_BLOCK];
+  const uint32_t *mh = p.mark + (c->stamp & 1u) * p.mwords;
+  const uint32_t per = (p.mwords + gridDim.x - 1u) / gridDim.x;
+  const uint32_t b = min(p.mwords, blockIdx.x * per), e = min(p.mwords, b + per);
+  uint32_t sum = 0;
+  for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) sum += (uint32_t)__popc(mh[i]);
+  sum = __reduce_add_sync(FULL, sum);
+  if ((threadIdx.x & 31u) == 0u) wsum[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += wsum[w];
+    p.fpart[blockIdx.x] = t;
+  }
+}
+__global__ void k_ffill(const KParams p) {
+  Ctr *c = p.ctr;
+  if (c->halt) return;
+  __shared__ uint32_t wsum[33];
+  __shared__ uint32_t s_base;
+  const uint32_t cur = c->cur;
+  uint32_t *F = cur ? p.front1 : p.front0;
+  const uint32_t *mh = p.mark + (c->stamp & 1u) * p.mwords;
+  uint32_t x = 0;
+  for (uint32_t i = threadIdx.x; i < blockIdx.x; i += blockDim.x) x += p.fpart[i];
+  x = __reduce_add_sync(FULL, x);
+  if (threadIdx.x == 0) s_base = 0u;
+  __syncthreads();
+  if ((threadIdx.x & 31u) == 0u && x) atomicAdd(&s_base, x);
+  __syncthreads();
+  const uint32_t base = s_base;
+  const uint32_t per = (p.mwords + gridDim.x - 1u) / gridDim.x;
+  const uint32_t b = min(p.mwords, blockIdx.x * per), e = min(p.mwords, b + per);
+  block_fill_bits(mh, b, e, base, F, (uint32_t)p.n_nodes, c, wsum);
+  if (blockIdx.x == gridDim.x - 1u && threadIdx.x == 0) {
+    c->fsize[cur] = base + p.fpart[blockIdx.x];
+    c->next_slot = 0u;
+    if (c->overflow) c->halt = 1u;
   }
 }
 
@@ -1481,7 +1556,7 @@ __global__ void k_init_frontier(const KParams p, const uint32_t *reach, unsigned
   const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
   for (unsigned long long i0 = gw * 32ull; i0 < n_reach; i0 += nw * 32ull) {
     const unsigned long long i = i0 + lane;
-    push_preds_warp(p, c, sm, i < n_reach ? reach[i] : 0u, i < n_reach, p.front0, &c->fsize[0], c->stamp, lane);
+    push_preds_warp(p, c, sm, i < n_reach ? reach[i] : 0u, i < n_reach, c->stamp, lane);
   }
 }
 
@@ -1737,7 +1812,7 @@ struct DeviceGamesImpl {
   uint32_t *row = nullptr, *col = nullptr, *wt = nullptr, *rrow = nullptr, *rcol = nullptr;
   uint8_t *flags = nullptr;
   unsigned long long *desc = nullptr, *desc_init = nullptr, *slot_new = nullptr;
-  uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr;
+  uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr, *fpart = nullptr;
   uint32_t *init_data = nullptr;
   unsigned long long init_total = 0;
   char *inbuf = nullptr;  // row, col, wt, flags, reach, init_data, [desc_init], node bases
@@ -1932,6 +2007,13 @@ geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
   CU(cudaEventCreate(&s.evb));
   CU(cudaHostAlloc((void **)&s.h_ctr, sizeof(Ctr), cudaHostAllocDefault));
   CU(cudaMalloc((void **)&s.d_err, sizeof(uint32_t)));
+  // the round kernels want shared memory for several resident blocks
+  CU(cudaFuncSetAttribute(k_round<CodecStd, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round<CodecStd, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round<CodecStd, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round<CodecGen, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round<CodecGen, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round<CodecGen, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int bps = 0;
   CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_round<CodecStd, 3>, BLOCK, 0));
   eng->tuning.blocks_per_sm = (uint32_t)std::max(2, std::min(bps, 3));
@@ -2073,8 +2155,9 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   D.d_node_base = (unsigned long long *)(D.inbuf + off_base);
   if (any_init) D.desc_init = (unsigned long long *)(D.inbuf + off_desc);
   if (!D.alloc(D.rrow, N + 1) || !D.alloc(D.rcol, M) || !D.alloc(D.desc, N) ||
-      (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, N) ||
-      !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1))
+      (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, 2 * ((N + 31) / 32)) ||
+      !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1) ||
+      !D.alloc(D.fpart, (size_t)std::max(1, n_sms * 2)))
     return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
@@ -2088,7 +2171,7 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
       k_init_reach<<<(unsigned)std::min<unsigned long long>((n_reach + 255) / 256, 4096), 256, 0, S>>>(
           D.desc_init, D.reach, n_reach);
   }
-  if (N) CU(cudaMemsetAsync(D.mark, 0, N * 4, S));
+  CU(cudaMemsetAsync(D.mark, 0, 2 * ((N + 31) / 32) * 4, S));
   CU(cudaMemsetAsync(s.d_err, 0, 4, S));
   const unsigned grid = (unsigned)std::max(1, n_sms * 8);
   if (D.n_games > 1)
@@ -2122,6 +2205,9 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   kp.row = D.row; kp.col = D.col; kp.wt = D.wt; kp.rrow = D.rrow; kp.rcol = D.rcol;
   kp.flags = D.flags; kp.desc = D.desc; kp.mark = D.mark; kp.front0 = D.front0; kp.front1 = D.front1;
   kp.slot_new = D.slot_new; kp.ctr = D.ctr; kp.n_nodes = N; kp.n_edges = M;
+  kp.mwords = (uint32_t)((N + 31) / 32);
+  kp.fpart = D.fpart;
+  kp.fblocks = (uint32_t)std::max(1, n_sms * 2);
   kp.el = D.conf.elements; kp.mx = D.conf.max; kp.eb = D.conf.energy_bits(); kp.em = D.conf.energy_mask();
   kp.ub = D.conf.update_bits(); kp.um = D.conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
@@ -2178,6 +2264,8 @@ static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent
   else k_round<Cd, 4><<<grid, BLOCK, 0, S>>>(kp);
   if (eb) cudaEventRecord(eb, S);
   k_commit<<<(unsigned)std::max(1, E.n_sms * 2), 256, 0, S>>>(kp);
+  k_fcount<<<kp.fblocks, 256, 0, S>>>(kp);
+  k_ffill<<<kp.fblocks, 256, 0, S>>>(kp);
 }
 
 // One captured graph of R rounds per codec, shared by every upload: before a
@@ -2233,10 +2321,8 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
   CU(cudaEventRecord(s.ev0, S));
   if (dg.N) CU(cudaMemcpyAsync(dg.desc, dg.desc_init, dg.N * 8, cudaMemcpyDeviceToDevice, S));
   CU(cudaMemcpyAsync(dg.arena[a0], dg.init_data, dg.init_total * 4, cudaMemcpyDeviceToDevice, S));
-  if (dg.next_stamp > 0xF0000000u) {
-    if (dg.N) CU(cudaMemsetAsync(dg.mark, 0, dg.N * 4, S));
-    dg.next_stamp = 1;
-  }
+  if (dg.next_stamp > 0xF0000000u) dg.next_stamp = 1;
+  CU(cudaMemsetAsync(dg.mark, 0, 2ull * dg.kp.mwords * 4, S));
   Ctr h{};
   h.arena = dg.arena[a0];
   h.arena_cap = dg.arena_cap[a0];
@@ -2248,7 +2334,9 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
     const unsigned grid = (unsigned)std::max<unsigned long long>(
         1, std::min<unsigned long long>((dg.n_reach + 7) / 8, (unsigned long long)n_sms * 16));
     k_init_frontier<<<grid, 256, 0, S>>>(dg.kp, dg.reach, dg.n_reach);
-    launches++;
+    k_fcount<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
+    k_ffill<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
+    launches += 3;
   }
   CU(cudaGetLastError());
   const bool profile = (tuning.flags & GEQ_TUNE_PROFILE) != 0;
@@ -2274,7 +2362,7 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
       if (dg.generic) launch_round<CodecGen>(*this, dg.kp, S, ea, eb);
       else launch_round<CodecStd>(*this, dg.kp, S, ea, eb);
     }
-    launches += 2ull * R;
+    launches += 4ull * R;
     CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
     CU(cudaStreamSynchronize(S));
     const Ctr c = *s.h_ctr;
@@ -2524,7 +2612,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
   for (unsigned long long v = tid; v < N; v += BLOCK)
     for (uint32_t k = p.row[v]; k < p.row[v + 1]; k++) rcol[atomicAdd(&p.mark[p.col[k]], 1u)] = (uint32_t)v;
   __syncthreads();
-  for (unsigned long long v = tid; v < N; v += BLOCK) p.mark[v] = 0u;
+  for (unsigned long long v = tid; v < 2ull * p.mwords; v += BLOCK) p.mark[v] = 0u;
   __syncthreads();
   // -- standard initialisation: {0} at the positions to reach (EnergyGame::with_reach)
   auto is_reach = [&](unsigned long long v) { return !(p.flags[v] & 1u) && p.row[v + 1] == p.row[v]; };
@@ -2543,10 +2631,17 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
       v = a.reach ? a.reach[i] : (uint32_t)i;
       f = a.reach ? true : is_reach(i);
     }
-    push_preds_warp(p, c, sm, v, f, p.front0, &c->fsize[0], c->stamp, lane);
+    push_preds_warp(p, c, sm, v, f, c->stamp, lane);
   }
   __syncthreads();
-  // -- rounds (k_round + k_commit in one block)
+  __shared__ uint32_t s_wsum[33];
+  {
+    const uint32_t n0 = block_fill_bits(p.mark + (c->stamp & 1u) * p.mwords, 0u, p.mwords, 0u, p.front0,
+                                        (uint32_t)N, c, s_wsum);
+    if (tid == 0) c->fsize[0] = n0;
+    __syncthreads();
+  }
+  // -- rounds (k_round + k_commit + k_fcount/k_ffill in one block)
   uint32_t *scr = tscr + warp * (TSCR * 32) + lane;
   const Cd cd = make_codec<Cd>(p);
   uint32_t *arena = a.arena;
@@ -2567,8 +2662,6 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
     if (s_stop) break;
     const uint32_t cur = s_cur, fs = s_fs;
     const uint32_t *F = cur ? p.front1 : p.front0;
-    uint32_t *NF = cur ? p.front0 : p.front1;
-    uint32_t *nf_size = &c->fsize[cur ^ 1u];
     const uint32_t stamp = c->stamp + 1u;
     for (uint32_t base = warp * 32u; base < fs; base += BLOCK) {
       const uint32_t slot = base + lane;
@@ -2612,9 +2705,10 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
           p.slot_new[base + l] = (rs.st == R_CHANGED) ? rs.d : NONE_DESC;
         if (lane == l) big_changed = rs.st == R_CHANGED;
       }
-      push_preds_warp(p, c, sm, v, ts == T_CHANGED || big_changed, NF, nf_size, stamp, lane);
+      push_preds_warp(p, c, sm, v, ts == T_CHANGED || big_changed, stamp, lane);
     }
     __syncthreads();
+    for (uint32_t i = tid; i < p.mwords; i += BLOCK) p.mark[(c->stamp & 1u) * p.mwords + i] = 0u;
     for (uint32_t s2 = tid; s2 < fs; s2 += BLOCK) {
       const unsigned long long d = p.slot_new[s2];
       if (d != NONE_DESC) {
@@ -2629,6 +2723,11 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
       c->stamp = c->stamp + 1u;
       c->rounds = c->rounds + 1ull;
     }
+    __syncthreads();
+    // the next frontier, in position order, from the half this round filled
+    const uint32_t nn = block_fill_bits(p.mark + (c->stamp & 1u) * p.mwords, 0u, p.mwords, 0u,
+                                        cur ? p.front0 : p.front1, (uint32_t)N, c, s_wsum);
+    if (tid == 0) c->fsize[cur ^ 1u] = nn;
     __syncthreads();
   }
 #pragma unroll
@@ -2711,7 +2810,8 @@ geq_status Engine::run_static(int device, const geq_game_graph &g, const uint32_
   };
   const size_t o_ctr = take(sizeof(Ctr)), o_row = take((N + 1) * 4), o_col = take(M * 4), o_wt = take(M * 4),
                o_flags = take(N), o_reach = take((size_t)n_reach * 4), o_rrow = take((N + 1) * 4),
-               o_rcol = take(M * 4), o_desc = take(N * 8), o_slot = take(N * 8), o_mark = take(N * 4),
+               o_rcol = take(M * 4), o_desc = take(N * 8), o_slot = take(N * 8),
+               o_mark = take(std::max<unsigned long long>(N, 2 * ((N + 31) / 32)) * 4),
                o_f0 = take(N * 4), o_f1 = take(N * 4), o_out = take((N + 1) * 8);
   const size_t min_arena = 4096 * 4;
   if (N >= 0xFFFFFFF0ull || M >= 0xFFFFFFF0ull || top + min_arena > GEQ_STATIC_SCRATCH_BYTES)
@@ -2736,6 +2836,7 @@ geq_status Engine::run_static(int device, const geq_game_graph &g, const uint32_
   kp.ctr = (Ctr *)(base + o_ctr);
   kp.n_nodes = N;
   kp.n_edges = M;
+  kp.mwords = (uint32_t)((N + 31) / 32);
   kp.el = conf.elements; kp.mx = conf.max; kp.eb = conf.energy_bits(); kp.em = conf.energy_mask();
   kp.ub = conf.update_bits(); kp.um = conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
