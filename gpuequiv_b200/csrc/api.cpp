@@ -81,7 +81,7 @@ static geq_status make_inputs(uint32_t n_games, const geq_game_graph *graphs, co
                               std::vector<GameInput> &in) {
   if (n_games == 0 || !graphs) return fail(GEQ_ERR_INVALID_INPUT, "no games");
   in.resize(n_games);
-  for (uint32_t g = 0; g < n_games; g++) {
+  auto one = [&](uint32_t g) -> geq_status {
     GameInput &gi = in[g];
     gi.g = graphs[g];
     geq_status st = validate_graph(gi.g);
@@ -101,6 +101,27 @@ static geq_status make_inputs(uint32_t n_games, const geq_game_graph *graphs, co
       gi.to_reach = gi.reach_storage.data();
       gi.n_reach = (uint32_t)gi.reach_storage.size();
     }
+    return GEQ_OK;
+  };
+  if (n_games < 64) {
+    for (uint32_t g = 0; g < n_games; g++) {
+      const geq_status st = one(g);
+      if (st) return st;
+    }
+  } else {
+    // large batches: games checked on all host cores; the first failing game
+    // (in batch order) decides the status and message
+    std::vector<geq_status> sts(n_games, GEQ_OK);
+    std::vector<std::string> msgs(n_games);
+    parallel_for(n_games, [&](uint32_t g) {
+      sts[g] = one(g);
+      if (sts[g]) msgs[g] = geq_last_error();
+    });
+    for (uint32_t g = 0; g < n_games; g++)
+      if (sts[g]) {
+        set_last_error(msgs[g]);
+        return sts[g];
+      }
   }
   if (!Conf(graphs[0].conf).supported())
     return fail(GEQ_ERR_UNSUPPORTED, "EnergyConf {%u, %u} is outside the device codecs", graphs[0].conf.elements,

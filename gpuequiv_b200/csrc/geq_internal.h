@@ -1,12 +1,15 @@
 // geq_internal.h - declarations shared by the sources of libgeq.so.
 #pragma once
 
+#include <algorithm>
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/geq.h"
@@ -54,6 +57,29 @@ struct GameInput {
 // energygame.rs:65-83, plus update-code checks).
 geq_status validate_graph(const geq_game_graph &g);
 geq_status validate_lists(const geq_game_graph &g, const geq_energy_lists *l);
+
+// ---- host threads -----------------------------------------------------------
+// f(i) for i < n on up to `max_threads` host threads (all cores when 0).
+template <class F>
+void parallel_for(uint32_t n, F f, uint32_t max_threads = 0) {
+  uint32_t threads = std::max(1u, std::min<uint32_t>(std::thread::hardware_concurrency(), n));
+  if (max_threads) threads = std::min(threads, max_threads);
+  if (threads <= 1) {
+    for (uint32_t i = 0; i < n; i++) f(i);
+    return;
+  }
+  std::atomic<uint32_t> next{0};
+  std::vector<std::thread> pool;
+  for (uint32_t t = 0; t < threads; t++)
+    pool.emplace_back([&]() {
+      for (;;) {
+        const uint32_t i = next.fetch_add(1);
+        if (i >= n) break;
+        f(i);
+      }
+    });
+  for (auto &th : pool) th.join();
+}
 
 // ---- page-locked host memory for results -------------------------------------
 // Blocks are cached by size class so that downloads copy straight into

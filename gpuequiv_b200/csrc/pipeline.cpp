@@ -46,26 +46,6 @@ GameInput input_of(const GameBuilder &b) {
   return gi;
 }
 
-template <class F>
-void parallel_for(uint32_t n, F f) {
-  uint32_t threads = std::max(1u, std::min<uint32_t>(std::thread::hardware_concurrency(), n));
-  if (threads <= 1) {
-    for (uint32_t i = 0; i < n; i++) f(i);
-    return;
-  }
-  std::atomic<uint32_t> next{0};
-  std::vector<std::thread> pool;
-  for (uint32_t t = 0; t < threads; t++)
-    pool.emplace_back([&]() {
-      for (;;) {
-        uint32_t i = next.fetch_add(1);
-        if (i >= n) break;
-        f(i);
-      }
-    });
-  for (auto &th : pool) th.join();
-}
-
 // EnergyArray::test_equivalence (energy.rs:307-318) for STANDARD energies.
 bool holds(const uint32_t *e, uint64_t n, uint32_t eq) {
   for (uint64_t k = 0; k < n; k++) {
