@@ -139,8 +139,9 @@ struct KParams {
   uint32_t thread_path;  // 1: lane-per-position path for small positions
   uint32_t ib, ibm, inl; // inline descriptors: bits per energy, its mask, capacity
   uint32_t mwords;       // words of one half of the frontier bitmap `mark`
-  uint32_t *fpart;       // per-block set-bit counts of the bitmap (k_fcount)
+  uint32_t *fpart;       // per-block set-bit counts of the bitmap (k_fcount): attackers, defenders
   uint32_t fblocks;      // blocks of k_fcount / k_ffill
+  const uint32_t *abits; // attacker positions as a bitmap (mwords words)
 };
 
 // Energy-list descriptors (one u64 per position):
@@ -1299,16 +1300,17 @@ __global__ void k_commit(const KParams p) {
   }
 }
 
-// Ids of the set bits of words [b, e) of `mh`, in order, to F[base ...];
-// every thread of the block calls it.  Returns the count.  wsum: 33 words of
-// shared memory.
+// Ids of the set bits of words [b, e) of `mh` (and of `mask` ^ flip when a
+// mask is given), in order, to F[base ...]; every thread of the block calls
+// it.  Returns the count.  wsum: 33 words of shared memory.
 __device__ uint32_t block_fill_bits(const uint32_t *mh, uint32_t b, uint32_t e, uint32_t base, uint32_t *F,
-                                    uint32_t nmax, Ctr *c, uint32_t *wsum) {
+                                    uint32_t nmax, Ctr *c, uint32_t *wsum, const uint32_t *mask = nullptr,
+                                    uint32_t flip = 0u) {
   const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5, nwarps = blockDim.x >> 5;
   uint32_t total = 0;
   for (uint32_t t0 = b; t0 < e; t0 += blockDim.x) {
     const uint32_t i = t0 + tid;
-    const uint32_t w = i < e ? mh[i] : 0u;
+    const uint32_t w = i < e ? (mh[i] & (mask ? (mask[i] ^ flip) : ~0u)) : 0u;
     const uint32_t cnt = (uint32_t)__popc(w);
     const uint32_t incl = warp_incl_scan(cnt, lane);
     if (lane == 31u) wsum[warp] = incl;
@@ -1330,50 +1332,93 @@ __device__ uint32_t block_fill_bits(const uint32_t *mh, uint32_t b, uint32_t e, 
 }
 
 // k_fcount + k_ffill: the next frontier (stamp parity half of the bitmap)
-// as a list in position order.  The last k_ffill block publishes its size,
-// resets the slot counter and, after an arena overflow, halts the remaining
-// rounds of the graph until the host has compacted the arena.
+// as a list in position order, attackers first, then defenders, so that a
+// warp of the next round mostly meets one kind of position.  The last k_ffill
+// block publishes its size, resets the slot counter and, after an arena
+// overflow, halts the remaining rounds of the graph until the host has
+// compacted the arena.
 __global__ void k_fcount(const KParams p) {
   Ctr *c = p.ctr;
   if (c->halt) return;
-  __shared__ uint32_t wsum[WARPS_PER_BLOCK];
+  __shared__ uint32_t wsum[2 * WARPS_PER_BLOCK];
   const uint32_t *mh = p.mark + (c->stamp & 1u) * p.mwords;
   const uint32_t per = (p.mwords + gridDim.x - 1u) / gridDim.x;
   const uint32_t b = min(p.mwords, blockIdx.x * per), e = min(p.mwords, b + per);
-  uint32_t sum = 0;
-  for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) sum += (uint32_t)__popc(mh[i]);
-  sum = __reduce_add_sync(FULL, sum);
-  if ((threadIdx.x & 31u) == 0u) wsum[threadIdx.x >> 5] = sum;
+  uint32_t sa = 0, sd = 0;
+  for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+    const uint32_t w = mh[i], a = p.abits[i];
+    sa += (uint32_t)__popc(w & a);
+    sd += (uint32_t)__popc(w & ~a);
+  }
+  sa = __reduce_add_sync(FULL, sa);
+  sd = __reduce_add_sync(FULL, sd);
+  if ((threadIdx.x & 31u) == 0u) {
+    wsum[threadIdx.x >> 5] = sa;
+    wsum[WARPS_PER_BLOCK + (threadIdx.x >> 5)] = sd;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    uint32_t t = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += wsum[w];
-    p.fpart[blockIdx.x] = t;
+    uint32_t ta = 0, td = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      ta += wsum[w];
+      td += wsum[WARPS_PER_BLOCK + w];
+    }
+    p.fpart[2 * blockIdx.x] = ta;
+    p.fpart[2 * blockIdx.x + 1] = td;
   }
 }
 __global__ void k_ffill(const KParams p) {
   Ctr *c = p.ctr;
   if (c->halt) return;
   __shared__ uint32_t wsum[33];
-  __shared__ uint32_t s_base;
+  __shared__ uint32_t s_pa, s_pd, s_ta;
   const uint32_t cur = c->cur;
   uint32_t *F = cur ? p.front1 : p.front0;
   const uint32_t *mh = p.mark + (c->stamp & 1u) * p.mwords;
-  uint32_t x = 0;
-  for (uint32_t i = threadIdx.x; i < blockIdx.x; i += blockDim.x) x += p.fpart[i];
-  x = __reduce_add_sync(FULL, x);
-  if (threadIdx.x == 0) s_base = 0u;
+  // attackers before this block, defenders before this block, all attackers
+  uint32_t pa = 0, pd = 0, ta = 0;
+  for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+    const uint32_t a = p.fpart[2 * i], d = p.fpart[2 * i + 1];
+    ta += a;
+    if (i < blockIdx.x) {
+      pa += a;
+      pd += d;
+    }
+  }
+  pa = __reduce_add_sync(FULL, pa);
+  pd = __reduce_add_sync(FULL, pd);
+  ta = __reduce_add_sync(FULL, ta);
+  if (threadIdx.x == 0) {
+    s_pa = 0u;
+    s_pd = 0u;
+    s_ta = 0u;
+  }
   __syncthreads();
-  if ((threadIdx.x & 31u) == 0u && x) atomicAdd(&s_base, x);
+  if ((threadIdx.x & 31u) == 0u) {
+    atomicAdd(&s_pa, pa);
+    atomicAdd(&s_pd, pd);
+    atomicAdd(&s_ta, ta);
+  }
   __syncthreads();
-  const uint32_t base = s_base;
   const uint32_t per = (p.mwords + gridDim.x - 1u) / gridDim.x;
   const uint32_t b = min(p.mwords, blockIdx.x * per), e = min(p.mwords, b + per);
-  block_fill_bits(mh, b, e, base, F, (uint32_t)p.n_nodes, c, wsum);
+  block_fill_bits(mh, b, e, s_pa, F, (uint32_t)p.n_nodes, c, wsum, p.abits, 0u);
+  block_fill_bits(mh, b, e, s_ta + s_pd, F, (uint32_t)p.n_nodes, c, wsum, p.abits, ~0u);
   if (blockIdx.x == gridDim.x - 1u && threadIdx.x == 0) {
-    c->fsize[cur] = base + p.fpart[blockIdx.x];
+    c->fsize[cur] = s_ta + s_pd + p.fpart[2 * blockIdx.x + 1];
     c->next_slot = 0u;
     if (c->overflow) c->halt = 1u;
+  }
+}
+// Attacker positions as a bitmap (frontier ordering by kind).
+__global__ void k_abits(const uint8_t *flags, unsigned long long n, uint32_t words, uint32_t *abits) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) {
+    uint32_t w = 0;
+    for (uint32_t k = 0; k < 32u; k++) {
+      const unsigned long long v = (unsigned long long)i * 32u + k;
+      if (v < n && (flags[v] & 1u)) w |= 1u << k;
+    }
+    abits[i] = w;
   }
 }
 
@@ -1812,7 +1857,7 @@ struct DeviceGamesImpl {
   uint32_t *row = nullptr, *col = nullptr, *wt = nullptr, *rrow = nullptr, *rcol = nullptr;
   uint8_t *flags = nullptr;
   unsigned long long *desc = nullptr, *desc_init = nullptr, *slot_new = nullptr;
-  uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr, *fpart = nullptr;
+  uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr, *fpart = nullptr, *abits = nullptr;
   uint32_t *init_data = nullptr;
   unsigned long long init_total = 0;
   char *inbuf = nullptr;  // row, col, wt, flags, reach, init_data, [desc_init], node bases
@@ -2157,7 +2202,7 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   if (!D.alloc(D.rrow, N + 1) || !D.alloc(D.rcol, M) || !D.alloc(D.desc, N) ||
       (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, 2 * ((N + 31) / 32)) ||
       !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1) ||
-      !D.alloc(D.fpart, (size_t)std::max(1, n_sms * 2)))
+      !D.alloc(D.fpart, 2 * (size_t)std::max(1, n_sms * 2)) || !D.alloc(D.abits, (N + 31) / 32))
     return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
@@ -2194,6 +2239,7 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   k_u64_to_u32<<<grid, 256, 0, S>>>(roff, N + 1, D.rrow);
   CU(cudaMemcpyAsync(s.cnt, D.rrow, N * 4, cudaMemcpyDeviceToDevice, S));
   k_fill_reverse<<<grid, 256, 0, S>>>(D.row, D.col, N, s.cnt, D.rcol);
+  if (N) k_abits<<<grid, 256, 0, S>>>(D.flags, N, (uint32_t)((N + 31) / 32), D.abits);
   CU(cudaMemcpyAsync(&s.h_ctr->pad, s.d_err, 4, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   s.pool.put(roff, (N + 1) * 8);
@@ -2208,6 +2254,7 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   kp.mwords = (uint32_t)((N + 31) / 32);
   kp.fpart = D.fpart;
   kp.fblocks = (uint32_t)std::max(1, n_sms * 2);
+  kp.abits = D.abits;
   kp.el = D.conf.elements; kp.mx = D.conf.max; kp.eb = D.conf.energy_bits(); kp.em = D.conf.energy_mask();
   kp.ub = D.conf.update_bits(); kp.um = D.conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
