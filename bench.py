@@ -56,33 +56,43 @@ def parse():
 
 # ---- distributed plumbing -------------------------------------------------------
 class Dist:
-    def __init__(self):
+    """One process per GPU.  NCCL between GPUs; `backend="gloo"` runs the same
+    host logic on CPU ranks (the multi-rank tests)."""
+
+    def __init__(self, backend: str | None = None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                    device_id=torch.device("cuda", self.local_rank))
+            backend = backend or "nccl"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+                self.device = "cuda"
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                        device_id=torch.device("cuda", self.local_rank))
+            else:
+                dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
         if self.pg:
             import torch
-            t = torch.zeros(1, device="cuda")
+            t = torch.zeros(1, device=self.device)
             self.pg.all_reduce(t)
-            torch.cuda.synchronize()
+            if self.device == "cuda":
+                torch.cuda.synchronize()
 
     def max(self, x: float) -> float:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -90,7 +100,7 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t)
         return float(t.item())
 
@@ -230,13 +240,14 @@ def peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes of k_round from the committed ncu summary."""
+def profile_traffic_ratio():
+    """DRAM bytes per algorithmic byte of k_round, from the committed ncu
+    summary (all round launches of a smaller case of the same workload)."""
     p = os.path.join(ROOT, "profiles", "k_round_batched.md")
     try:
         with open(p) as f:
             for line in f:
-                if line.strip().startswith("traffic_bytes_per_launch:"):
+                if line.strip().startswith("dram_per_algorithmic_byte:"):
                     return float(line.split(":", 1)[1].strip())
     except OSError:
         pass
@@ -325,7 +336,9 @@ def run_ours(args, d: Dist):
     k_ms = st_prof["round_kernel_ms"]
     k_launch = max(1, st_prof["round_kernel_launches"])
     achieved = st_prof["algorithmic_bytes"] / (k_ms / 1e3) / 1e9 if k_ms > 0 else None
-    traffic = profile_traffic()
+    ratio = profile_traffic_ratio()
+    alg_per_launch = st_prof["algorithmic_bytes"] / k_launch
+    traffic = ratio * alg_per_launch if ratio else None
 
     # ---- e2e: host buffers through the C ABI (geq_energy_game_run_batch) ----
     views = geq.c_views(graphs)
@@ -378,6 +391,10 @@ def run_ours(args, d: Dist):
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "traffic_source": "ncu DRAM bytes per algorithmic byte of all round launches of the "
+                                           "1024-job case (profiles/k_round_batched.md) x algorithmic bytes "
+                                           "per full-size launch",
+                         "algorithmic_bytes_per_launch": alg_per_launch,
                          "kernel": "k_round", "peak_kind": peak_kind,
                          "algorithmic_bytes_per_solve": st_prof["algorithmic_bytes"],
                          "round_kernel_ms_per_solve": k_ms, "round_kernel_launches": k_launch},
