@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--plain-sample", type=int, default=256)
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch shape)")
+    ap.add_argument("--serve-rates", default="1000,5000",
+                    help="Poisson arrival rates (req/s) of the serving leg; empty: no serving leg")
+    ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrivals per serving rate (s)")
     ap.add_argument("--solve-only", action="store_true",
                     help="build, upload and solve only (the command profiled with ncu)")
     return ap.parse_args()
@@ -254,6 +257,58 @@ def profile_traffic_ratio():
     return None
 
 
+def run_serving(ctx, graphs, lam: float, seconds: float, seed: int) -> dict:
+    """Poisson arrivals of single-game requests (drawn from `graphs`) into the
+    serving loop; latency = submit -> result in the caller's hands."""
+    import queue
+    import threading
+
+    from gpuequiv_b200.serving import Server
+    rng = np.random.default_rng(seed)
+    n = max(1, int(lam * seconds))
+    arrivals = np.cumsum(rng.exponential(1.0 / lam, n))
+    pick = rng.integers(0, len(graphs), n)
+    t_sub = np.zeros(n)
+    t_done = np.zeros(n)
+    with Server(ctx) as srv:
+        for g in graphs[:32]:  # warm the pipelines (graphs, pools)
+            srv.poll(srv.submit(g))
+        q: "queue.Queue" = queue.Queue()
+
+        def poller():
+            while True:
+                item = q.get()
+                if item is None:
+                    return
+                i, t = item
+                srv.poll(t)
+                t_done[i] = time.perf_counter()
+
+        pollers = [threading.Thread(target=poller) for _ in range(4)]
+        for th in pollers:
+            th.start()
+        st0 = srv.stats()
+        t0 = time.perf_counter()
+        for i in range(n):
+            wait = t0 + arrivals[i] - time.perf_counter()
+            if wait > 0:
+                time.sleep(wait)
+            t_sub[i] = time.perf_counter()
+            q.put((i, srv.submit(graphs[pick[i]])))
+        for _ in pollers:
+            q.put(None)
+        for th in pollers:
+            th.join()
+        st = srv.stats()
+    lat = (t_done - t_sub) * 1e3
+    span = t_done.max() - t0
+    batches = st["batches"] - st0["batches"]
+    return {"lambda_req_s": lam, "requests": n, "seconds": round(float(span), 3),
+            "throughput_games_s": n / span, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+            "batches": int(batches), "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches)}
+
+
 # ---- arms -----------------------------------------------------------------------
 def run_reference(args, d: Dist):
     if d.rank != 0:
@@ -366,6 +421,12 @@ def run_ours(args, d: Dist):
     plain_s = time.perf_counter() - t
     plain_rate = len(idx) / plain_s  # every k-th job: the batch's size mix
 
+    # ---- serving loop: Poisson arrivals of single games (not part of value) ----
+    serving = []
+    rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
+    for k, lam in enumerate(rates):
+        serving.append(run_serving(ctx, graphs, lam, args.serve_seconds, seed=100 + k + 1000 * d.rank))
+
     # ---- CPU baseline: the oracle on one host thread (rank 0, N=1) ----
     cpu = None
     if d.rank == 0 and d.world == 1:
@@ -404,6 +465,9 @@ def run_ours(args, d: Dist):
             "plain_cuda": {"value": plain_rate, "unit": UNIT, "sample": f"{len(idx)} games (every "
                            f"{max(1, len(graphs) // len(idx))}th job), one geq_energy_game_run call each"},
             "batched_vs_plain": value / plain_rate if plain_rate else None,
+            "serving": {"workload": "Poisson arrivals of single compare(p,q) games drawn from this batch "
+                                    "(LTS 20-5000 states), geq_server with 2 pipelines, 150 GB admission budget",
+                        "runs": serving},
             "gpu_launches": int(launches),
             "clocks": ck,
             "solve_stats": {k: st_last[k] for k in ("rounds", "positions_computed", "edges_relaxed",

@@ -44,6 +44,20 @@ class geq_tuning(C.Structure):
                 ("small_limit", C.c_uint32), ("flags", C.c_uint32)]
 
 
+class geq_server_config(C.Structure):
+    _fields_ = [("n_pipelines", C.c_uint32), ("max_batch_games", C.c_uint32), ("max_wait_us", C.c_uint32),
+                ("reserved", C.c_uint32), ("hbm_budget_bytes", C.c_uint64), ("max_queued", C.c_uint64)]
+
+
+class geq_server_stats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("batches", C.c_uint64), ("queued", C.c_uint64), ("running", C.c_uint64),
+                ("games_in_batches", C.c_uint64), ("max_batch_footprint", C.c_uint64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class geq_position(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("p", C.c_uint32), ("q", C.POINTER(C.c_uint32)), ("n_q", C.c_uint32),
                 ("qx", C.POINTER(C.c_uint32)), ("n_qx", C.c_uint32)]
@@ -115,6 +129,11 @@ _SIGS = {
     "geq_device_games_solve": ([vp, vp, C.POINTER(geq_solve_stats)], C.c_int),
     "geq_device_games_download": ([vp, vp, C.POINTER(vp)], C.c_int),
     "geq_device_games_free": ([vp], None),
+    "geq_server_create": ([vp, C.POINTER(geq_server_config), C.POINTER(vp)], C.c_int),
+    "geq_server_submit": ([vp, C.POINTER(geq_game_graph), C.POINTER(C.c_uint64)], C.c_int),
+    "geq_server_poll": ([vp, C.c_uint64, C.c_int32, C.POINTER(vp)], C.c_int),
+    "geq_server_get_stats": ([vp, C.POINTER(geq_server_stats)], None),
+    "geq_server_destroy": ([vp], None),
     "geq_lts_from_edges": ([C.c_uint64, u32p, u32p, i32p, C.POINTER(vp)], C.c_int),
     "geq_lts_from_csv_file": ([C.c_char_p, C.POINTER(vp)], C.c_int),
     "geq_lts_n_vertices": ([vp], C.c_uint32),

@@ -63,7 +63,7 @@ geq_status validate_lists(const geq_game_graph &g, const geq_energy_lists *l) {
   return GEQ_OK;
 }
 
-static std::vector<uint32_t> standard_reach_of(const geq_game_graph &g) {
+std::vector<uint32_t> standard_reach_of(const geq_game_graph &g) {
   std::vector<uint32_t> r;
   for (uint32_t v = 0; v < g.n_vertices; v++)
     if (!g.attacker_pos[v] && g.row_offsets[v + 1] == g.row_offsets[v]) r.push_back(v);

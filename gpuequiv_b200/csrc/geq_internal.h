@@ -57,6 +57,8 @@ struct GameInput {
 // energygame.rs:65-83, plus update-code checks).
 geq_status validate_graph(const geq_game_graph &g);
 geq_status validate_lists(const geq_game_graph &g, const geq_energy_lists *l);
+// EnergyGame::standard_reach (energygame.rs:347-352): defenders without successors.
+std::vector<uint32_t> standard_reach_of(const geq_game_graph &g);
 
 // ---- host threads -----------------------------------------------------------
 // f(i) for i < n on up to `max_threads` host threads (all cores when 0).

@@ -229,6 +229,52 @@ geq_status geq_device_games_download(geq_context *ctx, geq_device_games *dg,
                                      geq_solution **out);
 void geq_device_games_free(geq_device_games *dg);
 
+/* ---- serving loop ---------------------------------------------------------
+ * Requests (one game each, standard initialisation) are queued by
+ * geq_server_submit and solved by pipeline threads, each with its own CUDA
+ * stream, staging and device memory: a pipeline takes every queued request
+ * that fits its batch limits, uploads the batch as one id space, solves it
+ * with the batched round loop and splits the lists per request, while the
+ * other pipelines upload or solve the batches before and after it (continuous
+ * batching over alternating pipelines).  A batch is admitted only while its
+ * estimated device footprint stays within hbm_budget_bytes / n_pipelines.
+ * Results are identical to geq_energy_game_run of the same game: every game
+ * keeps its own positions and frontier inside a batch.  The crate has no
+ * server; its callers run EnergyGame::run per request (energygame.rs:379-383),
+ * which geq_energy_game_run replaces one to one. */
+typedef struct geq_server geq_server;
+typedef struct geq_server_config {
+  uint32_t n_pipelines;       /* pipeline threads/streams (0: 2) */
+  uint32_t max_batch_games;   /* requests per batch at most (0: 4096) */
+  uint32_t max_wait_us;       /* a pipeline waits this long for more requests
+                                 once it holds fewer than max_batch_games (0: 200) */
+  uint32_t reserved;
+  uint64_t hbm_budget_bytes;  /* device footprint of all in-flight batches (0: 150 GB) */
+  uint64_t max_queued;        /* queued requests before submit answers BUSY (0: 1,000,000) */
+} geq_server_config;
+typedef struct geq_server_stats {
+  uint64_t submitted, completed, failed, batches, queued, running;
+  uint64_t games_in_batches;     /* sum of batch sizes */
+  uint64_t max_batch_footprint;  /* bytes, largest admitted batch estimate */
+} geq_server_stats;
+/* The server solves on the device of `ctx` and copies its tuning; ctx may be
+ * destroyed afterwards.  cfg may be NULL (defaults). */
+geq_status geq_server_create(geq_context *ctx, const geq_server_config *cfg, geq_server **out);
+/* Queue one game (copied; the caller's buffers may be reused at once).
+ * GEQ_ERR_BUSY when max_queued requests wait; GEQ_ERR_INVALID_INPUT for a
+ * malformed graph (the same checks as geq_energy_game_run); a game whose
+ * estimated footprint alone exceeds a pipeline's budget: GEQ_ERR_OUT_OF_MEMORY. */
+geq_status geq_server_submit(geq_server *srv, const geq_game_graph *graph, uint64_t *ticket);
+/* Wait up to timeout_ms (< 0: forever) for request `ticket`.  GEQ_OK: *out
+ * is its solution (one game; free with geq_solution_free) and the ticket is
+ * retired.  GEQ_ERR_TIMEOUT: not finished yet (poll again).  Any other
+ * status: the request failed with that status (message in geq_last_error)
+ * and the ticket is retired.  GEQ_ERR_INVALID_INPUT for an unknown ticket. */
+geq_status geq_server_poll(geq_server *srv, uint64_t ticket, int32_t timeout_ms, geq_solution **out);
+void geq_server_get_stats(geq_server *srv, geq_server_stats *out);
+/* Finishes the batches in flight, fails the queued requests, frees all. */
+void geq_server_destroy(geq_server *srv);
+
 /* Solver tuning (autotuner output).  Zero fields keep the current value. */
 typedef struct geq_tuning {
   uint32_t blocks_per_sm;     /* resident 256-thread blocks per SM of the round kernel

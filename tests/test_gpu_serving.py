@@ -1,0 +1,117 @@
+"""The serving loop (geq_server_*): every result, solved in a mix of
+concurrently submitted requests, equals the same game solved alone."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import csr_from_edges
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def geq():
+    import gpuequiv_b200 as geq
+    return geq
+
+
+@pytest.fixture(scope="module")
+def ctx(geq):
+    c = geq.Context(0)
+    yield c
+    c.close()
+
+
+def _canon(offs, data):
+    offs = np.asarray(offs, np.int64)
+    return [tuple(sorted(int(x) for x in data[offs[v]:offs[v + 1]])) for v in range(len(offs) - 1)]
+
+
+def _games(geq, n):
+    from gpuequiv_b200 import synth
+    rows = synth.batched_manifest()["jobs"]
+    seeds = [r[0] for r in rows if r[1] <= 60_000][:n]
+    out = []
+    for seed in seeds:
+        src, dst, lab, p, q = synth.batched_lts(seed)
+        red, mp = geq.TransitionSystem.from_arrays(src, dst, lab).bisimilar_minimize()
+        out.append(geq.GameBuild.compare(red, int(mp[p]), int(mp[q])).game)
+    return out
+
+
+def _alone(geq, ctx, g):
+    offs, data, _ = geq.run_batch_raw([g], ctx)
+    return _canon(offs[0], data[0])
+
+
+def test_results_alone_equal_in_the_mix(geq, ctx):
+    from gpuequiv_b200.serving import Server
+    games = _games(geq, 160)
+    expect = [_alone(geq, ctx, g) for g in games]
+    with Server(ctx, n_pipelines=2, max_wait_us=500) as srv:
+        # submissions interleaved with polls: batches start while requests keep arriving
+        tickets = []
+        got = {}
+        for i, g in enumerate(games):
+            tickets.append(srv.submit(g))
+            if i % 16 == 15:
+                r = srv.poll(tickets[i - 15], timeout_ms=0)
+                if r is not None:
+                    got[i - 15] = _canon(r[0], r[1])
+        for i, t in enumerate(tickets):
+            if i not in got:
+                r = srv.poll(t, timeout_ms=60_000)
+                assert r is not None, f"request {i} not done"
+                got[i] = _canon(r[0], r[1])
+        st = srv.stats()
+    for i in range(len(games)):
+        assert got[i] == expect[i], f"game {i} differs from its solve alone"
+    assert st["completed"] == len(games) and st["failed"] == 0
+    assert st["games_in_batches"] == len(games)
+
+
+def test_admission_budget_splits_batches(geq, ctx):
+    from gpuequiv_b200.serving import Server
+    games = _games(geq, 40)
+    expect = [_alone(geq, ctx, g) for g in games]
+    budget = 2 * (40 << 20)  # two pipelines, about 40 MB each: several batches
+    with Server(ctx, n_pipelines=2, hbm_budget_bytes=budget, max_wait_us=2000) as srv:
+        tickets = [srv.submit(g) for g in games]
+        got = [_canon(*srv.poll(t)[:2]) for t in tickets]
+        st = srv.stats()
+    assert got == expect
+    assert st["batches"] > 1
+    assert st["max_batch_footprint"] <= budget // 2 or st["games_in_batches"] == st["batches"]
+
+
+def test_faulty_request_fails_alone(geq, ctx):
+    from gpuequiv_b200 import GeqError
+    from gpuequiv_b200.serving import Server
+    games = _games(geq, 6)
+    expect = [_alone(geq, ctx, g) for g in games]
+    # a successor index beyond the game: caught on the device at upload
+    row, col, wt, att = csr_from_edges(3, [(0, 1, [-1]), (1, 2, [0])], [True, False, False])
+    col = np.array(col, np.uint32)
+    col[1] = 7
+    bad = geq.GameGraph.from_csr(row, col, wt, att, geq.EnergyConf(6, 3))
+    with Server(ctx, n_pipelines=1, max_wait_us=20_000) as srv:
+        tickets = [srv.submit(g) for g in games[:3]] + [srv.submit(bad)] + [srv.submit(g) for g in games[3:]]
+        results = []
+        for t in tickets:
+            try:
+                r = srv.poll(t)
+                results.append(_canon(r[0], r[1]))
+            except GeqError as e:
+                results.append(e.name)
+    assert results[3] == "INVALID_INPUT"
+    assert results[:3] + results[4:] == expect
+
+
+def test_unknown_ticket_and_busy(geq, ctx):
+    from gpuequiv_b200 import GeqError
+    from gpuequiv_b200.serving import Server
+    with Server(ctx, n_pipelines=1) as srv:
+        with pytest.raises(GeqError) as e:
+            srv.poll(12345, timeout_ms=0)
+        assert e.value.name == "INVALID_INPUT"
