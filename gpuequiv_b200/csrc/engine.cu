@@ -98,7 +98,9 @@ struct Ctr {
   uint32_t done_blocks;
   uint32_t pad;
   uint32_t next_slot;  // k_round: next frontier slot to hand out (32 per grab)
-  uint32_t pad2;
+  uint32_t nbig;       // large positions queued by k_round for k_round_big
+  uint32_t next_big;   // k_round_big: next queue entry to hand out
+  uint32_t pad3;
   unsigned long long positions, edges, bytes, rounds;
 #if GEQ_PATH_PROFILE
   unsigned long long prof[32];
@@ -142,6 +144,7 @@ struct KParams {
   uint32_t *fpart;       // per-block set-bit counts of the bitmap (k_fcount): attackers, defenders
   uint32_t fblocks;      // blocks of k_fcount / k_ffill
   const uint32_t *abits; // attacker positions as a bitmap (mwords words)
+  uint32_t *bigq;        // frontier slots of the large positions of the round
 };
 
 // Energy-list descriptors (one u64 per position):
@@ -967,8 +970,7 @@ __device__ Res solve_position(const WarpCtx &x, const Cd &cd, uint32_t v) {
 // routines.
 template <class Cd>
 __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32_t *arena, unsigned long long cap,
-                            uint32_t v, uint32_t *scr, uint32_t &out_cnt, unsigned long long &edges,
-                            unsigned long long &bytes) {
+                            uint32_t v, uint32_t *scr, uint32_t &out_cnt, uint32_t &edges, uint32_t &bytes) {
   const uint32_t e0 = ld(p.row, v, p.n_nodes + 1, c), e1 = ld(p.row, (unsigned long long)v + 1, p.n_nodes + 1, c);
   const uint32_t d = e1 - e0;
   if (d == 0) return T_SKIPPED;
@@ -1008,7 +1010,7 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
     for (uint32_t q = 0; q < cv; q++)
       if (!ac_insert(scr, 0, n, om, cd.to_t(lelem(dv, q, arena, cap, c, p.ib, p.ibm)), true)) return T_BIG;
     edges += d;
-    bytes += 12ull + 4ull * cv + 16ull * d + 4ull * tot;
+    bytes += 12u + 4u * cv + 16u * d + 4u * tot;
     if (om == (1u << n) - 1u) return T_UNCHANGED;
     for (uint32_t q = 0; q < n; q++) SCR(TK + q) = cd.to_p(SCR(q));
     out_cnt = n;
@@ -1069,7 +1071,7 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
       n = ns;
     }
     edges += d;
-    bytes += 12ull + 16ull * d + 4ull * tot;
+    bytes += 12u + 16u * d + 4u * (uint32_t)tot;
   }
   // EnergyArray PartialEq (energy.rs:334-350) against the old list
   bool changed = n != cv;
@@ -1146,9 +1148,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
   uint32_t *arena = c->arena;
   const unsigned long long cap = c->arena_cap;
   WarpAlloc wa{0, 0};
-  unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0;  // warp routines (lane-uniform)
-  unsigned long long t_edges = 0, t_bytes = 0, t_pos = 0;  // thread path (per lane)
-  WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes, scr};
+  uint32_t t_edges = 0, t_bytes = 0, t_pos = 0;  // per lane, this launch
 #if GEQ_PATH_PROFILE
   unsigned long long prof_acc[16] = {};
   const long long t_all0 = clock64();
@@ -1191,10 +1191,19 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
         nd = mkdesc(off, need);
       }
     }
-    if (ts == T_CHANGED) t_bytes += 4ull * cnt;
+    if (ts == T_CHANGED) t_bytes += 4u * cnt;
     if (active && ts != T_BIG && CHECK_IDX(c, slot, p.n_nodes)) p.slot_new[slot] = (ts == T_CHANGED) ? nd : NONE_DESC;
-    // large positions: the whole warp on one position at a time
-    uint32_t big = __ballot_sync(FULL, ts == T_BIG);
+    // large positions go to k_round_big (a whole warp per position)
+    const uint32_t big = __ballot_sync(FULL, ts == T_BIG);
+    if (big) {
+      uint32_t b0 = 0;
+      if (lane == 0) b0 = atomicAdd(&c->nbig, (uint32_t)__popc(big));
+      b0 = __shfl_sync(FULL, b0, 0);
+      if (ts == T_BIG) {
+        const uint32_t k = b0 + (uint32_t)__popc(big & lanemask_lt());
+        if (CHECK_IDX(c, k, p.n_nodes)) p.bigq[k] = slot;
+      }
+    }
 #if GEQ_PATH_PROFILE
     const long long tq1 = clock64();
     if (lane == 0) { PROF_ADD(PF_CYC_THREAD, tq1 - tq0); PROF_ADD(PF_ITERS, 1); }
@@ -1208,33 +1217,11 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
       }
     }
 #endif
-    bool big_changed = false;
-    while (big) {
-      const uint32_t l = __ffs(big) - 1u;
-      big &= big - 1u;
-      const uint32_t vb = __shfl_sync(FULL, v, l);
-#if GEQ_PATH_PROFILE
-      if (lane == 0) {
-        PROF_ADD((p.flags[vb] & 1u) ? PF_B_ATT : PF_B_DEF, 1);
-        PROF_ADD(PF_B_DEG, p.row[vb + 1] - p.row[vb]);
-      }
-#endif
-      const Res r = solve_position(x, cd, vb);
-      if (r.st != R_SKIPPED) w_pos++;
-      if (lane == 0 && CHECK_IDX(c, base + l, p.n_nodes))
-        p.slot_new[base + l] = (r.st == R_CHANGED) ? r.d : NONE_DESC;
-      if (lane == l) big_changed = r.st == R_CHANGED;
-      if (r.st == R_OVERFLOW && lane == 0) mark_push(p, vb, stamp);  // retried after compaction
-    }
-#if GEQ_PATH_PROFILE
-    const long long tq2 = clock64();
-    if (lane == 0) PROF_ADD(PF_CYC_BIG, tq2 - tq1);
-#endif
-    push_preds_warp(p, c, sm, v, ts == T_CHANGED || big_changed, stamp, lane);
+    push_preds_warp(p, c, sm, v, ts == T_CHANGED, stamp, lane);
     if (ts == T_OVERFLOW) mark_push(p, v, stamp);
 #if GEQ_PATH_PROFILE
-    if (lane == 0) PROF_ADD(PF_CYC_PUSH, clock64() - tq2);
-    if ((ts == T_CHANGED || big_changed)) PROF_ADD(PF_PUSHED, p.rrow[v + 1] - p.rrow[v]);
+    if (lane == 0) PROF_ADD(PF_CYC_PUSH, clock64() - tq1);
+    if (ts == T_CHANGED) PROF_ADD(PF_PUSHED, p.rrow[v + 1] - p.rrow[v]);
 #endif
   }
 #if GEQ_PATH_PROFILE
@@ -1247,16 +1234,71 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
     if (lane == 0 && a) atomicAdd(&c->prof[i], a);
   }
 #endif
+  unsigned long long te = t_edges, tb = t_bytes, tp = t_pos;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    t_edges += __shfl_xor_sync(FULL, t_edges, o);
-    t_bytes += __shfl_xor_sync(FULL, t_bytes, o);
-    t_pos += __shfl_xor_sync(FULL, t_pos, o);
+    te += __shfl_xor_sync(FULL, te, o);
+    tb += __shfl_xor_sync(FULL, tb, o);
+    tp += __shfl_xor_sync(FULL, tp, o);
   }
-  if (lane == 0 && (t_pos || w_pos)) {
-    atomicAdd(&c->positions, t_pos + w_pos);
-    atomicAdd(&c->edges, t_edges + w_edges);
-    atomicAdd(&c->bytes, t_bytes + w_bytes);
+  if (lane == 0 && tp) {
+    atomicAdd(&c->positions, tp);
+    atomicAdd(&c->edges, te);
+    atomicAdd(&c->bytes, tb);
+  }
+}
+
+// The large positions k_round queued: one warp per position with the warp
+// routines (tree fold, register and bitmap paths), then its predecessors.
+template <class Cd>
+__global__ void __launch_bounds__(BLOCK, 2) k_round_big(const KParams p) {
+  __shared__ uint32_t smem[WARPS_PER_BLOCK * SM_WORDS];
+  __shared__ uint32_t tscr[WARPS_PER_BLOCK * TSCR * 32];
+  Ctr *c = p.ctr;
+  if (c->halt) return;
+  const uint32_t nb = c->nbig;
+  if (nb == 0) return;
+  const uint32_t cur = c->cur;
+  const uint32_t *F = cur ? p.front1 : p.front0;
+  const uint32_t stamp = c->stamp + 1u;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t *sm = smem + (threadIdx.x >> 5) * SM_WORDS;
+  uint32_t *scr = tscr + (threadIdx.x >> 5) * (TSCR * 32) + lane;
+  const Cd cd = make_codec<Cd>(p);
+  uint32_t *arena = c->arena;
+  const unsigned long long cap = c->arena_cap;
+  WarpAlloc wa{0, 0};
+  unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0;  // lane-uniform
+  WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes, scr};
+#if GEQ_PATH_PROFILE
+  const long long t0 = clock64();
+#endif
+  for (;;) {
+    uint32_t i = 0;
+    if (lane == 0) i = atomicAdd(&c->next_big, 1u);
+    i = __shfl_sync(FULL, i, 0);
+    if (i >= nb) break;
+    const uint32_t slot = ld(p.bigq, i, p.n_nodes, c);
+    const uint32_t v = ld(F, slot, p.n_nodes, c);
+#if GEQ_PATH_PROFILE
+    if (lane == 0) {
+      atomicAdd(&c->prof[(p.flags[v] & 1u) ? PF_B_ATT : PF_B_DEF], 1ull);
+      atomicAdd(&c->prof[PF_B_DEG], (unsigned long long)(p.row[v + 1] - p.row[v]));
+    }
+#endif
+    const Res r = solve_position(x, cd, v);
+    if (r.st != R_SKIPPED) w_pos++;
+    if (lane == 0 && CHECK_IDX(c, slot, p.n_nodes)) p.slot_new[slot] = (r.st == R_CHANGED) ? r.d : NONE_DESC;
+    push_preds_warp(p, c, sm, v, lane == 0 && r.st == R_CHANGED, stamp, lane);
+    if (r.st == R_OVERFLOW && lane == 0) mark_push(p, v, stamp);  // retried after compaction
+  }
+#if GEQ_PATH_PROFILE
+  if (lane == 0) atomicAdd(&c->prof[PF_CYC_BIG], (unsigned long long)(clock64() - t0));
+#endif
+  if (lane == 0 && w_pos) {
+    atomicAdd(&c->positions, w_pos);
+    atomicAdd(&c->edges, w_edges);
+    atomicAdd(&c->bytes, w_bytes);
   }
 }
 
@@ -1407,6 +1449,8 @@ __global__ void k_ffill(const KParams p) {
   if (blockIdx.x == gridDim.x - 1u && threadIdx.x == 0) {
     c->fsize[cur] = s_ta + s_pd + p.fpart[2 * blockIdx.x + 1];
     c->next_slot = 0u;
+    c->nbig = 0u;
+    c->next_big = 0u;
     if (c->overflow) c->halt = 1u;
   }
 }
@@ -1857,7 +1901,7 @@ struct DeviceGamesImpl {
   uint32_t *row = nullptr, *col = nullptr, *wt = nullptr, *rrow = nullptr, *rcol = nullptr;
   uint8_t *flags = nullptr;
   unsigned long long *desc = nullptr, *desc_init = nullptr, *slot_new = nullptr;
-  uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr, *fpart = nullptr, *abits = nullptr;
+  uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr, *fpart = nullptr, *abits = nullptr, *bigq = nullptr;
   uint32_t *init_data = nullptr;
   unsigned long long init_total = 0;
   char *inbuf = nullptr;  // row, col, wt, flags, reach, init_data, [desc_init], node bases
@@ -2059,6 +2103,8 @@ geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
   CU(cudaFuncSetAttribute(k_round<CodecGen, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round<CodecGen, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round<CodecGen, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round_big<CodecStd>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round_big<CodecGen>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int bps = 0;
   CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_round<CodecStd, 3>, BLOCK, 0));
   eng->tuning.blocks_per_sm = (uint32_t)std::max(2, std::min(bps, 3));
@@ -2202,7 +2248,8 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   if (!D.alloc(D.rrow, N + 1) || !D.alloc(D.rcol, M) || !D.alloc(D.desc, N) ||
       (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, 2 * ((N + 31) / 32)) ||
       !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1) ||
-      !D.alloc(D.fpart, 2 * (size_t)std::max(1, n_sms * 2)) || !D.alloc(D.abits, (N + 31) / 32))
+      !D.alloc(D.fpart, 2 * (size_t)std::max(1, n_sms * 2)) || !D.alloc(D.abits, (N + 31) / 32) ||
+      !D.alloc(D.bigq, N))
     return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
@@ -2255,6 +2302,7 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   kp.fpart = D.fpart;
   kp.fblocks = (uint32_t)std::max(1, n_sms * 2);
   kp.abits = D.abits;
+  kp.bigq = D.bigq;
   kp.el = D.conf.elements; kp.mx = D.conf.max; kp.eb = D.conf.energy_bits(); kp.em = D.conf.energy_mask();
   kp.ub = D.conf.update_bits(); kp.um = D.conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
@@ -2309,6 +2357,7 @@ static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent
   if (bps == 2) k_round<Cd, 2><<<grid, BLOCK, 0, S>>>(kp);
   else if (bps == 3) k_round<Cd, 3><<<grid, BLOCK, 0, S>>>(kp);
   else k_round<Cd, 4><<<grid, BLOCK, 0, S>>>(kp);
+  k_round_big<Cd><<<(unsigned)std::max(1, E.n_sms * 2), BLOCK, 0, S>>>(kp);
   if (eb) cudaEventRecord(eb, S);
   k_commit<<<(unsigned)std::max(1, E.n_sms * 2), 256, 0, S>>>(kp);
   k_fcount<<<kp.fblocks, 256, 0, S>>>(kp);
@@ -2409,7 +2458,7 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
       if (dg.generic) launch_round<CodecGen>(*this, dg.kp, S, ea, eb);
       else launch_round<CodecStd>(*this, dg.kp, S, ea, eb);
     }
-    launches += 4ull * R;
+    launches += 5ull * R;
     CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
     CU(cudaStreamSynchronize(S));
     const Ctr c = *s.h_ctr;
@@ -2694,7 +2743,8 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
   uint32_t *arena = a.arena;
   const unsigned long long cap = a.arena_cap;
   WarpAlloc wa{0, 0};
-  unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0, t_edges = 0, t_bytes = 0, t_pos = 0;
+  unsigned long long w_edges = 0, w_bytes = 0, w_pos = 0;
+  uint32_t t_edges = 0, t_bytes = 0, t_pos = 0;
   WarpCtx x{p, c, arena, cap, lane, sm, wa, w_edges, w_bytes, scr};
   __shared__ uint32_t s_cur, s_fs, s_stop;
   for (uint32_t r = 0;; r++) {
@@ -2738,7 +2788,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
           nd = mkdesc(off, need);
         }
       }
-      if (ts == T_CHANGED) t_bytes += 4ull * cnt;
+      if (ts == T_CHANGED) t_bytes += 4u * cnt;
       if (active && ts != T_BIG && CHECK_IDX(c, slot, p.n_nodes)) p.slot_new[slot] = (ts == T_CHANGED) ? nd : NONE_DESC;
       uint32_t big = __ballot_sync(FULL, ts == T_BIG);
       bool big_changed = false;
@@ -2777,16 +2827,17 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
     if (tid == 0) c->fsize[cur ^ 1u] = nn;
     __syncthreads();
   }
+  unsigned long long te = t_edges, tb = t_bytes, tp = t_pos;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    t_edges += __shfl_xor_sync(FULL, t_edges, o);
-    t_bytes += __shfl_xor_sync(FULL, t_bytes, o);
-    t_pos += __shfl_xor_sync(FULL, t_pos, o);
+    te += __shfl_xor_sync(FULL, te, o);
+    tb += __shfl_xor_sync(FULL, tb, o);
+    tp += __shfl_xor_sync(FULL, tp, o);
   }
   if (lane == 0) {
-    atomicAdd(&c->positions, t_pos + w_pos);
-    atomicAdd(&c->edges, t_edges + w_edges);
-    atomicAdd(&c->bytes, t_bytes + w_bytes);
+    atomicAdd(&c->positions, tp + w_pos);
+    atomicAdd(&c->edges, te + w_edges);
+    atomicAdd(&c->bytes, tb + w_bytes);
   }
   __syncthreads();
   if (c->overflow) {
