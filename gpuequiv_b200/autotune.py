@@ -12,7 +12,7 @@ import os
 
 from .energygame import Context, DeviceGames
 
-CANDIDATES = [(bps, r) for bps in (2, 3, 4) for r in (4, 8, 16)]
+CANDIDATES = [(bps, r) for bps in (3, 4, 5) for r in (4, 8, 16)]
 
 
 def _cache_path() -> str:

@@ -280,7 +280,7 @@ geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t) {
   geq_status st = ctx_engine(ctx, e);
   if (st) return st;
   if (!t) return fail(GEQ_ERR_INVALID_INPUT, "tuning is NULL");
-  if (t->blocks_per_sm) e->tuning.blocks_per_sm = std::min<uint32_t>(std::max<uint32_t>(t->blocks_per_sm, 2), 4);
+  if (t->blocks_per_sm) e->tuning.blocks_per_sm = std::min<uint32_t>(std::max<uint32_t>(t->blocks_per_sm, 2), 5);
   if (t->rounds_per_graph) e->tuning.rounds_per_graph = std::min<uint32_t>(t->rounds_per_graph, 256);
   if (t->small_limit) e->tuning.small_limit = std::min<uint32_t>(t->small_limit, 32);
   e->tuning.flags = t->flags;

@@ -2100,14 +2100,16 @@ geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
   CU(cudaFuncSetAttribute(k_round<CodecStd, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round<CodecStd, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round<CodecStd, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round<CodecStd, 5>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round<CodecGen, 2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round<CodecGen, 3>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round<CodecGen, 4>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CU(cudaFuncSetAttribute(k_round<CodecGen, 5>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round_big<CodecStd>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CU(cudaFuncSetAttribute(k_round_big<CodecGen>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   int bps = 0;
-  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_round<CodecStd, 3>, BLOCK, 0));
-  eng->tuning.blocks_per_sm = (uint32_t)std::max(2, std::min(bps, 3));
+  CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_round<CodecStd, 4>, BLOCK, 0));
+  eng->tuning.blocks_per_sm = (uint32_t)std::max(2, std::min(bps, 4));
   eng->tuning.rounds_per_graph = 8;
   eng->tuning.small_limit = 32;
   out = std::move(eng);
@@ -2351,12 +2353,13 @@ static geq_status compact(Engine &E, DeviceGamesImpl &dg, unsigned long long &la
 template <class Cd>
 static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent_t ea = nullptr,
                          cudaEvent_t eb = nullptr) {
-  const uint32_t bps = std::min<uint32_t>(std::max<uint32_t>(E.tuning.blocks_per_sm, 2), 4);
+  const uint32_t bps = std::min<uint32_t>(std::max<uint32_t>(E.tuning.blocks_per_sm, 2), 5);
   const unsigned grid = (unsigned)std::max<uint32_t>(1, E.n_sms * bps);
   if (ea) cudaEventRecord(ea, S);
   if (bps == 2) k_round<Cd, 2><<<grid, BLOCK, 0, S>>>(kp);
   else if (bps == 3) k_round<Cd, 3><<<grid, BLOCK, 0, S>>>(kp);
-  else k_round<Cd, 4><<<grid, BLOCK, 0, S>>>(kp);
+  else if (bps == 4) k_round<Cd, 4><<<grid, BLOCK, 0, S>>>(kp);
+  else k_round<Cd, 5><<<grid, BLOCK, 0, S>>>(kp);
   k_round_big<Cd><<<(unsigned)std::max(1, E.n_sms * 2), BLOCK, 0, S>>>(kp);
   if (eb) cudaEventRecord(eb, S);
   k_commit<<<(unsigned)std::max(1, E.n_sms * 2), 256, 0, S>>>(kp);

@@ -278,7 +278,7 @@ void geq_server_destroy(geq_server *srv);
 /* Solver tuning (autotuner output).  Zero fields keep the current value. */
 typedef struct geq_tuning {
   uint32_t blocks_per_sm;     /* resident 256-thread blocks per SM of the round kernel
-                                 (2, 3 or 4: selects the register budget) */
+                                 (2 to 5: selects the register budget) */
   uint32_t rounds_per_graph;  /* worklist rounds captured per CUDA graph launch */
   uint32_t small_limit;       /* candidates handled in registers per position (1..32) */
   uint32_t flags;             /* GEQ_TUNE_* bits */

@@ -23,6 +23,9 @@ MODES = {
     "generic": dict(flags=1),
     "generic_large": dict(flags=3),
     "nograph": dict(flags=4),
+    # every register budget of the round kernel
+    "bps2": dict(blocks_per_sm=2, rounds_per_graph=3),
+    "bps5": dict(blocks_per_sm=5, rounds_per_graph=16),
 }
 
 
