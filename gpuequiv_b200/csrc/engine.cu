@@ -720,14 +720,15 @@ __device__ __noinline__ Res defend_small(const WarpCtx &x, const Cd &cd, unsigne
 // antichain outgrows TK members or one combination step TW pairs.
 template <class Cd>
 __device__ Res defend_tree(const WarpCtx &x, const Cd &cd, unsigned long long e0, unsigned long long e1,
-                           unsigned long long dv, bool &fits) {
+                           unsigned long long dv, bool &fits, bool &empty) {
   const uint32_t lane = x.lane;
   uint32_t *scr = x.scr;
   uint32_t n = 0, om = 0, tot = 0;
-  bool ok = true, first = true;
+  bool ok = true, first = true, emp = false;
   for (unsigned long long k = e0 + lane; k < e1; k += 32) {
     const EdgeInfo e = edge_info(x, k);
     tot += e.cw;
+    emp |= e.cw == 0u;
     if (!ok) continue;
     const auto pu = cd.prep(e.u);
     if (first) {
@@ -746,6 +747,9 @@ __device__ Res defend_tree(const WarpCtx &x, const Cd &cd, unsigned long long e0
     }
   }
   fits = false;
+  // skipped while a successor has no energies (energygame.rs:789-792)
+  empty = __any_sync(FULL, emp);
+  if (empty) return Res{R_SKIPPED, 0};
   if (__any_sync(FULL, !ok)) return Res{R_UNCHANGED, 0};
   const uint32_t dl = (uint32_t)min(32ull, e1 - e0);
   for (uint32_t st = 1; st < dl; st <<= 1) {
@@ -924,6 +928,18 @@ __device__ Res solve_position(const WarpCtx &x, const Cd &cd, uint32_t v) {
     if constexpr (Cd::kBitmap) { const Res r = attack_bitmap(x, cd, e0, e1, dv); PROF_WARP(x.c, PF_AB_N, t0); return r; }
     else return attack_list(x, cd, e0, e1, dv);
   }
+  if (d >= 2u && x.p.small_limit > 0) {
+    // the tree fold reads every successor's list and sees the empty ones
+    bool fits = false, emp = false;
+    const Res r = defend_tree(x, cd, e0, e1, dv, fits, emp);
+    if (emp) { PROF_WARP(x.c, PF_DK_N, t0); return Res{R_SKIPPED, 0}; }
+    if (fits) {
+      x.edges += d;
+      x.bytes += 12ull;
+      PROF_WARP(x.c, PF_DT_N, t0);
+      return r;
+    }
+  }
   // defender: skipped while a successor has no energies (energygame.rs:789-792)
   bool empty = false;
   for (unsigned long long k0 = e0; k0 < e1; k0 += 32) {
@@ -943,11 +959,6 @@ __device__ Res solve_position(const WarpCtx &x, const Cd &cd, uint32_t v) {
     const Res r = defend_single(x, cd, shfl_edge(e, 0), dv);
     PROF_WARP(x.c, PF_D1_N, t0);
     return r;
-  }
-  if (x.p.small_limit > 0) {
-    bool fits = false;
-    const Res r = defend_tree(x, cd, e0, e1, dv, fits);
-    if (fits) { PROF_WARP(x.c, PF_DT_N, t0); return r; }
   }
   if (d <= 32u && x.p.small_limit > 0) {
     bool fits = false;
@@ -1251,7 +1262,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
 // The large positions k_round queued: one warp per position with the warp
 // routines (tree fold, register and bitmap paths), then its predecessors.
 template <class Cd>
-__global__ void __launch_bounds__(BLOCK, 2) k_round_big(const KParams p) {
+__global__ void __launch_bounds__(BLOCK, 3) k_round_big(const KParams p) {
   __shared__ uint32_t smem[WARPS_PER_BLOCK * SM_WORDS];
   __shared__ uint32_t tscr[WARPS_PER_BLOCK * TSCR * 32];
   Ctr *c = p.ctr;
@@ -2360,7 +2371,7 @@ static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent
   else if (bps == 3) k_round<Cd, 3><<<grid, BLOCK, 0, S>>>(kp);
   else if (bps == 4) k_round<Cd, 4><<<grid, BLOCK, 0, S>>>(kp);
   else k_round<Cd, 5><<<grid, BLOCK, 0, S>>>(kp);
-  k_round_big<Cd><<<(unsigned)std::max(1, E.n_sms * 2), BLOCK, 0, S>>>(kp);
+  k_round_big<Cd><<<(unsigned)std::max(1, E.n_sms * 3), BLOCK, 0, S>>>(kp);
   if (eb) cudaEventRecord(eb, S);
   k_commit<<<(unsigned)std::max(1, E.n_sms * 2), 256, 0, S>>>(kp);
   k_fcount<<<kp.fblocks, 256, 0, S>>>(kp);
