@@ -377,6 +377,16 @@ geq_status geq_energy_game_run_batch(geq_context *ctx, uint32_t n_games, const g
   if (st) return st;
   std::vector<GameInput> in;
   if ((st = make_inputs(n_games, graphs, initial, to_reach, n_to_reach, in))) return st;
+  if (n_games == 1) {
+    // a small single game: one launch of the one-block solver
+    std::unique_ptr<geq_solution> sol(new geq_solution());
+    bool handled = false;
+    if ((st = e->solve_small(in[0], *sol, handled))) return st;
+    if (handled) {
+      *out = sol.release();
+      return GEQ_OK;
+    }
+  }
   GamesPtr dg;
   if ((st = e->upload(in, dg))) return st;
   std::unique_ptr<geq_solution> sol(new geq_solution());

@@ -2641,6 +2641,8 @@ struct StaticArgs {
   unsigned long long arena_cap;  // words
   unsigned long long *out_off;   // n_nodes + 1 result offsets
 };
+// Games up to these sizes take the one-block path in geq_energy_game_run.
+constexpr unsigned long long SMALL_GAME_POSITIONS = 4096, SMALL_GAME_EDGES = 65536;
 // Ctr::pad bits of the static solve
 constexpr uint32_t SERR_COL = 1u, SERR_WEIGHT = 2u, SERR_ARENA = 4u, SERR_ROUNDS = 8u;
 
@@ -2897,6 +2899,72 @@ static geq_status static_scratch(int device, unsigned char *&out) {
   return GEQ_OK;
 }
 
+// Layout of a one-block solve (k_solve_static) inside one memory block:
+// control block, the game, reverse CSR, descriptors, frontiers, result
+// offsets, 256-byte aligned, then the energy arena up to the block's end.
+struct BlockLayout {
+  size_t ctr, row, col, wt, flags, reach, rrow, rcol, desc, slot, mark, f0, f1, out, top;
+};
+static BlockLayout block_layout(unsigned long long N, unsigned long long M, uint32_t n_reach) {
+  BlockLayout L{};
+  size_t top = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = top;
+    top = (top + std::max<size_t>(bytes, 1) + 255) & ~size_t(255);
+    return o;
+  };
+  L.ctr = take(sizeof(Ctr));
+  L.row = take((N + 1) * 4);
+  L.col = take(M * 4);
+  L.wt = take(M * 4);
+  L.flags = take(N);
+  L.reach = take((size_t)n_reach * 4);
+  L.rrow = take((N + 1) * 4);
+  L.rcol = take(M * 4);
+  L.desc = take(N * 8);
+  L.slot = take(N * 8);
+  L.mark = take(std::max<unsigned long long>(N, 2 * ((N + 31) / 32)) * 4);
+  L.f0 = take(N * 4);
+  L.f1 = take(N * 4);
+  L.out = take((N + 1) * 8);
+  L.top = top;
+  return L;
+}
+static void block_params(const BlockLayout &L, unsigned char *base, size_t bytes, unsigned long long N,
+                         unsigned long long M, const Conf &conf, const geq_tuning &t, bool explicit_reach,
+                         uint32_t n_reach, KParams &kp, StaticArgs &sa) {
+  kp = KParams{};
+  kp.row = (const uint32_t *)(base + L.row);
+  kp.col = (const uint32_t *)(base + L.col);
+  kp.wt = (const uint32_t *)(base + L.wt);
+  kp.rrow = (const uint32_t *)(base + L.rrow);
+  kp.rcol = (const uint32_t *)(base + L.rcol);
+  kp.flags = (const uint8_t *)(base + L.flags);
+  kp.desc = (unsigned long long *)(base + L.desc);
+  kp.mark = (uint32_t *)(base + L.mark);
+  kp.front0 = (uint32_t *)(base + L.f0);
+  kp.front1 = (uint32_t *)(base + L.f1);
+  kp.slot_new = (unsigned long long *)(base + L.slot);
+  kp.ctr = (Ctr *)(base + L.ctr);
+  kp.n_nodes = N;
+  kp.n_edges = M;
+  kp.mwords = (uint32_t)((N + 31) / 32);
+  kp.el = conf.elements; kp.mx = conf.max; kp.eb = conf.energy_bits(); kp.em = conf.energy_mask();
+  kp.ub = conf.update_bits(); kp.um = conf.update_mask();
+  kp.small_limit = (t.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(t.small_limit, 32);
+  kp.thread_path = (t.flags & (GEQ_TUNE_FORCE_LARGE | GEQ_TUNE_NO_THREAD_PATH)) ? 0u : 1u;
+  kp.ib = conf.elements * conf.energy_bits();
+  kp.ibm = kp.ib >= 32 ? 0xFFFFFFFFu : ((1u << kp.ib) - 1u);
+  kp.inl = std::min<uint32_t>(7u, 60u / kp.ib);
+  sa = StaticArgs{};
+  sa.reach = explicit_reach ? (const uint32_t *)(base + L.reach) : nullptr;
+  sa.n_reach = explicit_reach ? n_reach : 0u;
+  sa.max_rounds = 1u << 20;
+  sa.arena = (uint32_t *)(base + L.top);
+  sa.arena_cap = (bytes - L.top) / 4;
+  sa.out_off = (unsigned long long *)(base + L.out);
+}
+
 geq_status Engine::run_static(int device, const geq_game_graph &g, const uint32_t *to_reach, uint32_t n_reach,
                               uint64_t *offsets, uint32_t *data, uint64_t data_cap, uint64_t *n_words,
                               geq_solve_stats *stats) {
@@ -2913,65 +2981,27 @@ geq_status Engine::run_static(int device, const geq_game_graph &g, const uint32_
   if (!conf.supported())
     return fail(GEQ_ERR_UNSUPPORTED, "EnergyConf {%u, %u} is outside the device codecs", conf.elements, conf.max);
   const unsigned long long N = g.n_vertices, M = g.row_offsets[g.n_vertices];
-  // scratch layout, 256-byte aligned pieces
-  size_t top = 0;
-  auto take = [&](size_t bytes) {
-    const size_t o = top;
-    top = (top + std::max<size_t>(bytes, 1) + 255) & ~size_t(255);
-    return o;
-  };
-  const size_t o_ctr = take(sizeof(Ctr)), o_row = take((N + 1) * 4), o_col = take(M * 4), o_wt = take(M * 4),
-               o_flags = take(N), o_reach = take((size_t)n_reach * 4), o_rrow = take((N + 1) * 4),
-               o_rcol = take(M * 4), o_desc = take(N * 8), o_slot = take(N * 8),
-               o_mark = take(std::max<unsigned long long>(N, 2 * ((N + 31) / 32)) * 4),
-               o_f0 = take(N * 4), o_f1 = take(N * 4), o_out = take((N + 1) * 8);
+  const BlockLayout L = block_layout(N, M, n_reach);
   const size_t min_arena = 4096 * 4;
-  if (N >= 0xFFFFFFF0ull || M >= 0xFFFFFFF0ull || top + min_arena > GEQ_STATIC_SCRATCH_BYTES)
+  if (N >= 0xFFFFFFF0ull || M >= 0xFFFFFFF0ull || L.top + min_arena > GEQ_STATIC_SCRATCH_BYTES)
     return fail(GEQ_ERR_UNSUPPORTED,
                 "game of %llu positions / %llu edges needs %zu bytes of the %u-byte static scratch",
-                N, M, top + min_arena, (unsigned)GEQ_STATIC_SCRATCH_BYTES);
+                N, M, L.top + min_arena, (unsigned)GEQ_STATIC_SCRATCH_BYTES);
   unsigned char *base = nullptr;
   geq_status rc = static_scratch(device, base);
   if (rc) return rc;
-  KParams kp{};
-  kp.row = (const uint32_t *)(base + o_row);
-  kp.col = (const uint32_t *)(base + o_col);
-  kp.wt = (const uint32_t *)(base + o_wt);
-  kp.rrow = (const uint32_t *)(base + o_rrow);
-  kp.rcol = (const uint32_t *)(base + o_rcol);
-  kp.flags = (const uint8_t *)(base + o_flags);
-  kp.desc = (unsigned long long *)(base + o_desc);
-  kp.mark = (uint32_t *)(base + o_mark);
-  kp.front0 = (uint32_t *)(base + o_f0);
-  kp.front1 = (uint32_t *)(base + o_f1);
-  kp.slot_new = (unsigned long long *)(base + o_slot);
-  kp.ctr = (Ctr *)(base + o_ctr);
-  kp.n_nodes = N;
-  kp.n_edges = M;
-  kp.mwords = (uint32_t)((N + 31) / 32);
-  kp.el = conf.elements; kp.mx = conf.max; kp.eb = conf.energy_bits(); kp.em = conf.energy_mask();
-  kp.ub = conf.update_bits(); kp.um = conf.update_mask();
-  kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
-  kp.thread_path = (tuning.flags & (GEQ_TUNE_FORCE_LARGE | GEQ_TUNE_NO_THREAD_PATH)) ? 0u : 1u;
-  kp.ib = conf.elements * conf.energy_bits();
-  kp.ibm = kp.ib >= 32 ? 0xFFFFFFFFu : ((1u << kp.ib) - 1u);
-  kp.inl = std::min<uint32_t>(7u, 60u / kp.ib);
-  StaticArgs sa{};
-  sa.reach = to_reach ? (const uint32_t *)(base + o_reach) : nullptr;
-  sa.n_reach = to_reach ? n_reach : 0u;
-  sa.max_rounds = 1u << 20;
-  sa.arena = (uint32_t *)(base + top);
-  sa.arena_cap = (GEQ_STATIC_SCRATCH_BYTES - top) / 4;
-  sa.out_off = (unsigned long long *)(base + o_out);
+  KParams kp;
+  StaticArgs sa;
+  block_params(L, base, GEQ_STATIC_SCRATCH_BYTES, N, M, conf, tuning, to_reach != nullptr, n_reach, kp, sa);
   // the game, straight from the caller's buffers
   CU(cudaEventRecord(s.ev0, S));
-  CU(cudaMemcpyAsync(base + o_row, g.row_offsets, (N + 1) * 4, cudaMemcpyHostToDevice, S));
+  CU(cudaMemcpyAsync(base + L.row, g.row_offsets, (N + 1) * 4, cudaMemcpyHostToDevice, S));
   if (M) {
-    CU(cudaMemcpyAsync(base + o_col, g.column_indices, M * 4, cudaMemcpyHostToDevice, S));
-    CU(cudaMemcpyAsync(base + o_wt, g.weights, M * 4, cudaMemcpyHostToDevice, S));
+    CU(cudaMemcpyAsync(base + L.col, g.column_indices, M * 4, cudaMemcpyHostToDevice, S));
+    CU(cudaMemcpyAsync(base + L.wt, g.weights, M * 4, cudaMemcpyHostToDevice, S));
   }
-  if (N) CU(cudaMemcpyAsync(base + o_flags, g.attacker_pos, N, cudaMemcpyHostToDevice, S));
-  if (to_reach && n_reach) CU(cudaMemcpyAsync(base + o_reach, to_reach, (size_t)n_reach * 4, cudaMemcpyHostToDevice, S));
+  if (N) CU(cudaMemcpyAsync(base + L.flags, g.attacker_pos, N, cudaMemcpyHostToDevice, S));
+  if (to_reach && n_reach) CU(cudaMemcpyAsync(base + L.reach, to_reach, (size_t)n_reach * 4, cudaMemcpyHostToDevice, S));
   const bool generic = !conf.standard() || (tuning.flags & GEQ_TUNE_FORCE_GENERIC);
   if (generic) k_solve_static<CodecGen><<<1, BLOCK, 0, S>>>(kp, sa);
   else k_solve_static<CodecStd><<<1, BLOCK, 0, S>>>(kp, sa);
@@ -3007,6 +3037,84 @@ geq_status Engine::run_static(int device, const geq_game_graph &g, const uint32_
     stats->kernel_launches = 1;
     stats->device_ms = ms;
   }
+  return GEQ_OK;
+}
+
+
+// One small game in one launch of the one-block solver, in a pooled device
+// block: one upload from page-locked staging, one kernel, two read-backs.  A
+// game whose lists outgrow the block's arena is left to the general path
+// (handled = false), as is everything outside the limits.
+geq_status Engine::solve_small(const GameInput &gi, geq_solution &sol, bool &handled) {
+  handled = false;
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  const Conf conf(gi.g.conf);
+  const unsigned long long N = gi.g.n_vertices, M = gi.g.row_offsets[gi.g.n_vertices];
+  if (gi.init || tuning.flags || N > SMALL_GAME_POSITIONS || M > SMALL_GAME_EDGES || !conf.supported())
+    return GEQ_OK;
+  const BlockLayout L = block_layout(N, M, gi.n_reach);
+  const size_t bytes = L.top + 4 * (16 * (size_t)(N + M) + 65536);
+  unsigned char *base = (unsigned char *)s.pool.get(bytes);
+  if (!base) return GEQ_OK;
+  struct Give {
+    DevPool &pool;
+    void *p;
+    size_t b;
+    ~Give() { pool.put(p, b); }
+  } give{s.pool, base, bytes};
+  geq_status rc = ensure_stage(s, L.rrow);
+  if (rc) return rc;
+  char *H = s.stage;
+  std::memcpy(H + L.row, gi.g.row_offsets, (N + 1) * 4);
+  if (M) {
+    std::memcpy(H + L.col, gi.g.column_indices, M * 4);
+    std::memcpy(H + L.wt, gi.g.weights, M * 4);
+  }
+  if (N) std::memcpy(H + L.flags, gi.g.attacker_pos, N);
+  if (gi.n_reach) std::memcpy(H + L.reach, gi.to_reach, (size_t)gi.n_reach * 4);
+  KParams kp;
+  StaticArgs sa;
+  block_params(L, base, bytes, N, M, conf, tuning, true, gi.n_reach, kp, sa);
+  CU(cudaEventRecord(s.ev0, S));
+  CU(cudaMemcpyAsync(base, H, L.rrow, cudaMemcpyHostToDevice, S));
+  if (!conf.standard()) k_solve_static<CodecGen><<<1, BLOCK, 0, S>>>(kp, sa);
+  else k_solve_static<CodecStd><<<1, BLOCK, 0, S>>>(kp, sa);
+  CU(cudaGetLastError());
+  sol.n_offsets = N + 1;
+  if (!sol.off_buf.alloc(s.hpool, (N + 1) * 8)) return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for offsets");
+  CU(cudaMemcpyAsync(s.h_ctr, kp.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
+  CU(cudaMemcpyAsync(sol.off_buf.p, sa.out_off, (N + 1) * 8, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  const Ctr h = *s.h_ctr;
+  if ((h.pad & SERR_ARENA) || (h.error & ~DERR_BOUNDS)) {
+    sol.off_buf.reset();
+    return GEQ_OK;  // the general path grows its arena
+  }
+  handled = true;
+  if (h.pad & SERR_COL) return fail(GEQ_ERR_INVALID_INPUT, "Node index too high: a successor index is out of range");
+  if (h.pad & SERR_WEIGHT) return fail(GEQ_ERR_INVALID_INPUT, "an edge update names no element or sets padding bits");
+  if (h.error) return fail(GEQ_ERR_INTERNAL, "device error %u (line %u)", h.error, h.err_line);
+  if (h.pad & SERR_ROUNDS) return fail(GEQ_ERR_TIMEOUT, "no fixpoint after %u rounds", sa.max_rounds);
+  const unsigned long long total = ((const uint64_t *)sol.off_buf.p)[N];
+  sol.n_words = total;
+  if (!sol.data_buf.alloc(s.hpool, total * 4)) return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu words", total);
+  if (total) CU(cudaMemcpyAsync(sol.data_buf.p, sa.arena + h.arena_top, total * 4, cudaMemcpyDeviceToHost, S));
+  CU(cudaEventRecord(s.ev1, S));
+  CU(cudaStreamSynchronize(S));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, s.ev0, s.ev1);
+  sol.energy_size = 1;
+  sol.n_vertices.assign(1, (uint32_t)N);
+  sol.offsets_base.assign(1, 0);
+  sol.data_base.assign(1, 0);
+  sol.stats = geq_solve_stats{};
+  sol.stats.rounds = h.rounds;
+  sol.stats.positions_computed = h.positions;
+  sol.stats.edges_relaxed = h.edges;
+  sol.stats.algorithmic_bytes = h.bytes;
+  sol.stats.kernel_launches = 1;
+  sol.stats.device_ms = ms;
   return GEQ_OK;
 }
 

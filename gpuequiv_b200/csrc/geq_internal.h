@@ -173,6 +173,9 @@ class Engine {
   // become game g of the solution.
   geq_status download_selected(DeviceGamesImpl &dg, const std::vector<uint32_t> &first,
                                const std::vector<uint32_t> &count, geq_solution &sol);
+  // One small game (no initial lists, default tuning) by the one-block
+  // solver in a pooled block; handled = false leaves it to upload/solve.
+  geq_status solve_small(const GameInput &gi, geq_solution &sol, bool &handled);
   // geq_energy_game_run_static: one game in the file-scope scratch, no allocation.
   geq_status run_static(int device, const geq_game_graph &g, const uint32_t *to_reach, uint32_t n_reach,
                         uint64_t *offsets, uint32_t *data, uint64_t data_cap, uint64_t *n_words,
