@@ -271,8 +271,12 @@ def run_serving(ctx, graphs, lam: float, seconds: float, seed: int) -> dict:
     t_sub = np.zeros(n)
     t_done = np.zeros(n)
     with Server(ctx) as srv:
-        for g in graphs[:32]:  # warm the pipelines (graphs, pools)
+        # warm the pipelines (CUDA graphs, device and host pools): single
+        # requests, then a burst
+        for g in graphs[:32]:
             srv.poll(srv.submit(g))
+        for t in [srv.submit(g) for g in graphs[:512]]:
+            srv.poll(t)
         q: "queue.Queue" = queue.Queue()
 
         def poller():

@@ -47,6 +47,7 @@
 #include <mutex>
 #include <set>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "codec.cuh"
@@ -1770,15 +1771,19 @@ class DevPool {
     }
     return (b + (8u << 20) - 1) & ~size_t((8u << 20) - 1);
   }
+  // A cached block of the request's size class, or of a larger class up to
+  // 4x: a serving loop's batches vary in size, and reusing a larger block
+  // avoids a cudaMalloc for every new size.
   void *get(size_t bytes) {
     const size_t r = round_size(bytes);
-    auto it = free_.find(r);
-    if (it != free_.end() && !it->second.empty()) {
-      void *p = it->second.back();
-      it->second.pop_back();
-      cached_ -= r;
-      return p;
-    }
+    for (auto it = free_.lower_bound(r); it != free_.end() && it->first <= 4 * r; ++it)
+      if (!it->second.empty()) {
+        void *p = it->second.back();
+        it->second.pop_back();
+        cached_ -= it->first;
+        size_[p] = it->first;
+        return p;
+      }
     void *p = nullptr;
     if (cudaMalloc(&p, r) != cudaSuccess) {
       cudaGetLastError();
@@ -1788,11 +1793,15 @@ class DevPool {
         return nullptr;
       }
     }
+    size_[p] = r;
     return p;
   }
+  // Back to the cache under the block's real size (`bytes` is the request).
   void put(void *p, size_t bytes) {
     if (!p) return;
-    const size_t r = round_size(bytes);
+    auto it = size_.find(p);
+    const size_t r = it != size_.end() ? it->second : round_size(bytes);
+    if (it != size_.end()) size_.erase(it);
     if (cached_ + r > limit_) {
       cudaFree(p);
       return;
@@ -1810,6 +1819,7 @@ class DevPool {
 
  private:
   std::map<size_t, std::vector<void *>> free_;
+  std::unordered_map<void *, size_t> size_;  // blocks handed out: real size
   size_t cached_ = 0;
   size_t limit_ = (size_t)16 << 30;
 };
@@ -1826,14 +1836,16 @@ size_t HostPool::round_size(size_t b) {
 void *HostPool::get(size_t bytes, size_t &cap) {
   cap = round_size(bytes);
   {
+    // the request's size class or a larger one up to 4x (see DevPool::get)
     std::lock_guard<std::mutex> g(mu_);
-    auto it = free_.find(cap);
-    if (it != free_.end() && !it->second.empty()) {
-      void *p = it->second.back();
-      it->second.pop_back();
-      cached_ -= cap;
-      return p;
-    }
+    for (auto it = free_.lower_bound(cap); it != free_.end() && it->first <= 4 * cap; ++it)
+      if (!it->second.empty()) {
+        void *p = it->second.back();
+        it->second.pop_back();
+        cached_ -= it->first;
+        cap = it->first;
+        return p;
+      }
   }
   void *p = nullptr;
   if (cudaHostAlloc(&p, cap, cudaHostAllocDefault) != cudaSuccess) {

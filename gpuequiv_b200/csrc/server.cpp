@@ -100,6 +100,21 @@ void run_batch(Engine &e, std::vector<Request *> &batch) {
     gi.to_reach = r.reach.data();
     gi.n_reach = (uint32_t)r.reach.size();
   }
+  if (batch.size() == 1) {
+    // a lone small game: one launch of the one-block solver
+    std::unique_ptr<geq_solution> one(new geq_solution());
+    bool handled = false;
+    const geq_status st = e.solve_small(in[0], *one, handled);
+    if (st) {
+      batch[0]->st = st;
+      batch[0]->err = geq_last_error();
+      return;
+    }
+    if (handled) {
+      batch[0]->sol = std::move(one);
+      return;
+    }
+  }
   GamesPtr dg;
   geq_solution sol;
   geq_status st = e.upload(in, dg);
