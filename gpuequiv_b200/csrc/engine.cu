@@ -142,8 +142,8 @@ struct KParams {
   uint32_t thread_path;  // 1: lane-per-position path for small positions
   uint32_t ib, ibm, inl; // inline descriptors: bits per energy, its mask, capacity
   uint32_t mwords;       // words of one half of the frontier bitmap `mark`
-  uint32_t *fpart;       // per-block set-bit counts of the bitmap (k_fcount): attackers, defenders
-  uint32_t fblocks;      // blocks of k_fcount / k_ffill
+  uint32_t *fpart;       // per-block set-bit counts of the bitmap (k_commit / k_fcount): attackers, defenders
+  uint32_t fblocks;      // blocks of k_commit, k_fcount, k_ffill
   const uint32_t *abits; // attacker positions as a bitmap (mwords words)
   uint32_t *bigq;        // frontier slots of the large positions of the round
 };
@@ -1100,9 +1100,9 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
 
 // The next frontier is a bitmap: one bit per position in each of two halves
 // of `mark`, chosen by the parity of the stamp of the round that pushes.
-// k_fcount / k_ffill turn the half into the frontier list in position order
-// after the round, and k_commit clears the half that the round after next
-// uses.  The bitmap (N/16 bytes) stays in L2.
+// After the round k_commit counts the half's bits per block and clears the
+// half that the round after next uses, and k_ffill turns the half into the
+// frontier list in position order.  The bitmap (N/16 bytes) stays in L2.
 __device__ __forceinline__ void mark_push(const KParams &p, uint32_t u, uint32_t stamp) {
   atomicOr(p.mark + (stamp & 1u) * p.mwords + (u >> 5), 1u << (u & 31u));
 }
@@ -1314,30 +1314,65 @@ __global__ void __launch_bounds__(BLOCK, 3) k_round_big(const KParams p) {
   }
 }
 
-// Publish the round's new descriptors and advance to the next frontier.
+// Publish the round's new descriptors, clear the bitmap half of the round
+// after next, count this round's pushes per block (for k_ffill) and advance
+// to the next round.  Launched with exactly fblocks blocks.
 __global__ void k_commit(const KParams p) {
   Ctr *c = p.ctr;
   // k_round only raises `overflow` (never `halt`) for arena exhaustion, so
-  // the round that overflowed still commits its finished positions; the
-  // last block then halts the remaining rounds of the graph until the host
-  // has compacted the arena.
+  // the round that overflowed still commits its finished positions; k_ffill
+  // then halts the remaining rounds of the graph until the host has
+  // compacted the arena.
   if (c->halt) return;
+  __shared__ uint32_t wsum[2 * WARPS_PER_BLOCK];
+  __shared__ bool last;
   const uint32_t cur = c->cur;
   const uint32_t fs = c->fsize[cur];
-  if (fs == 0) return;
-  const uint32_t *F = cur ? p.front1 : p.front0;
-  // the next round pushes with stamp + 2: clear that half of the bitmap
-  uint32_t *mh = p.mark + (c->stamp & 1u) * p.mwords;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.mwords; i += gridDim.x * blockDim.x) mh[i] = 0u;
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < fs; s += gridDim.x * blockDim.x) {
-    const unsigned long long d = p.slot_new[s];
-    if (d != NONE_DESC) {
-      const uint32_t v = F[s];
-      if (CHECK_IDX(c, v, p.n_nodes)) p.desc[v] = d;
+  const uint32_t stamp = c->stamp;
+  if (fs) {
+    const uint32_t *F = cur ? p.front1 : p.front0;
+    // the round after next pushes with stamp + 2: clear that half
+    uint32_t *mh = p.mark + (stamp & 1u) * p.mwords;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < p.mwords; i += gridDim.x * blockDim.x) mh[i] = 0u;
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < fs; s += gridDim.x * blockDim.x) {
+      const unsigned long long d = p.slot_new[s];
+      if (d != NONE_DESC) {
+        const uint32_t v = F[s];
+        if (CHECK_IDX(c, v, p.n_nodes)) p.desc[v] = d;
+      }
+    }
+  }
+  // this round's pushes (stamp + 1 half): attackers and defenders per block.
+  // With an empty frontier both halves are clear and the counts are zero.
+  {
+    const uint32_t *mh = p.mark + ((stamp + 1u) & 1u) * p.mwords;
+    const uint32_t per = (p.mwords + gridDim.x - 1u) / gridDim.x;
+    const uint32_t b = min(p.mwords, blockIdx.x * per), e = min(p.mwords, b + per);
+    uint32_t sa = 0, sd = 0;
+    for (uint32_t i = b + threadIdx.x; i < e; i += blockDim.x) {
+      const uint32_t w = mh[i], a = p.abits[i];
+      sa += (uint32_t)__popc(w & a);
+      sd += (uint32_t)__popc(w & ~a);
+    }
+    sa = __reduce_add_sync(FULL, sa);
+    sd = __reduce_add_sync(FULL, sd);
+    if ((threadIdx.x & 31u) == 0u) {
+      wsum[threadIdx.x >> 5] = sa;
+      wsum[WARPS_PER_BLOCK + (threadIdx.x >> 5)] = sd;
     }
   }
   __syncthreads();
-  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    uint32_t ta = 0, td = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      ta += wsum[w];
+      td += wsum[WARPS_PER_BLOCK + w];
+    }
+    p.fpart[2 * blockIdx.x] = ta;
+    p.fpart[2 * blockIdx.x + 1] = td;
+  }
+  if (!fs) return;
+  __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     last = atomicAdd(&c->done_blocks, 1u) == gridDim.x - 1u;
@@ -1347,7 +1382,7 @@ __global__ void k_commit(const KParams p) {
     __threadfence();
     c->fsize[cur] = 0u;
     c->cur = cur ^ 1u;
-    c->stamp = c->stamp + 1u;
+    c->stamp = stamp + 1u;
     c->rounds = c->rounds + 1ull;
     c->done_blocks = 0u;
     __threadfence();
@@ -1385,7 +1420,8 @@ __device__ uint32_t block_fill_bits(const uint32_t *mh, uint32_t b, uint32_t e, 
   return total;
 }
 
-// k_fcount + k_ffill: the next frontier (stamp parity half of the bitmap)
+// k_fcount (after the initial pushes; k_commit counts after a round) +
+// k_ffill: the next frontier (stamp parity half of the bitmap)
 // as a list in position order, attackers first, then defenders, so that a
 // warp of the next round mostly meets one kind of position.  The last k_ffill
 // block publishes its size, resets the slot counter and, after an arena
@@ -2385,8 +2421,7 @@ static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent
   else k_round<Cd, 5><<<grid, BLOCK, 0, S>>>(kp);
   k_round_big<Cd><<<(unsigned)std::max(1, E.n_sms * 3), BLOCK, 0, S>>>(kp);
   if (eb) cudaEventRecord(eb, S);
-  k_commit<<<(unsigned)std::max(1, E.n_sms * 2), 256, 0, S>>>(kp);
-  k_fcount<<<kp.fblocks, 256, 0, S>>>(kp);
+  k_commit<<<kp.fblocks, 256, 0, S>>>(kp);
   k_ffill<<<kp.fblocks, 256, 0, S>>>(kp);
 }
 
@@ -2484,7 +2519,7 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
       if (dg.generic) launch_round<CodecGen>(*this, dg.kp, S, ea, eb);
       else launch_round<CodecStd>(*this, dg.kp, S, ea, eb);
     }
-    launches += 5ull * R;
+    launches += 4ull * R;
     CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
     CU(cudaStreamSynchronize(S));
     const Ctr c = *s.h_ctr;
