@@ -456,11 +456,11 @@ def run_ours(args, d: Dist):
             },
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "traffic_source": "ncu DRAM bytes per algorithmic byte of all round launches of the "
-                                           "1024-job case (profiles/k_round_batched.md) x algorithmic bytes "
-                                           "per full-size launch",
+                         "traffic_source": "ncu DRAM bytes per algorithmic byte of all round-kernel launches (k_round + "
+                                           "k_round_big) of the 1024-job case (profiles/k_round_batched.md) x "
+                                           "algorithmic bytes per full-size round",
                          "algorithmic_bytes_per_launch": alg_per_launch,
-                         "kernel": "k_round", "peak_kind": peak_kind,
+                         "kernel": "k_round + k_round_big (one round)", "peak_kind": peak_kind,
                          "algorithmic_bytes_per_solve": st_prof["algorithmic_bytes"],
                          "round_kernel_ms_per_solve": k_ms, "round_kernel_launches": k_launch},
             "cpu_baseline": cpu,
