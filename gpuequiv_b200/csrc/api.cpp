@@ -29,12 +29,12 @@ geq_status fail(geq_status st, const char *fmt, ...) {
 
 // TryFrom<SerdeGameGraph> (energygame.rs:65-83): CSR shape, successor ids,
 // and update codes that name an element (pack_upd rejects others, energy.rs:551-556).
-geq_status validate_graph(const geq_game_graph &g) {
+geq_status validate_graph(const geq_game_graph &g, bool check_rows) {
   Conf c(g.conf);
   if (c.elements == 0) return fail(GEQ_ERR_INVALID_INPUT, "EnergyConf with zero elements");
   if (!g.row_offsets) return fail(GEQ_ERR_INVALID_INPUT, "row_offsets is NULL");
   if (g.row_offsets[0] != 0) return fail(GEQ_ERR_INVALID_INPUT, "row_offsets[0] must be 0");
-  for (uint32_t v = 0; v < g.n_vertices; v++)
+  for (uint32_t v = 0; check_rows && v < g.n_vertices; v++)
     if (g.row_offsets[v + 1] < g.row_offsets[v]) return fail(GEQ_ERR_INVALID_INPUT, "row_offsets not monotone at %u", v);
   const uint64_t m = g.row_offsets[g.n_vertices];
   if (m && (!g.column_indices || !g.weights)) return fail(GEQ_ERR_INVALID_INPUT, "edges without column_indices/weights");
@@ -81,10 +81,14 @@ static geq_status make_inputs(uint32_t n_games, const geq_game_graph *graphs, co
                               std::vector<GameInput> &in) {
   if (n_games == 0 || !graphs) return fail(GEQ_ERR_INVALID_INPUT, "no games");
   in.resize(n_games);
+  // large batches: row monotonicity and the standard reach are left to the
+  // device (k_check_rows, k_std_reach), which reads every row anyway
+  const bool on_device = n_games >= 64 && !initial;
   auto one = [&](uint32_t g) -> geq_status {
     GameInput &gi = in[g];
     gi.g = graphs[g];
-    geq_status st = validate_graph(gi.g);
+    gi.rows_unchecked = on_device;
+    geq_status st = validate_graph(gi.g, !on_device);
     if (st) return st;
     if (!(Conf(gi.g.conf) == Conf(graphs[0].conf))) return fail(GEQ_ERR_INVALID_INPUT, "games of one batch need one EnergyConf");
     gi.init = initial ? initial[g] : nullptr;
@@ -96,6 +100,8 @@ static geq_status make_inputs(uint32_t n_games, const geq_game_graph *graphs, co
         if (gi.to_reach[i] >= gi.g.n_vertices) return fail(GEQ_ERR_INVALID_INPUT, "to_reach index out of range");
     } else if (to_reach && !to_reach[g] && n_to_reach && n_to_reach[g]) {
       return fail(GEQ_ERR_INVALID_INPUT, "to_reach is NULL with a non-zero count");
+    } else if (!to_reach && on_device) {
+      gi.std_reach = true;
     } else if (!to_reach) {
       gi.reach_storage = standard_reach_of(gi.g);
       gi.to_reach = gi.reach_storage.data();

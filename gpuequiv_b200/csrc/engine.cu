@@ -1620,14 +1620,20 @@ __global__ void k_u64_to_u32(const unsigned long long *in, unsigned long long n,
     out[i] = (uint32_t)in[i];
 }
 
-__global__ void k_fill_reverse(const uint32_t *row, const uint32_t *col, unsigned long long n, uint32_t *cursor,
-                               uint32_t *rcol) {
+// Predecessor lists.  Successor ids and row offsets are not trusted yet (the
+// error flags of the checks are read after the upload): edges outside
+// [0, m) and successors outside [0, n) are skipped, as k_indegree skips them,
+// so every write stays inside the lists counted for it.
+__global__ void k_fill_reverse(const uint32_t *row, const uint32_t *col, unsigned long long n,
+                               unsigned long long m, uint32_t *cursor, uint32_t *rcol) {
   for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n;
        v += (unsigned long long)gridDim.x * blockDim.x) {
-    for (uint32_t k = row[v]; k < row[v + 1]; k++) {
-      uint32_t w = col[k];
-      uint32_t pos = atomicAdd(&cursor[w], 1u);
-      rcol[pos] = (uint32_t)v;
+    const unsigned long long e = min((unsigned long long)row[v + 1], m);
+    for (unsigned long long k = row[v]; k < e; k++) {
+      const uint32_t w = col[k];
+      if (w >= n) continue;
+      const uint32_t pos = atomicAdd(&cursor[w], 1u);
+      if (pos < m) rcol[pos] = (uint32_t)v;
     }
   }
 }
@@ -1644,6 +1650,27 @@ __device__ __forceinline__ uint32_t game_of(const unsigned long long *base, uint
 }
 
 // Shift per-game local ids of a concatenated batch into the global id space.
+// Row offsets of every game, before they are made global: each game's first
+// offset is 0 and offsets do not decrease up to the game's edge count.
+__global__ void k_check_rows(const uint32_t *row, unsigned long long n, const unsigned long long *node_base,
+                             const unsigned long long *edge_base, uint32_t n_games, uint32_t *err) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n;
+       v += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t g = game_of(node_base, n_games, v);
+    const uint32_t r = row[v];
+    const unsigned long long next =
+        (v + 1 < node_base[g + 1]) ? row[v + 1] : (edge_base[g + 1] - edge_base[g]);
+    if ((v == node_base[g] && r != 0u) || r > next) atomicOr(err, 4u);
+  }
+}
+// EnergyGame::standard_reach + with_reach (energygame.rs:347-365) on the
+// device: {0} at every defender without successors.
+__global__ void k_std_reach(const uint32_t *row, const uint8_t *flags, unsigned long long n,
+                            unsigned long long *desc) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n;
+       v += (unsigned long long)gridDim.x * blockDim.x)
+    if (!(flags[v] & 1u) && row[v] == row[v + 1]) desc[v] = inl_hdr(1u);
+}
 __global__ void k_fix_rows(uint32_t *row, unsigned long long n, const unsigned long long *node_base,
                            const unsigned long long *edge_base, uint32_t n_games) {
   for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < n;
@@ -1684,6 +1711,21 @@ __global__ void k_init_reach(unsigned long long *desc, const uint32_t *reach, un
 }
 
 // initialize_visit_lists (energygame.rs:1461-1465): predecessors of to_reach.
+// The initial frontier of the standard reach: predecessors of every defender
+// without successors.
+__global__ void k_init_frontier_std(const KParams p) {
+  __shared__ uint32_t smem[(256 / 32) * SM_WORDS];
+  Ctr *c = p.ctr;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t *sm = smem + (threadIdx.x >> 5) * SM_WORDS;
+  const unsigned long long gw = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long i0 = gw * 32ull; i0 < p.n_nodes; i0 += nw * 32ull) {
+    const unsigned long long v = i0 + lane;
+    const bool f = v < p.n_nodes && !(p.flags[v] & 1u) && p.row[v] == p.row[v + 1];
+    push_preds_warp(p, c, sm, (uint32_t)(v < p.n_nodes ? v : 0u), f, c->stamp, lane);
+  }
+}
 __global__ void k_init_frontier(const KParams p, const uint32_t *reach, unsigned long long n_reach) {
   __shared__ uint32_t smem[(256 / 32) * SM_WORDS];
   Ctr *c = p.ctr;
@@ -1964,6 +2006,8 @@ struct DeviceGamesImpl {
   uint32_t *init_data = nullptr;
   unsigned long long init_total = 0;
   char *inbuf = nullptr;  // row, col, wt, flags, reach, init_data, [desc_init], node bases
+  bool std_reach = false;       // standard reach computed on the device (no reach list)
+  bool rows_on_device = false;  // row offsets checked by k_check_rows
   uint32_t *arena[2] = {nullptr, nullptr};
   unsigned long long arena_cap[2] = {0, 0};
   int arena_cur = 0;
@@ -2208,6 +2252,10 @@ uint64_t Engine::game_node_base(const DeviceGamesImpl &dg, uint32_t g) { return 
 geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   State &s = *st;
   if (games.empty()) return fail(GEQ_ERR_INVALID_INPUT, "no games");
+#if GEQ_PATH_PROFILE
+  const auto tu0 = std::chrono::steady_clock::now();
+  auto tsince = [&]() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tu0).count(); };
+#endif
   GamesPtr dg(new DeviceGamesImpl());
   dg->owner = &s;
   s.live.insert(dg.get());
@@ -2221,6 +2269,13 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   dg->edge_base.assign(dg->n_games + 1, 0);
   unsigned long long init_total = 0, n_reach = 0;
   bool any_init = false;
+  // standard reach and row checks on the device when every game asks for it
+  dg->std_reach = true;
+  dg->rows_on_device = true;
+  for (const GameInput &gi : games) {
+    dg->std_reach = dg->std_reach && gi.std_reach;
+    dg->rows_on_device = dg->rows_on_device && gi.rows_unchecked;
+  }
   for (uint32_t g = 0; g < dg->n_games; g++) {
     const GameInput &gi = games[g];
     if (!(Conf(gi.g.conf) == dg->conf)) return fail(GEQ_ERR_INVALID_INPUT, "games of one batch need one EnergyConf");
@@ -2316,19 +2371,29 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
   D.arena_cap[0] = DevPool::round_size(cap * 4) / 4;
   cudaStream_t S = s.stream;
+#if GEQ_PATH_PROFILE
+  const double t_stage0 = tsince();
+#endif
   geq_status ust = staged_upload(copies, H, D.inbuf, total_bytes, S);
+#if GEQ_PATH_PROFILE
+  const double t_stage1 = tsince();
+#endif
   if (ust) return ust;
-  if (!any_init) {
-    if (N) CU(cudaMemsetAsync(D.desc_init, 0, N * 8, S));
-    if (n_reach)
-      k_init_reach<<<(unsigned)std::min<unsigned long long>((n_reach + 255) / 256, 4096), 256, 0, S>>>(
-          D.desc_init, D.reach, n_reach);
-  }
   CU(cudaMemsetAsync(D.mark, 0, 2 * ((N + 31) / 32) * 4, S));
   CU(cudaMemsetAsync(s.d_err, 0, 4, S));
   const unsigned grid = (unsigned)std::max(1, n_sms * 8);
+  if (N && D.rows_on_device)
+    k_check_rows<<<grid, 256, 0, S>>>(D.row, N, D.d_node_base, D.d_node_base + (D.n_games + 1), D.n_games,
+                                      s.d_err);
   if (D.n_games > 1)
     k_fix_rows<<<grid, 256, 0, S>>>(D.row, N, D.d_node_base, D.d_node_base + (D.n_games + 1), D.n_games);
+  if (!any_init) {
+    if (N) CU(cudaMemsetAsync(D.desc_init, 0, N * 8, S));
+    if (D.std_reach && N) k_std_reach<<<grid, 256, 0, S>>>(D.row, D.flags, N, D.desc_init);
+    else if (n_reach)
+      k_init_reach<<<(unsigned)std::min<unsigned long long>((n_reach + 255) / 256, 4096), 256, 0, S>>>(
+          D.desc_init, D.reach, n_reach);
+  }
   // successor ids into the global id space, checked against each game's size
   k_fix_cols<<<grid, 256, 0, S>>>(D.col, M, D.d_node_base, D.d_node_base + (D.n_games + 1), D.n_games,
                                   D.d_node_base + 2 * (D.n_games + 1), s.d_err);
@@ -2346,15 +2411,20 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   if (a) { s.pool.put(roff, (N + 1) * 8); return a; }
   k_u64_to_u32<<<grid, 256, 0, S>>>(roff, N + 1, D.rrow);
   CU(cudaMemcpyAsync(s.cnt, D.rrow, N * 4, cudaMemcpyDeviceToDevice, S));
-  k_fill_reverse<<<grid, 256, 0, S>>>(D.row, D.col, N, s.cnt, D.rcol);
+  k_fill_reverse<<<grid, 256, 0, S>>>(D.row, D.col, N, M, s.cnt, D.rcol);
   if (N) k_abits<<<grid, 256, 0, S>>>(D.flags, N, (uint32_t)((N + 31) / 32), D.abits);
   CU(cudaMemcpyAsync(&s.h_ctr->pad, s.d_err, 4, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   s.pool.put(roff, (N + 1) * 8);
   CU(cudaGetLastError());
   const uint32_t h_err = s.h_ctr->pad;
+#if GEQ_PATH_PROFILE
+  std::fprintf(stderr, "GEQ_UPLOAD host_prep_ms %.2f staged_ms %.2f device_ms %.2f total_ms %.2f bytes %zu\n", t_stage0,
+               t_stage1 - t_stage0, tsince() - t_stage1, tsince(), total_bytes);
+#endif
   if (h_err & 1u) return fail(GEQ_ERR_INVALID_INPUT, "Node index too high: a successor index is out of range");
   if (h_err & 2u) return fail(GEQ_ERR_INVALID_INPUT, "an edge update names no element or sets padding bits");
+  if (h_err & 4u) return fail(GEQ_ERR_INVALID_INPUT, "row_offsets must start at 0 and must not decrease");
   KParams &kp = D.kp;
   kp.row = D.row; kp.col = D.col; kp.wt = D.wt; kp.rrow = D.rrow; kp.rcol = D.rcol;
   kp.flags = D.flags; kp.desc = D.desc; kp.mark = D.mark; kp.front0 = D.front0; kp.front1 = D.front1;
@@ -2487,7 +2557,12 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
   h.stamp = dg.next_stamp;
   *s.h_ctr = h;
   CU(cudaMemcpyAsync(dg.ctr, s.h_ctr, sizeof(Ctr), cudaMemcpyHostToDevice, S));
-  if (dg.n_reach) {
+  if (dg.std_reach && dg.N) {
+    k_init_frontier_std<<<(unsigned)std::max(1, n_sms * 16), 256, 0, S>>>(dg.kp);
+    k_fcount<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
+    k_ffill<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
+    launches += 3;
+  } else if (dg.n_reach) {
     const unsigned grid = (unsigned)std::max<unsigned long long>(
         1, std::min<unsigned long long>((dg.n_reach + 7) / 8, (unsigned long long)n_sms * 16));
     k_init_frontier<<<grid, 256, 0, S>>>(dg.kp, dg.reach, dg.n_reach);

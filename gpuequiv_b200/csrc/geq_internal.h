@@ -51,11 +51,13 @@ struct GameInput {
   const uint32_t *to_reach = nullptr;
   uint32_t n_reach = 0;
   std::vector<uint32_t> reach_storage;  // standard reach when none was given
+  bool std_reach = false;       // standard reach, to be computed on the device (no list)
+  bool rows_unchecked = false;  // row monotonicity left to the device (large batches)
 };
 
 // Validation of a graph view (TryFrom<SerdeGameGraph> checks,
 // energygame.rs:65-83, plus update-code checks).
-geq_status validate_graph(const geq_game_graph &g);
+geq_status validate_graph(const geq_game_graph &g, bool check_rows = true);
 geq_status validate_lists(const geq_game_graph &g, const geq_energy_lists *l);
 // EnergyGame::standard_reach (energygame.rs:347-352): defenders without successors.
 std::vector<uint32_t> standard_reach_of(const geq_game_graph &g);

@@ -301,3 +301,45 @@ def test_invalid_inputs(geq, ctx):
     with pytest.raises(geq.GeqError) as e:
         geq.EnergyGame.standard_reach(g1).run(ctx)
     assert e.value.name == "UNSUPPORTED"
+
+
+def test_invalid_inputs_large_batch(geq, ctx):
+    """Batches of 64 games and more leave the row checks and the standard
+    reach to the device: a faulty game still fails the call cleanly, and the
+    context solves the next batch correctly."""
+    games = [random_bipartite_game(100 + i, 40) for i in range(70)]
+    graphs = [geq.GameGraph.from_csr(r, c, w, a, geq.EnergyConf.STANDARD) for r, c, w, a in games]
+    good = geq.run_batch_raw(graphs, ctx)
+    for i in (0, 41, 69):
+        o = oracle_run(*games[i])
+        got = [np.asarray(good[1][i][good[0][i][v]:good[0][i][v + 1]], np.uint32) for v in range(len(good[0][i]) - 1)]
+        assert_parity(got, o, f"batch game {i}")
+
+    def with_bad(i, fix):
+        r, c, w, a = [np.array(x) for x in games[i]]
+        r, c = fix(r.astype(np.uint32), c.astype(np.uint32))
+        bad = geq.GameGraph.from_csr(r, c, w, a, geq.EnergyConf.STANDARD)
+        return graphs[:i] + [bad] + graphs[i + 1:]
+
+    def unsorted_rows(r, c):
+        r = r.copy()
+        k = int(np.argmax(np.diff(r)[1:] > 0))  # position k+1 has successors: r[k+1] < r[k+2]
+        r[k + 1], r[k + 2] = r[k + 2], r[k + 1]
+        return r, c
+
+    def far_successor(r, c):
+        c = c.copy()
+        c[0] = 0xFFFFFF00
+        return r, c
+
+    def other_games_successor(r, c):
+        c = c.copy()
+        c[0] = 41  # beyond this 40-position game, inside the batch's id space
+        return r, c
+
+    for i, fix in ((40, unsorted_rows), (3, far_successor), (5, other_games_successor)):
+        with pytest.raises(geq.GeqError) as e:
+            geq.run_batch_raw(with_bad(i, fix), ctx)
+        assert e.value.name == "INVALID_INPUT", fix.__name__
+    again = geq.run_batch_raw(graphs, ctx)
+    assert all(np.array_equal(a, b) for a, b in zip(again[1], good[1]))
