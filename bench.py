@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--serve-rates", default="1000,5000",
                     help="Poisson arrival rates (req/s) of the serving leg; empty: no serving leg")
     ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrivals per serving rate (s)")
+    ap.add_argument("--no-stress", dest="stress", action="store_false", help="skip the stress-game leg")
     ap.add_argument("--solve-only", action="store_true",
                     help="build, upload and solve only (the command profiled with ncu)")
     return ap.parse_args()
@@ -431,6 +432,22 @@ def run_ours(args, d: Dist):
     for k, lam in enumerate(rates):
         serving.append(run_serving(ctx, graphs, lam, args.serve_seconds, seed=100 + k + 1000 * d.rank))
 
+    # ---- stress configuration: one 2M-position / 10M-edge game, resident ----
+    stress = None
+    if args.stress:
+        srow, scol, swt, satt = synth_mod().stress_game()
+        sg = geq.GameGraph.from_csr(srow, scol, swt, satt, geq.EnergyConf.STANDARD)
+        sdg = geq.DeviceGames([sg], ctx)
+        for _ in range(2):
+            sdg.solve()
+        sts = [sdg.solve() for _ in range(3)]
+        sdg.close()
+        sms = float(np.median([x["device_ms"] for x in sts]))
+        stress = {"workload": "stress: 2,000,000 positions (60 % attackers), 10,000,000 edges, seed 2, standard reach",
+                  "solve_ms": sms, "edges_relaxed": sts[0]["edges_relaxed"],
+                  "positions_computed": sts[0]["positions_computed"], "rounds": sts[0]["rounds"],
+                  "edges_relaxed_per_s": sts[0]["edges_relaxed"] / (sms / 1e3)}
+
     # ---- CPU baseline: the oracle on one host thread (rank 0, N=1) ----
     cpu = None
     if d.rank == 0 and d.world == 1:
@@ -469,6 +486,7 @@ def run_ours(args, d: Dist):
             "plain_cuda": {"value": plain_rate, "unit": UNIT, "sample": f"{len(idx)} games (every "
                            f"{max(1, len(graphs) // len(idx))}th job), one geq_energy_game_run call each"},
             "batched_vs_plain": value / plain_rate if plain_rate else None,
+            "stress": stress,
             "serving": {"workload": "Poisson arrivals of single compare(p,q) games drawn from this batch "
                                     "(LTS 20-5000 states), geq_server with 2 pipelines, 150 GB admission budget",
                         "runs": serving},

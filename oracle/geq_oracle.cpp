@@ -748,6 +748,64 @@ void parallel_for(uint32_t n, uint32_t threads, F f) {
   for (auto &th : pool) th.join();
 }
 
+// One worklist step of position v against the lists E, as a round of
+// run_game applies it (energygame.rs:774-944, attack_update.wgsl:77-113,
+// attack_minimize.wgsl:180-235, defend_iterative.wgsl:283-368): true when
+// the reference would change v's list.  Defenders whose suprema outgrow the
+// preallocated memory are retried with more, as run_game does in a later
+// round.
+bool step_changes(const Graph &g, const Arith &ar, const std::vector<EList> &E, uint32_t v) {
+  const uint32_t es = ar.es, us = ar.us;
+  if (g.row[v] == g.row[v + 1]) return false;  // never visited: no successors
+  std::vector<uint32_t> upd_tmp(es), cand;
+  if (g.attacker[v]) {
+    for (uint32_t k = g.row[v]; k < g.row[v + 1]; k++) {
+      const EList &ew = E[g.col[k]];
+      for (size_t x = 0; x < ew.size(); x += es) {
+        ar.inv_update(&ew[x], &g.wt[(size_t)k * us], upd_tmp.data());
+        cand.insert(cand.end(), upd_tmp.begin(), upd_tmp.end());
+      }
+    }
+    const size_t own_start = cand.size() / es;
+    std::vector<uint32_t> zero(us, 0);
+    for (size_t x = 0; x < E[v].size(); x += es) {
+      ar.inv_update(&E[v][x], zero.data(), upd_tmp.data());
+      cand.insert(cand.end(), upd_tmp.begin(), upd_tmp.end());
+    }
+    const size_t K = cand.size() / es;
+    for (size_t i = 0; i < own_start; i++) {
+      bool keep = true;
+      for (size_t j = 0; j < K && keep; j++) {
+        bool eq = ar.eq(&cand[j * es], &cand[i * es]);
+        if (j != i && ((eq && i < j) || (!eq && ar.less_eq(&cand[j * es], &cand[i * es])))) keep = false;
+      }
+      if (keep) return true;  // a kept candidate from a successor
+    }
+    return false;
+  }
+  for (uint32_t k = g.row[v]; k < g.row[v + 1]; k++)
+    if (E[g.col[k]].empty()) return false;  // :789-792, not visited
+  EList en;
+  std::vector<uint32_t> so;
+  for (uint32_t k = g.row[v]; k < g.row[v + 1]; k++) {
+    const EList &ew = E[g.col[k]];
+    so.push_back((uint32_t)(en.size() / es));
+    for (size_t x = 0; x < ew.size(); x += es) {
+      ar.inv_update(&ew[x], &g.wt[(size_t)k * us], upd_tmp.data());
+      en.insert(en.end(), upd_tmp.begin(), upd_tmp.end());
+    }
+  }
+  so.push_back((uint32_t)(en.size() / es));
+  EList res;
+  uint32_t mem = DEFAULT_SUPREMA_MEMORY;
+  for (;;) {
+    const int32_t stt = wg_intersection(ar, en.data(), so.data(), (uint32_t)so.size() - 1, mem, res);
+    if (stt >= 0) break;
+    mem = std::max(next_pow2((uint32_t)(-(int64_t)stt)), 128u);
+  }
+  return !earray_eq(ar, E[v], res);
+}
+
 }  // namespace
 
 struct OraSolution {
@@ -1015,6 +1073,42 @@ void ora_compare_batch(uint32_t n_jobs, const OraLts *const *lts, const uint32_t
   parallel_for(n_jobs, n_threads, [&](uint32_t i) {
     compare_job(lts[i]->l, p[i], q[i], out_counts[i], out_nodes[i]);
   });
+}
+
+uint64_t ora_check_fixpoint(uint32_t elements, uint32_t max, uint32_t n, const uint32_t *row_offsets,
+                            const uint32_t *col, const uint32_t *weights, const uint8_t *attacker,
+                            const uint64_t *offsets, const uint32_t *data, uint32_t n_threads, uint32_t *first_bad) {
+  Graph g;
+  g.conf = Conf{elements, max};
+  g.n = n;
+  g.row.assign(row_offsets, row_offsets + n + 1);
+  const uint32_t m = g.row[n];
+  g.col.assign(col, col + m);
+  g.wt.assign(weights, weights + (size_t)m * g.conf.update_size());
+  g.attacker.assign(attacker, attacker + n);
+  const Arith ar(g.conf);
+  const uint32_t es = ar.es;
+  std::vector<EList> E(n);
+  for (uint32_t v = 0; v < n; v++) E[v].assign(data + offsets[v] * es, data + offsets[v + 1] * es);
+  const uint32_t chunks = (n + 4095) / 4096;
+  std::vector<uint64_t> bad(chunks, 0);
+  std::vector<uint32_t> first(chunks, 0xFFFFFFFFu);
+  parallel_for(chunks, n_threads, [&](uint32_t c) {
+    const uint32_t b = c * 4096, e = std::min(n, b + 4096);
+    for (uint32_t v = b; v < e; v++)
+      if (step_changes(g, ar, E, v)) {
+        if (!bad[c]) first[c] = v;
+        bad[c]++;
+      }
+  });
+  uint64_t total = 0;
+  uint32_t f = 0xFFFFFFFFu;
+  for (uint32_t c = 0; c < chunks; c++) {
+    total += bad[c];
+    if (bad[c] && f == 0xFFFFFFFFu) f = first[c];
+  }
+  if (first_bad) *first_bad = f;
+  return total;
 }
 
 void ora_run_games_parallel(uint32_t n_games, uint32_t elements, uint32_t max, const uint32_t *n_pos,

@@ -116,6 +116,15 @@ void ora_compare_batch(uint32_t n_jobs, const OraLts *const *lts,
                        const uint32_t *p, const uint32_t *q, uint32_t n_threads,
                        uint64_t *out_counts, uint64_t *out_nodes);
 /* EnergyGame::run on many games in parallel (graph given as CSR arrays). */
+/* Test support, at sizes the sequential solve would take too long for:
+ * the number of positions whose list one more worklist step (the update of
+ * a run_game round) would change, given final lists (offsets[n+1] in
+ * energies, data packed); 0 for a fixpoint.  *first_bad = the first such
+ * position (0xFFFFFFFF when none). */
+uint64_t ora_check_fixpoint(uint32_t elements, uint32_t max, uint32_t n, const uint32_t *row_offsets,
+                            const uint32_t *col, const uint32_t *weights, const uint8_t *attacker,
+                            const uint64_t *offsets, const uint32_t *data, uint32_t n_threads,
+                            uint32_t *first_bad);
 void ora_run_games_parallel(uint32_t n_games, uint32_t elements, uint32_t max,
                             const uint32_t *n_pos, /* positions per game */
                             const uint32_t *const *row_offsets,

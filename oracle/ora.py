@@ -95,6 +95,9 @@ def lib():
         L.ora_run_games_parallel.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u32p,
                                              C.POINTER(u32p), C.POINTER(u32p), C.POINTER(u32p),
                                              C.POINTER(u8p), C.c_uint32, u64p]
+        L.ora_check_fixpoint.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p, u32p, u8p, u64p, u32p,
+                                         C.c_uint32, u32p]
+        L.ora_check_fixpoint.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -360,6 +363,24 @@ def run_games_parallel(games, threads=1, elements=6, max_=3):
     lib().ora_run_games_parallel(n, elements, max_, _p(npos, C.c_uint32), rows, cols, wts, atts, threads,
                                  _p(out, C.c_uint64))
     return out
+
+
+def check_fixpoint(row, col, wt, att, offsets, data, threads=0, elements=6, max_=3):
+    """(count, first) of positions whose list one more worklist step would
+    change; (0, None) when the lists are a fixpoint (test support for sizes
+    the sequential solve would take too long for)."""
+    import os
+    r = np.ascontiguousarray(row, dtype=np.uint32)
+    c = np.ascontiguousarray(col if len(col) else np.zeros(1), dtype=np.uint32)
+    w = np.ascontiguousarray(wt if len(wt) else np.zeros(1), dtype=np.uint32)
+    a = np.ascontiguousarray(att, dtype=np.uint8)
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    d = np.ascontiguousarray(data if len(data) else np.zeros(1), dtype=np.uint32)
+    first = C.c_uint32(0)
+    n_bad = lib().ora_check_fixpoint(elements, max_, len(r) - 1, _p(r, C.c_uint32), _p(c, C.c_uint32),
+                                     _p(w, C.c_uint32), _p(a, C.c_uint8), _p(o, C.c_uint64), _p(d, C.c_uint32),
+                                     threads or (os.cpu_count() or 1), C.byref(first))
+    return int(n_bad), (None if n_bad == 0 else int(first.value))
 
 
 # ---------------------------------------------------------------------------
