@@ -135,6 +135,7 @@ _SIGS = {
     "geq_server_get_stats": ([vp, C.POINTER(geq_server_stats)], None),
     "geq_server_destroy": ([vp], None),
     "geq_lts_from_edges": ([C.c_uint64, u32p, u32p, i32p, C.POINTER(vp)], C.c_int),
+    "geq_lts_from_adjacency": ([C.c_uint32, C.c_uint64, u32p, u32p, i32p, C.POINTER(vp)], C.c_int),
     "geq_lts_from_csv_file": ([C.c_char_p, C.POINTER(vp)], C.c_int),
     "geq_lts_n_vertices": ([vp], C.c_uint32),
     "geq_lts_n_transitions": ([vp], C.c_uint64),

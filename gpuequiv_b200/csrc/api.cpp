@@ -442,6 +442,20 @@ geq_status geq_lts_from_edges(uint64_t n_edges, const uint32_t *src, const uint3
   return GEQ_OK;
 }
 
+geq_status geq_lts_from_adjacency(uint32_t n_vertices, uint64_t n_edges, const uint32_t *src, const uint32_t *dst,
+                                  const int32_t *label, geq_lts **out) {
+  if (!out) return fail(GEQ_ERR_INVALID_INPUT, "out is NULL");
+  *out = nullptr;
+  if (n_edges && (!src || !dst || !label)) return fail(GEQ_ERR_INVALID_INPUT, "edge arrays are NULL");
+  for (uint64_t i = 0; i < n_edges; i++)
+    if (src[i] >= n_vertices || dst[i] >= n_vertices) return fail(GEQ_ERR_INVALID_INPUT, "Node index too high");
+  std::unique_ptr<geq_lts> l(new geq_lts());
+  geq_status st = Lts::from_edges(n_edges, src, dst, label, l->l, n_vertices);
+  if (st) return st;
+  *out = l.release();
+  return GEQ_OK;
+}
+
 geq_status geq_lts_from_csv_file(const char *path, geq_lts **out) {
   if (!out || !path) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
   *out = nullptr;

@@ -47,8 +47,9 @@ void Lts::finish_from_buckets(uint32_t nv, const std::vector<uint32_t> &src, con
 
 // FromIterator<Edge> (lib.rs:523-536): the vertex count is one more than the
 // largest id mentioned by any edge.
-geq_status Lts::from_edges(uint64_t m, const uint32_t *src, const uint32_t *dst, const int32_t *label, Lts &out) {
-  uint64_t nv = 0;
+geq_status Lts::from_edges(uint64_t m, const uint32_t *src, const uint32_t *dst, const int32_t *label, Lts &out,
+                           uint32_t min_vertices) {
+  uint64_t nv = min_vertices;
   for (uint64_t i = 0; i < m; i++) nv = std::max<uint64_t>(nv, (uint64_t)std::max(src[i], dst[i]) + 1);
   if (nv > 0xFFFFFFF0ull) return fail(GEQ_ERR_INVALID_INPUT, "process id too large");
   std::vector<uint32_t> s(src, src + m), d(dst, dst + m);

@@ -14,7 +14,7 @@ struct Lts {
   std::vector<int32_t> lab_;  // label of each transition (rows sorted by label)
 
   static geq_status from_edges(uint64_t m, const uint32_t *src, const uint32_t *dst, const int32_t *label,
-                               Lts &out);
+                               Lts &out, uint32_t min_vertices = 0);
   static geq_status from_csv_file(const char *path, Lts &out);
   uint64_t signature_refinement(std::vector<uint64_t> &part) const;
   void minimize(std::vector<uint64_t> &mapping, Lts &out) const;

@@ -44,8 +44,19 @@ class TransitionSystem:
         return h
 
     @classmethod
-    def from_arrays(cls, src, dst, label) -> "TransitionSystem":
-        return cls(_handle=cls._from_arrays(src, dst, label))
+    def from_arrays(cls, src, dst, label, n_vertices: int | None = None) -> "TransitionSystem":
+        """Edges as arrays; with n_vertices, processes beyond the largest id
+        keep empty adjacency lists (From<Vec<Vec<Transition>>>)."""
+        if n_vertices is None:
+            return cls(_handle=cls._from_arrays(src, dst, label))
+        s = np.ascontiguousarray(src, dtype=np.uint32)
+        d = np.ascontiguousarray(dst, dtype=np.uint32)
+        l = np.ascontiguousarray(label, dtype=np.int32)
+        h = C.c_void_p()
+        n = len(s)
+        check(lib.geq_lts_from_adjacency(n_vertices, n, _p(s if n else _Z32, _u32), _p(d if n else _Z32, _u32),
+                                         _p(l if n else _ZI32, _i32), C.byref(h)))
+        return cls(_handle=h)
 
     @classmethod
     def from_csv_file(cls, path: str) -> "TransitionSystem":

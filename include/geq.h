@@ -296,6 +296,11 @@ typedef struct geq_lts geq_lts;
 /* FromIterator<(u32, u32, i32)> (lib.rs:523-536): edges (src, dst, label). */
 geq_status geq_lts_from_edges(uint64_t n_edges, const uint32_t *src, const uint32_t *dst,
                               const int32_t *label, geq_lts **out);
+/* From<Vec<Vec<Transition>>> (lib.rs:507-514): n_vertices adjacency lists
+ * given as edges (src, dst, label); processes beyond the largest id in the
+ * edges keep empty lists (the serde layout's trailing isolated processes). */
+geq_status geq_lts_from_adjacency(uint32_t n_vertices, uint64_t n_edges, const uint32_t *src,
+                                  const uint32_t *dst, const int32_t *label, geq_lts **out);
 /* TransitionSystem::from_csv_file (lib.rs:364-406). */
 geq_status geq_lts_from_csv_file(const char *path, geq_lts **out);
 uint32_t geq_lts_n_vertices(const geq_lts *l);
