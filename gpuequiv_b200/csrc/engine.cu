@@ -11,15 +11,19 @@
 // graph.  Here the whole loop stays on the device:
 //
 //   * The game (CSR + reverse CSR), the per-position energy lists and the
-//     frontier queues are resident in HBM.  An energy list is a slice of one
-//     energy arena; position v's descriptor desc[v] = (offset << 24 | count).
-//   * k_round: one warp per frontier position reads its successors' lists
-//     straight from the arena (no gather copy), applies the inverse edge
-//     update, minimises (attacker) or intersects up-sets (defender), writes
-//     the new list to fresh arena space and, if the list changed, appends
-//     its predecessors to the next frontier (deduplicated by round stamps).
+//     frontier are resident in HBM.  A list of up to 5 energies sits inline
+//     in its position's 64-bit descriptor; longer ones are slices of one
+//     energy arena (offset << 24 | count).
+//   * k_round: each lane of a warp solves one frontier position (the lane
+//     path: the successors' lists read straight from HBM, the inverse edge
+//     update applied, candidates streamed into an antichain in shared
+//     memory), stores the new list in a per-slot buffer and, if the list
+//     changed, marks its predecessors in the next-frontier bitmap.  Positions
+//     too large for a lane are queued for k_round_big, one warp each.
 //   * k_commit: publishes the new descriptors (Jacobi: every position of a
-//     round reads the lists of the previous round) and flips the frontier.
+//     round reads the lists of the previous round), counts the bitmap, and
+//     flips the round; k_ffill turns the bitmap into the next frontier list
+//     (attackers first, each kind in position order).
 //   * Rounds are launched as CUDA graphs of several rounds each; the host
 //     reads one small counter block per graph launch to detect termination.
 //
