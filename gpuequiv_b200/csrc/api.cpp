@@ -70,6 +70,9 @@ std::vector<uint32_t> standard_reach_of(const geq_game_graph &g) {
   return r;
 }
 
+// Batches of at least this many positions run as two pipelined halves.
+static constexpr unsigned long long SPLIT_MIN_POSITIONS = 1ull << 21;
+
 static geq_status ctx_engine(geq_context *ctx, Engine *&e) {
   if (!ctx || !ctx->engine) return fail(GEQ_ERR_INVALID_INPUT, "context is NULL");
   e = ctx->engine.get();
@@ -392,6 +395,23 @@ geq_status geq_energy_game_run_batch(geq_context *ctx, uint32_t n_games, const g
       *out = sol.release();
       return GEQ_OK;
     }
+  }
+  unsigned long long positions = 0;
+  for (auto &gi : in) positions += gi.g.n_vertices;
+  if (n_games >= 2 && positions >= SPLIT_MIN_POSITIONS &&
+      !(e->tuning.flags & (GEQ_TUNE_NO_SPLIT | GEQ_TUNE_PROFILE))) {
+    // two halves on two engines: the second half's upload overlaps the
+    // first half's rounds
+    if (!ctx->engine2) {
+      std::unique_ptr<Engine> e2;
+      if ((st = Engine::create(ctx->device, e2))) return st;
+      ctx->engine2 = std::move(e2);
+    }
+    ctx->engine2->tuning = e->tuning;
+    std::unique_ptr<geq_solution> sol(new geq_solution());
+    if ((st = run_batch_pipelined(ctx->device, *e, *ctx->engine2, in, *sol))) return st;
+    *out = sol.release();
+    return GEQ_OK;
   }
   GamesPtr dg;
   if ((st = e->upload(in, dg))) return st;

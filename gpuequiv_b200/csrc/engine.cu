@@ -47,6 +47,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <map>
 #include <mutex>
 #include <set>
@@ -2650,54 +2651,172 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
   return GEQ_OK;
 }
 
-geq_status Engine::download(DeviceGamesImpl &dg, geq_solution &sol) {
+// Result lists of all positions: gathered on the device (counts, scan,
+// gather into one buffer, per-game relative offsets), then read back.  The
+// two steps are separate so that two uploads' results can be read into one
+// host buffer (run_batch_pipelined).
+geq_status Engine::download_prepare(DeviceGamesImpl &dg, Readback &rb) {
   State &s = *st;
   cudaStream_t S = s.stream;
   const unsigned long long N = dg.N;
   unsigned long long launches = 0;
   geq_status a = ensure_cnt(s, N + 1);
   if (a) return a;
-  unsigned long long *goff = (unsigned long long *)s.pool.get((N + 1) * 8);
-  unsigned long long *rel = (unsigned long long *)s.pool.get((N + dg.n_games) * 8);
-  if (!goff || !rel) {
-    s.pool.put(goff, (N + 1) * 8);
-    s.pool.put(rel, (N + dg.n_games) * 8);
+  rb.goff = (unsigned long long *)s.pool.get((N + 1) * 8);
+  rb.rel = (unsigned long long *)s.pool.get((N + dg.n_games) * 8);
+  if (!rb.goff || !rb.rel) {
+    download_release(dg, rb);
     return fail(GEQ_ERR_OUT_OF_MEMORY, "download offsets");
   }
   const unsigned grid = (unsigned)std::max(1, n_sms * 8);
   k_desc_counts<<<grid, 256, 0, S>>>(dg.desc, N, s.cnt);
-  if ((a = scan_u32(s, s.cnt, N, goff, launches))) return a;
-  CU(cudaMemcpyAsync(&s.h_ctr->positions, goff + N, 8, cudaMemcpyDeviceToHost, S));
+  if ((a = scan_u32(s, s.cnt, N, rb.goff, launches))) return a;
+  CU(cudaMemcpyAsync(&s.h_ctr->positions, rb.goff + N, 8, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
-  const unsigned long long total = s.h_ctr->positions;
-  uint32_t *out = (uint32_t *)s.pool.get(std::max<unsigned long long>(total, 1) * 4);
-  if (!out) return fail(GEQ_ERR_OUT_OF_MEMORY, "download data");
-  k_gather<<<grid, 256, 0, S>>>(dg.desc, N, goff, dg.arena[dg.arena_cur], dg.kp.ib, dg.kp.ibm, out);
-  k_rel_offsets<<<grid, 256, 0, S>>>(goff, N, dg.d_node_base, dg.n_games, rel);
-  sol.energy_size = 1;
-  // straight into page-locked host memory (no staging copy, no zero fill)
-  sol.n_offsets = N + dg.n_games;
-  sol.n_words = total;
-  if (!sol.off_buf.alloc(s.hpool, sol.n_offsets * 8) || !sol.data_buf.alloc(s.hpool, total * 4))
-    return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu result words", total);
-  CU(cudaMemcpyAsync(sol.off_buf.p, rel, sol.n_offsets * 8, cudaMemcpyDeviceToHost, S));
-  if (total) CU(cudaMemcpyAsync(sol.data_buf.p, out, total * 4, cudaMemcpyDeviceToHost, S));
+  rb.total = s.h_ctr->positions;
+  rb.out = (uint32_t *)s.pool.get(std::max<unsigned long long>(rb.total, 1) * 4);
+  if (!rb.out) return fail(GEQ_ERR_OUT_OF_MEMORY, "download data");
+  k_gather<<<grid, 256, 0, S>>>(dg.desc, N, rb.goff, dg.arena[dg.arena_cur], dg.kp.ib, dg.kp.ibm, rb.out);
+  k_rel_offsets<<<grid, 256, 0, S>>>(rb.goff, N, dg.d_node_base, dg.n_games, rb.rel);
+  CU(cudaGetLastError());
+  return GEQ_OK;
+}
+geq_status Engine::download_copy(DeviceGamesImpl &dg, Readback &rb, uint64_t *off_dst, uint32_t *data_dst) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  CU(cudaMemcpyAsync(off_dst, rb.rel, (dg.N + dg.n_games) * 8, cudaMemcpyDeviceToHost, S));
+  if (rb.total) CU(cudaMemcpyAsync(data_dst, rb.out, rb.total * 4, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   CU(cudaGetLastError());
-  s.pool.put(goff, (N + 1) * 8);
-  s.pool.put(rel, (N + dg.n_games) * 8);
-  s.pool.put(out, std::max<unsigned long long>(total, 1) * 4);
+  download_release(dg, rb);
+  return GEQ_OK;
+}
+void Engine::download_release(DeviceGamesImpl &dg, Readback &rb) {
+  State &s = *st;
+  s.pool.put(rb.goff, (dg.N + 1) * 8);
+  s.pool.put(rb.rel, (dg.N + dg.n_games) * 8);
+  s.pool.put(rb.out, std::max<unsigned long long>(rb.total, 1) * 4);
+  rb.goff = rb.rel = nullptr;
+  rb.out = nullptr;
+}
+
+// Per-game bases of a solution whose offsets are in place, starting at game
+// g0 with offset index ob and word db.
+static void fill_bases(const DeviceGamesImpl &dg, geq_solution &sol, uint32_t g0, uint64_t ob, uint64_t db) {
+  const uint64_t *offs = sol.off_ptr();
+  for (uint32_t g = 0; g < dg.n_games; g++) {
+    const uint32_t n = (uint32_t)(dg.node_base[g + 1] - dg.node_base[g]);
+    sol.n_vertices[g0 + g] = n;
+    sol.offsets_base[g0 + g] = ob;
+    sol.data_base[g0 + g] = db;
+    db += offs[ob + n];
+    ob += (uint64_t)n + 1;
+  }
+}
+
+geq_status Engine::download(DeviceGamesImpl &dg, geq_solution &sol) {
+  State &s = *st;
+  Readback rb;
+  geq_status a = download_prepare(dg, rb);
+  if (a) {
+    download_release(dg, rb);
+    return a;
+  }
+  sol.energy_size = 1;
+  // straight into page-locked host memory (no staging copy, no zero fill)
+  sol.n_offsets = dg.N + dg.n_games;
+  sol.n_words = rb.total;
+  if (!sol.off_buf.alloc(s.hpool, sol.n_offsets * 8) || !sol.data_buf.alloc(s.hpool, rb.total * 4)) {
+    download_release(dg, rb);
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu result words", rb.total);
+  }
+  if ((a = download_copy(dg, rb, (uint64_t *)sol.off_buf.p, (uint32_t *)sol.data_buf.p))) return a;
   sol.n_vertices.resize(dg.n_games);
   sol.offsets_base.resize(dg.n_games);
   sol.data_base.resize(dg.n_games);
-  const uint64_t *offs = sol.off_ptr();
-  unsigned long long db = 0;
-  for (uint32_t g = 0; g < dg.n_games; g++) {
-    sol.n_vertices[g] = (uint32_t)(dg.node_base[g + 1] - dg.node_base[g]);
-    sol.offsets_base[g] = dg.node_base[g] + g;
-    sol.data_base[g] = db;
-    db += offs[sol.offsets_base[g] + sol.n_vertices[g]];
+  fill_bases(dg, sol, 0, 0, 0);
+  return GEQ_OK;
+}
+
+// A large batch on two engines: the first half is uploaded, then solved
+// while the second half uploads on the other engine's stream, so the link
+// transfer of one half overlaps the rounds of the other; both halves' lists
+// are read back into one flat solution.
+geq_status run_batch_pipelined(int device, Engine &ea, Engine &eb, std::vector<GameInput> &in, geq_solution &sol) {
+  const uint32_t n_games = (uint32_t)in.size();
+  unsigned long long total = 0;
+  for (auto &gi : in) total += gi.g.n_vertices;
+  uint32_t k = 0;
+  unsigned long long acc = 0;
+  while (k + 1 < n_games && acc < total / 2) acc += in[k++].g.n_vertices;
+  auto part = [&](uint32_t b, uint32_t e) {
+    std::vector<GameInput> v(e - b);
+    for (uint32_t i = b; i < e; i++) {
+      GameInput &d = v[i - b];
+      d.g = in[i].g;
+      d.init = in[i].init;
+      d.to_reach = in[i].to_reach;  // points into in[i], alive for the call
+      d.n_reach = in[i].n_reach;
+      d.std_reach = in[i].std_reach;
+      d.rows_unchecked = in[i].rows_unchecked;
+    }
+    return v;
+  };
+  std::vector<GameInput> ia = part(0, k), ib = part(k, n_games);
+  GamesPtr da, db;
+  Engine::Readback ra, rb;
+  geq_solve_stats sa{}, sb{};
+  geq_status st_a = GEQ_OK, st_b = GEQ_OK;
+  std::string err_b;
+  std::promise<void> a_up;
+  std::future<void> a_up_done = a_up.get_future();
+  std::thread tb([&]() {
+    cudaSetDevice(device);
+    a_up_done.wait();
+    st_b = eb.upload(ib, db);
+    if (!st_b) st_b = eb.solve(*db, &sb);
+    if (!st_b) st_b = eb.download_prepare(*db, rb);
+    if (st_b) err_b = geq_last_error();
+  });
+  st_a = ea.upload(ia, da);
+  a_up.set_value();
+  if (!st_a) st_a = ea.solve(*da, &sa);
+  if (!st_a) st_a = ea.download_prepare(*da, ra);
+  tb.join();
+  if (st_a || st_b) {
+    if (da) ea.download_release(*da, ra);
+    if (db) eb.download_release(*db, rb);
+    if (!st_a) set_last_error(err_b);
+    return st_a ? st_a : st_b;
   }
+  sol.energy_size = 1;
+  const uint64_t na = da->N + da->n_games;
+  sol.n_offsets = na + db->N + db->n_games;
+  sol.n_words = ra.total + rb.total;
+  if (!sol.off_buf.alloc(ea.st->hpool, sol.n_offsets * 8) || !sol.data_buf.alloc(ea.st->hpool, sol.n_words * 4)) {
+    ea.download_release(*da, ra);
+    eb.download_release(*db, rb);
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu result words", (unsigned long long)sol.n_words);
+  }
+  uint64_t *off = (uint64_t *)sol.off_buf.p;
+  uint32_t *data = (uint32_t *)sol.data_buf.p;
+  geq_status st = ea.download_copy(*da, ra, off, data);
+  if (!st) st = eb.download_copy(*db, rb, off + na, data + ra.total);
+  else eb.download_release(*db, rb);
+  if (st) return st;
+  sol.n_vertices.resize(n_games);
+  sol.offsets_base.resize(n_games);
+  sol.data_base.resize(n_games);
+  fill_bases(*da, sol, 0, 0, 0);
+  fill_bases(*db, sol, k, na, ra.total);
+  sol.stats = sa;
+  sol.stats.rounds = std::max(sa.rounds, sb.rounds);
+  sol.stats.positions_computed += sb.positions_computed;
+  sol.stats.edges_relaxed += sb.edges_relaxed;
+  sol.stats.algorithmic_bytes += sb.algorithmic_bytes;
+  sol.stats.arena_compactions += sb.arena_compactions;
+  sol.stats.kernel_launches += sb.kernel_launches;
+  sol.stats.device_ms = std::max(sa.device_ms, sb.device_ms);
   return GEQ_OK;
 }
 

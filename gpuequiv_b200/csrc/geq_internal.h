@@ -154,6 +154,8 @@ using GamesPtr = std::unique_ptr<DeviceGamesImpl, GamesDeleter>;
 struct geq_context {
   int device = 0;
   std::unique_ptr<geq::Engine> engine;
+  // second engine for large batches, created on first use
+  std::unique_ptr<geq::Engine> engine2;
 };
 
 struct geq_device_games {
@@ -171,6 +173,17 @@ class Engine {
   geq_status solve(DeviceGamesImpl &dg, geq_solve_stats *stats);
   // All positions of all games.
   geq_status download(DeviceGamesImpl &dg, geq_solution &sol);
+  // download in two steps: prepare gathers every list on the device and
+  // counts the words; copy reads offsets (relative to each game) and words
+  // into the given host memory and releases the device buffers.
+  struct Readback {
+    unsigned long long *goff = nullptr, *rel = nullptr;
+    uint32_t *out = nullptr;
+    unsigned long long total = 0;
+  };
+  geq_status download_prepare(DeviceGamesImpl &dg, Readback &rb);
+  geq_status download_copy(DeviceGamesImpl &dg, Readback &rb, uint64_t *off_dst, uint32_t *data_dst);
+  void download_release(DeviceGamesImpl &dg, Readback &rb);
   // Only the listed positions: game g's local positions first_g .. first_g+count_g-1
   // become game g of the solution.
   geq_status download_selected(DeviceGamesImpl &dg, const std::vector<uint32_t> &first,
@@ -192,5 +205,9 @@ class Engine {
   struct State;
   std::unique_ptr<State> st;
 };
+
+// A large batch split in two halves by positions on engines ea and eb: the
+// upload of the second half overlaps the solve of the first.
+geq_status run_batch_pipelined(int device, Engine &ea, Engine &eb, std::vector<GameInput> &in, geq_solution &sol);
 
 }  // namespace geq

@@ -127,6 +127,7 @@ def stress_game(seed: int = 2, n: int = 2_000_000, m: int = 10_000_000, p_att: f
         else:
             ok = idx[deg[idx] > 0]
             np.add.at(deg, ok, -1)
+            np.maximum(deg, 0, out=deg)  # a position drawn twice
         diff = m - int(deg.sum())
     row = np.zeros(n + 1, dtype=np.uint32)
     np.cumsum(deg, out=row[1:])

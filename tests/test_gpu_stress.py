@@ -62,3 +62,30 @@ def test_stress_full_size(geq, ctx):
     # changes no position
     assert ora.check_fixpoint(row, col, wt, att, got[0].astype(np.uint64), got[1]) == (0, None)
     assert stats["edges_relaxed"] >= sol.stats["edges_relaxed"] * 0 and stats["rounds"] >= 1
+
+
+def test_split_batch_matches_one_engine(geq, ctx):
+    """A batch of at least 2**21 positions runs as two halves on two engines
+    (the second half uploads while the first solves): every game's lists
+    equal those of the same batch on one engine, and the oracle's for a game
+    of each half."""
+    from gpuequiv_b200 import synth
+    from gpuequiv_b200._lib import TUNE_NO_SPLIT
+    games = [synth.scaled_stress_game(20 + i, 200_000, 1_000_000) for i in range(12)]
+    graphs = [geq.GameGraph.from_csr(r, c, w, a, geq.EnergyConf.STANDARD) for r, c, w, a in games]
+    offs, data, stats = geq.run_batch_raw(graphs, ctx)
+    ctx.set_tuning(flags=TUNE_NO_SPLIT)
+    try:
+        offs1, data1, stats1 = geq.run_batch_raw(graphs, ctx)
+    finally:
+        ctx.set_tuning()
+    assert stats["positions_computed"] == stats1["positions_computed"]
+    for i in range(len(games)):
+        a, b = canonical(offs[i], data[i]), canonical(offs1[i], data1[i])
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), f"game {i} differs"
+    for i in (0, len(games) - 1):
+        row, col, wt, att = games[i]
+        sol = ora.run_game(6, 3, row, col, wt, att, ora.standard_reach(row, att))
+        exp = canonical(sol.offsets, sol.data)
+        got = canonical(offs[i], data[i])
+        assert np.array_equal(got[0], exp[0]) and np.array_equal(got[1], exp[1]), f"game {i} differs from the oracle"
