@@ -315,6 +315,56 @@ def run_serving(ctx, graphs, lam: float, seconds: float, seed: int) -> dict:
 
 
 # ---- arms -----------------------------------------------------------------------
+def run_lts_pipeline(ctx, seeds, graphs, args, d: Dist) -> dict:
+    """compare_batch over the batch's LTSs: the whole LTS -> energies path
+    (minimisation on the host cores, GameBuild on the device, batched solve,
+    start-position energies read back), against the host GameBuild of the
+    same minimised LTSs on all host cores."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import gpuequiv_b200 as geq
+    synth = synth_mod()
+    jobs = []
+    for seed in seeds:
+        src, dst, lab, p, q = synth.batched_lts(seed)
+        jobs.append((geq.TransitionSystem.from_arrays(src, dst, lab), int(p), int(q)))
+    # the start energies agree with the resident solve's (first 64 games)
+    first = geq.compare_batch(jobs[:64], context=ctx)
+    offs, data, _ = geq.run_batch_raw(graphs[:64], ctx, geq.c_views(graphs[:64]))
+    for k in range(len(first)):
+        ref = sorted(int(x) for x in data[k][offs[k][0]:offs[k][1]].reshape(-1))
+        assert sorted(int(x) for x in np.asarray(first[k].array).reshape(-1)) == ref, f"job {k}"
+    geq.compare_batch(jobs, context=ctx)  # warm-up
+    d.barrier()
+    times = []
+    for _ in range(max(1, min(args.steps, 3))):
+        t = time.perf_counter()
+        geq.compare_batch(jobs, context=ctx)
+        times.append(time.perf_counter() - t)
+    pipe_s = d.max(float(np.median(times)))
+    # the two builders alone, on the minimised LTSs
+    reds = []
+    for lts, p, q in jobs:
+        red, mp = lts.bisimilar_minimize()
+        reds.append((red, int(mp[p]), int(mp[q])))
+    b = geq.GameBatch(reds, context=ctx)
+    dev_build = []
+    for _ in range(3):
+        b = geq.GameBatch(reds, context=ctx)
+        dev_build.append(b.stats["upload_ms"] + b.stats["build_ms"])
+    threads = os.cpu_count() or 4
+    t = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda j: geq.GameBuild.compare(*j), reds))
+    host_build_ms = (time.perf_counter() - t) * 1e3
+    return {"workload": "compare_batch over the same 4096 LTSs (unminimised): host minimisation, device GameBuild, "
+                        "batched solve, start energies read back",
+            "games_s": d.sum(len(jobs)) / pipe_s, "ms_per_step": pipe_s * 1e3,
+            "device_build_ms": float(np.median(dev_build)), "build_levels": b.stats["levels"],
+            "build_kernel_launches": b.stats["kernel_launches"],
+            "host_build_ms_all_cores": host_build_ms, "host_threads": threads}
+
+
 def run_reference(args, d: Dist):
     if d.rank != 0:
         return
@@ -415,6 +465,10 @@ def run_ours(args, d: Dist):
     e2e_s = d.max(float(np.median(e2e_t)))
     e2e = total_games / e2e_s
 
+    # ---- LTS -> verdict: compare_batch from the unminimised LTSs (host
+    # minimisation, games built on the device, solved, start energies back) ----
+    lts_pipe = run_lts_pipeline(ctx, seeds, graphs, args, d)
+
     # ---- plain CUDA: one call per game (sample) ----
     idx = sample_indices(len(graphs), args.plain_sample)
     pviews = [geq.c_views([graphs[i]]) for i in idx]
@@ -486,6 +540,7 @@ def run_ours(args, d: Dist):
             "plain_cuda": {"value": plain_rate, "unit": UNIT, "sample": f"{len(idx)} games (every "
                            f"{max(1, len(graphs) // len(idx))}th job), one geq_energy_game_run call each"},
             "batched_vs_plain": value / plain_rate if plain_rate else None,
+            "lts_pipeline": lts_pipe,
             "stress": stress,
             "serving": {"workload": "Poisson arrivals of single compare(p,q) games drawn from this batch "
                                     "(LTS 20-5000 states), geq_server with 2 pipelines, 150 GB admission budget",

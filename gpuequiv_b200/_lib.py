@@ -58,6 +58,15 @@ class geq_server_stats(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class geq_game_batch_info(C.Structure):
+    _fields_ = [("positions", C.c_uint64), ("edges", C.c_uint64), ("levels", C.c_uint32),
+                ("kernel_launches", C.c_uint32), ("attempts", C.c_uint32), ("upload_ms", C.c_double),
+                ("build_ms", C.c_double), ("download_ms", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class geq_position(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("p", C.c_uint32), ("q", C.POINTER(C.c_uint32)), ("n_q", C.c_uint32),
                 ("qx", C.POINTER(C.c_uint32)), ("n_qx", C.c_uint32)]
@@ -152,6 +161,12 @@ _SIGS = {
     "geq_game_build_n_starting_points": ([vp], C.c_uint32),
     "geq_game_build_position": ([vp, C.c_uint32, C.POINTER(geq_position)], C.c_int),
     "geq_game_build_free": ([vp], None),
+    "geq_game_build_compare_batch": ([vp, C.c_uint32, C.POINTER(vp), u32p, u32p, C.c_uint64, C.POINTER(vp)],
+                                     C.c_int),
+    "geq_game_batch_n_jobs": ([vp], C.c_uint32),
+    "geq_game_batch_graph": ([vp, C.c_uint32, C.POINTER(geq_game_graph)], C.c_int),
+    "geq_game_batch_stats": ([vp, C.POINTER(geq_game_batch_info)], None),
+    "geq_game_batch_free": ([vp], None),
     "geq_compare": ([vp, vp, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(vp)], C.c_int),
     "geq_compare_batch": ([vp, C.c_uint32, C.POINTER(vp), u32p, u32p, C.c_int, C.POINTER(vp)], C.c_int),
     "geq_equivalences": ([vp, vp, C.c_int, C.POINTER(vp)], C.c_int),

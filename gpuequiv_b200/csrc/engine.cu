@@ -2182,6 +2182,9 @@ static geq_status staged_upload(std::vector<CopyJob> &jobs, const char *stage, c
   return GEQ_OK;
 }
 
+void *Engine::stream_handle() const { return (void *)st->stream; }
+std::shared_ptr<HostPool> Engine::host_pool() const { return st->hpool; }
+
 geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
@@ -2366,6 +2369,95 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   D.init_data = (uint32_t *)(D.inbuf + off_init);
   D.d_node_base = (unsigned long long *)(D.inbuf + off_base);
   if (any_init) D.desc_init = (unsigned long long *)(D.inbuf + off_desc);
+  geq_status ast = alloc_work(D, any_init);
+  if (ast) return ast;
+  cudaStream_t S = s.stream;
+#if GEQ_PATH_PROFILE
+  const double t_stage0 = tsince();
+#endif
+  geq_status ust = staged_upload(copies, H, D.inbuf, total_bytes, S);
+#if GEQ_PATH_PROFILE
+  const double t_stage1 = tsince();
+  std::fprintf(stderr, "GEQ_UPLOAD host_prep_ms %.2f staged_ms %.2f bytes %zu\n", t_stage0, t_stage1 - t_stage0,
+               total_bytes);
+#endif
+  if (ust) return ust;
+  return finish_upload(dg, any_init, out);
+}
+
+// Games already on the device in the solver's input layout (built by the
+// device game builder on this engine's stream): copied into one input block
+// like a host upload, then the same device half.
+geq_status Engine::upload_built(const BuiltGames &b, GamesPtr &out) {
+  State &s = *st;
+  if (b.n_games == 0) return fail(GEQ_ERR_INVALID_INPUT, "no games");
+  GamesPtr dg(new DeviceGamesImpl());
+  dg->owner = &s;
+  s.live.insert(dg.get());
+  dg->conf = Conf(6, 3);
+  dg->generic = (tuning.flags & GEQ_TUNE_FORCE_GENERIC) != 0;
+  dg->n_games = b.n_games;
+  dg->node_base.assign(dg->n_games + 1, 0);
+  dg->edge_base.assign(dg->n_games + 1, 0);
+  for (uint32_t g = 0; g < b.n_games; g++) {
+    dg->node_base[g + 1] = dg->node_base[g] + b.n_nodes[g];
+    dg->edge_base[g + 1] = dg->edge_base[g] + b.n_edges[g];
+  }
+  dg->N = dg->node_base.back();
+  dg->M = dg->edge_base.back();
+  if (dg->N != b.N || dg->M != b.M) return fail(GEQ_ERR_INTERNAL, "built games: sizes disagree");
+  if (dg->N >= 0xFFFFFFF0ull || dg->M >= 0xFFFFFFF0ull)
+    return fail(GEQ_ERR_INVALID_INPUT, "too many positions/edges for 32-bit ids (%llu, %llu)", dg->N, dg->M);
+  dg->std_reach = true;
+  dg->rows_on_device = false;  // rows are valid by construction
+  dg->init_total = 1;
+  dg->n_reach = 0;
+  const unsigned long long N = dg->N, M = dg->M;
+  const size_t off_row = 0, off_col = off_row + (N + 1) * 4, off_wt = off_col + M * 4, off_flags = off_wt + M * 4;
+  const size_t off_init = (off_flags + N + 15) & ~size_t(15);
+  const size_t off_base = (off_init + 4 + 15) & ~size_t(15);
+  const size_t total_bytes = off_base + (dg->n_games + 1) * 8 * 3;
+  const size_t small = 16 + (dg->n_games + 1) * 8 * 3;
+  geq_status stt = ensure_stage(s, small);
+  if (stt) return stt;
+  uint32_t *h_tail = (uint32_t *)s.stage;  // row[N] = M, init[0] = 0
+  h_tail[0] = (uint32_t)M;
+  h_tail[1] = 0;
+  unsigned long long *h_nb = (unsigned long long *)(s.stage + 16);
+  unsigned long long *h_eb = h_nb + (dg->n_games + 1), *h_gn = h_eb + (dg->n_games + 1);
+  for (uint32_t g = 0; g <= dg->n_games; g++) {
+    h_nb[g] = dg->node_base[g];
+    h_eb[g] = dg->edge_base[g];
+    h_gn[g] = g < dg->n_games ? b.n_nodes[g] : 0;
+  }
+  DeviceGamesImpl &D = *dg;
+  if (!D.alloc(D.inbuf, total_bytes))
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation of %zu input bytes failed", total_bytes);
+  D.row = (uint32_t *)(D.inbuf + off_row);
+  D.col = (uint32_t *)(D.inbuf + off_col);
+  D.wt = (uint32_t *)(D.inbuf + off_wt);
+  D.flags = (uint8_t *)(D.inbuf + off_flags);
+  D.reach = (uint32_t *)(D.inbuf + off_init);
+  D.init_data = (uint32_t *)(D.inbuf + off_init);
+  D.d_node_base = (unsigned long long *)(D.inbuf + off_base);
+  geq_status ast = alloc_work(D, false);
+  if (ast) return ast;
+  cudaStream_t S = s.stream;
+  CU(cudaMemcpyAsync(D.row, b.row_rel, N * 4, cudaMemcpyDeviceToDevice, S));
+  CU(cudaMemcpyAsync(D.row + N, h_tail, 4, cudaMemcpyHostToDevice, S));
+  if (M) {
+    CU(cudaMemcpyAsync(D.col, b.col, M * 4, cudaMemcpyDeviceToDevice, S));
+    CU(cudaMemcpyAsync(D.wt, b.wt, M * 4, cudaMemcpyDeviceToDevice, S));
+  }
+  CU(cudaMemcpyAsync(D.flags, b.att, N, cudaMemcpyDeviceToDevice, S));
+  CU(cudaMemcpyAsync(D.init_data, h_tail + 1, 4, cudaMemcpyHostToDevice, S));
+  CU(cudaMemcpyAsync(D.d_node_base, h_nb, (dg->n_games + 1) * 8 * 3, cudaMemcpyHostToDevice, S));
+  return finish_upload(dg, false, out);
+}
+
+// Work arrays of an upload: reverse CSR, descriptors, frontier, arena.
+geq_status Engine::alloc_work(DeviceGamesImpl &D, bool any_init) {
+  const unsigned long long N = D.N, M = D.M;
   if (!D.alloc(D.rrow, N + 1) || !D.alloc(D.rcol, M) || !D.alloc(D.desc, N) ||
       (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, 2 * ((N + 31) / 32)) ||
       !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1) ||
@@ -2375,15 +2467,16 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
   D.arena_cap[0] = DevPool::round_size(cap * 4) / 4;
+  return GEQ_OK;
+}
+
+// Device half of an upload, once the inputs are in D.inbuf: row and column
+// ids into the global id space, checks, initial state, reverse CSR.
+geq_status Engine::finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out) {
+  State &s = *st;
+  DeviceGamesImpl &D = *dg;
+  const unsigned long long N = D.N, M = D.M, n_reach = D.n_reach;
   cudaStream_t S = s.stream;
-#if GEQ_PATH_PROFILE
-  const double t_stage0 = tsince();
-#endif
-  geq_status ust = staged_upload(copies, H, D.inbuf, total_bytes, S);
-#if GEQ_PATH_PROFILE
-  const double t_stage1 = tsince();
-#endif
-  if (ust) return ust;
   CU(cudaMemsetAsync(D.mark, 0, 2 * ((N + 31) / 32) * 4, S));
   CU(cudaMemsetAsync(s.d_err, 0, 4, S));
   const unsigned grid = (unsigned)std::max(1, n_sms * 8);
@@ -2423,10 +2516,6 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   s.pool.put(roff, (N + 1) * 8);
   CU(cudaGetLastError());
   const uint32_t h_err = s.h_ctr->pad;
-#if GEQ_PATH_PROFILE
-  std::fprintf(stderr, "GEQ_UPLOAD host_prep_ms %.2f staged_ms %.2f device_ms %.2f total_ms %.2f bytes %zu\n", t_stage0,
-               t_stage1 - t_stage0, tsince() - t_stage1, tsince(), total_bytes);
-#endif
   if (h_err & 1u) return fail(GEQ_ERR_INVALID_INPUT, "Node index too high: a successor index is out of range");
   if (h_err & 2u) return fail(GEQ_ERR_INVALID_INPUT, "an edge update names no element or sets padding bits");
   if (h_err & 4u) return fail(GEQ_ERR_INVALID_INPUT, "row_offsets must start at 0 and must not decrease");

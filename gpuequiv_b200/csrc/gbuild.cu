@@ -1,0 +1,405 @@
+// gbuild.cu - the device game builder (gbuild.cuh) on the CUDA stream of a
+// context: GameBuild::compare (src/gamebuild.rs:165-170) for a batch of
+// (LTS, p, q) jobs, one breadth-first level per group of launches, results
+// copied back as one CSR game graph per job.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstring>
+#include <mutex>
+
+#include "gbuild.cuh"
+#include "geq_internal.h"
+#include "lts.h"
+
+namespace geq {
+namespace gb {
+
+constexpr int EACH_T = 256;
+constexpr int SCAN_T = 256;
+constexpr int SCAN_ITEMS = 8;
+constexpr uint32_t SCAN_TILE = SCAN_T * SCAN_ITEMS;
+
+template <class F>
+__global__ void __launch_bounds__(EACH_T) k_each(uint32_t n, F f) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) f(i);
+}
+
+// exclusive scan of a block's values (one per thread); returns the block total
+__device__ __forceinline__ unsigned long long block_scan(unsigned long long x, unsigned long long &total) {
+  __shared__ unsigned long long ws[SCAN_T / 32];
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned long long inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= (uint32_t)o) inc += y;
+  }
+  if (lane == 31) ws[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    unsigned long long s = lane < SCAN_T / 32 ? ws[lane] : 0ull;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= (uint32_t)o) s += y;
+    }
+    if (lane < SCAN_T / 32) ws[lane] = s;
+  }
+  __syncthreads();
+  const unsigned long long before = (w ? ws[w - 1] : 0ull) + inc - x;
+  total = ws[SCAN_T / 32 - 1];
+  __syncthreads();
+  return before;
+}
+
+// per tile of SCAN_TILE values: its sum
+__global__ void __launch_bounds__(SCAN_T) k_scan_up(const uint32_t *in, uint32_t n, unsigned long long *part) {
+  const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  unsigned long long s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++)
+    if (base + k < n) s += in[base + k];
+  unsigned long long total;
+  block_scan(s, total);
+  if (threadIdx.x == 0) part[blockIdx.x] = total;
+}
+// exclusive scan of the tile sums in one block; the grand total to *tot
+__global__ void __launch_bounds__(SCAN_T) k_scan_mid(unsigned long long *part, uint32_t nb, unsigned long long *tot) {
+  unsigned long long carry = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += SCAN_T) {
+    const uint32_t i = b0 + threadIdx.x;
+    const unsigned long long x = i < nb ? part[i] : 0ull;
+    unsigned long long total;
+    const unsigned long long e = block_scan(x, total);
+    if (i < nb) part[i] = carry + e;
+    carry += total;
+  }
+  if (threadIdx.x == 0) *tot = carry;
+}
+__global__ void __launch_bounds__(SCAN_T) k_scan_down(const uint32_t *in, uint32_t n, const unsigned long long *part,
+                                                      uint32_t *out) {
+  const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+  uint32_t v[SCAN_ITEMS];
+  unsigned long long s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    v[k] = base + k < n ? in[base + k] : 0u;
+    s += v[k];
+  }
+  unsigned long long total;
+  unsigned long long e = block_scan(s, total) + part[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++)
+    if (base + k < n) {
+      out[base + k] = (uint32_t)e;
+      e += v[k];
+    }
+}
+
+// Backend of the level loop: stream-ordered allocation, kernels and copies on
+// the context's stream.
+struct DevBackend {
+  cudaStream_t s = nullptr;
+  int n_sms = 148;
+  cudaError_t err = cudaSuccess;
+  unsigned long long *part = nullptr;
+  uint32_t part_cap = 0;
+  uint32_t launches = 0;
+
+  void note(cudaError_t e) {
+    if (e != cudaSuccess && err == cudaSuccess) err = e;
+  }
+  bool ok() {
+    note(cudaGetLastError());
+    return err == cudaSuccess;
+  }
+  void *alloc(size_t b) {
+    void *p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, b, s);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return p;
+  }
+  void release(void *p) {
+    if (p) note(cudaFreeAsync(p, s));
+  }
+  void fill(void *p, int v, size_t b) { note(cudaMemsetAsync(p, v, b, s)); }
+  void copy(void *d, const void *src, size_t b) {
+    if (b) note(cudaMemcpyAsync(d, src, b, cudaMemcpyDefault, s));
+  }
+  void fetch(void *h, const void *d, size_t b) {
+    copy(h, d, b);
+    note(cudaStreamSynchronize(s));
+  }
+  template <class F>
+  void each(uint32_t n, const F &f) {
+    if (!n) return;
+    const uint32_t blocks = std::min<uint32_t>((n + EACH_T - 1) / EACH_T, (uint32_t)n_sms * 16);
+    k_each<<<blocks, EACH_T, 0, s>>>(n, f);
+    launches++;
+  }
+  void scan(const uint32_t *in, uint32_t *out, uint32_t n, unsigned long long *tot) {
+    const uint32_t nb = std::max<uint32_t>(1, (n + SCAN_TILE - 1) / SCAN_TILE);
+    if (nb > part_cap) {
+      release(part);
+      part_cap = std::max<uint32_t>(nb, 1024);
+      part = (unsigned long long *)alloc((size_t)part_cap * 8);
+      if (!part) {
+        part_cap = 0;
+        note(cudaErrorMemoryAllocation);
+        return;
+      }
+    }
+    k_scan_up<<<nb, SCAN_T, 0, s>>>(in, n, part);
+    k_scan_mid<<<1, SCAN_T, 0, s>>>(part, nb, tot);
+    k_scan_down<<<nb, SCAN_T, 0, s>>>(in, n, part, out);
+    launches += 3;
+  }
+  ~DevBackend() {
+    if (part) cudaFreeAsync(part, s);
+  }
+};
+
+}  // namespace gb
+}  // namespace geq
+
+namespace geq {
+
+// One device build: the LTSs of all jobs staged and uploaded as one id space,
+// then the level loop.  The result arrays live until the Build object dies.
+struct DeviceBuild {
+  gb::DevBackend be;
+  std::unique_ptr<gb::Builder<gb::DevBackend>> b;
+  gb::Result r;
+  char *din = nullptr;
+  HostBuf stage;
+  double upload_ms = 0, build_ms = 0;
+  ~DeviceBuild() {
+    b.reset();
+    be.release(din);
+    cudaStreamSynchronize(be.s);
+  }
+};
+
+static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *p,
+                               const uint32_t *q, uint64_t max_positions, DeviceBuild &db) {
+  using clk = std::chrono::steady_clock;
+  std::vector<uint64_t> sb(n_jobs + 1, 0), tb(n_jobs + 1, 0);
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    sb[j + 1] = sb[j] + L[j]->n;
+    tb[j + 1] = tb[j] + L[j]->n_transitions();
+  }
+  const uint64_t NS = sb[n_jobs], MS = tb[n_jobs];
+  if (NS >= (1ull << 31) || MS >= (1ull << 32) - 1)
+    return fail(GEQ_ERR_INVALID_INPUT, "batch too large: %llu states, %llu transitions", (unsigned long long)NS,
+                (unsigned long long)MS);
+  const uint32_t max_pos = max_positions >= (1ull << 31) ? 0u : (uint32_t)max_positions;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(GEQ_ERR_CUDA, "cudaSetDevice(%d) failed", device);
+  }
+  // the builder allocates stream-ordered from the device's default pool; keep
+  // freed blocks cached in this process instead of returning them at every
+  // synchronisation
+  static std::once_flag pool_once[64];
+  if (device >= 0 && device < 64)
+    std::call_once(pool_once[device], [device]() {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      cudaGetLastError();
+    });
+  gb::DevBackend &be = db.be;
+  be.s = (cudaStream_t)eng.stream_handle();
+  be.n_sms = eng.n_sms;
+  // stage the LTSs: soff | slab | stgt | sjob | p0 | q0
+  const auto t0 = clk::now();
+  const size_t o_soff = 0, o_slab = o_soff + (NS + 1) * 4, o_stgt = o_slab + MS * 4, o_sjob = o_stgt + MS * 4,
+               o_p0 = o_sjob + NS * 4, o_q0 = o_p0 + (size_t)n_jobs * 4, bytes = o_q0 + (size_t)n_jobs * 4;
+  if (!db.stage.alloc(eng.host_pool(), bytes)) return fail(GEQ_ERR_OUT_OF_MEMORY, "staging %zu bytes", bytes);
+  char *hs = (char *)db.stage.p;
+  parallel_for(n_jobs, [&](uint32_t j) {
+    const Lts &l = *L[j];
+    uint32_t *soff = (uint32_t *)(hs + o_soff) + sb[j];
+    int32_t *slab = (int32_t *)(hs + o_slab) + tb[j];
+    uint32_t *stgt = (uint32_t *)(hs + o_stgt) + tb[j];
+    uint32_t *sjob = (uint32_t *)(hs + o_sjob) + sb[j];
+    for (uint32_t s = 0; s < l.n; s++) {
+      soff[s] = (uint32_t)(tb[j] + l.off[s]);
+      sjob[s] = j;
+    }
+    const uint64_t m = l.n_transitions();
+    for (uint64_t k = 0; k < m; k++) {
+      slab[k] = l.lab_[k];
+      stgt[k] = (uint32_t)(sb[j] + l.tgt[k]);
+    }
+    ((uint32_t *)(hs + o_p0))[j] = (uint32_t)(sb[j] + p[j]);
+    ((uint32_t *)(hs + o_q0))[j] = (uint32_t)(sb[j] + q[j]);
+  });
+  ((uint32_t *)(hs + o_soff))[NS] = (uint32_t)MS;
+  db.din = (char *)be.alloc(bytes);
+  if (!db.din) return fail(GEQ_ERR_OUT_OF_MEMORY, "device input %zu bytes", bytes);
+  be.copy(db.din, hs, bytes);
+  gb::Input in;
+  in.NS = (uint32_t)NS;
+  in.MS = (uint32_t)MS;
+  in.n_jobs = n_jobs;
+  in.soff = (const uint32_t *)(db.din + o_soff);
+  in.slab = (const int32_t *)(db.din + o_slab);
+  in.stgt = (const uint32_t *)(db.din + o_stgt);
+  in.sjob = (const uint32_t *)(db.din + o_sjob);
+  in.p0 = (const uint32_t *)(db.din + o_p0);
+  in.q0 = (const uint32_t *)(db.din + o_q0);
+  in.max_pos = max_pos;
+  const auto t1 = clk::now();
+  db.b.reset(new gb::Builder<gb::DevBackend>(be));
+  const int rc = db.b->run(in, db.r);
+  db.upload_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+  db.build_ms = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
+  if (!be.ok()) return fail(GEQ_ERR_CUDA, "device game build: %s", cudaGetErrorString(be.err));
+  if (rc == 1) return fail(GEQ_ERR_OUT_OF_MEMORY, "device game build: out of device memory");
+  if (rc == 2) return fail(GEQ_ERR_INVALID_INPUT, "device game build: game beyond 2^31 positions or 2^32 edges");
+  if (rc == 3) return fail(GEQ_ERR_INTERNAL, "device game build: fingerprint collisions under four hash seeds");
+  return GEQ_OK;
+}
+
+// GameBuild::compare of every job on the device, handed to the solver as an
+// upload (the graphs never leave the device).  jobs whose game exceeds
+// max_positions (0 = no bound) fail with GEQ_ERR_OUT_OF_MEMORY.
+geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *p,
+                            const uint32_t *q, uint64_t max_positions, GamesPtr &out, double *build_ms) {
+  DeviceBuild db;
+  geq_status st = device_build(eng, device, n_jobs, L, p, q, max_positions, db);
+  if (st) return st;
+  std::vector<uint32_t> jcount(n_jobs), jm(n_jobs), jover(n_jobs);
+  db.be.copy(jcount.data(), db.r.jcount, (size_t)n_jobs * 4);
+  db.be.copy(jover.data(), db.r.jover, (size_t)n_jobs * 4);
+  db.be.fetch(jm.data(), db.r.jm, (size_t)n_jobs * 4);
+  if (!db.be.ok()) return fail(GEQ_ERR_CUDA, "device game build: %s", cudaGetErrorString(db.be.err));
+  for (uint32_t j = 0; j < n_jobs; j++)
+    if (jover[j]) return fail(GEQ_ERR_OUT_OF_MEMORY, "job %u: game exceeds %llu positions", j,
+                              (unsigned long long)max_positions);
+  if (build_ms) *build_ms = db.upload_ms + db.build_ms;
+  BuiltGames bg;
+  bg.n_games = n_jobs;
+  bg.n_nodes = jcount.data();
+  bg.n_edges = jm.data();
+  bg.N = db.r.N;
+  bg.M = db.r.M;
+  bg.row_rel = db.r.rrel;
+  bg.col = db.r.col;
+  bg.wt = db.r.wt;
+  bg.att = db.r.att;
+  return eng.upload_built(bg, out);  // copies on the same stream before db's buffers are freed
+}
+
+}  // namespace geq
+
+using namespace geq;
+
+struct geq_game_batch {
+  uint32_t n_jobs = 0;
+  std::vector<uint32_t> node_base, edge_base, n_nodes, n_edges;
+  std::vector<uint8_t> over;
+  HostBuf row, col, wt, att;
+  uint64_t N = 0, M = 0;
+  uint32_t levels = 0, launches = 0, attempts = 0;
+  double upload_ms = 0, build_ms = 0, download_ms = 0;
+};
+
+extern "C" geq_status geq_game_build_compare_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts,
+                                                   const uint32_t *p, const uint32_t *q, uint64_t max_positions,
+                                                   geq_game_batch **out) {
+  using clk = std::chrono::steady_clock;
+  if (!ctx || !ctx->engine) return fail(GEQ_ERR_INVALID_INPUT, "context is NULL");
+  if (!out || !lts || !p || !q) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  *out = nullptr;
+  if (n_jobs == 0) return fail(GEQ_ERR_INVALID_INPUT, "no jobs");
+  std::vector<const Lts *> L(n_jobs);
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    if (!lts[j]) return fail(GEQ_ERR_INVALID_INPUT, "job %u: LTS is NULL", j);
+    L[j] = &lts[j]->l;
+    if (p[j] >= L[j]->n || q[j] >= L[j]->n) return fail(GEQ_ERR_INVALID_INPUT, "job %u: process out of range", j);
+  }
+  Engine &eng = *ctx->engine;
+  std::unique_ptr<geq_game_batch> res(new geq_game_batch());
+  res->n_jobs = n_jobs;
+  DeviceBuild db;
+  geq_status st = device_build(eng, ctx->device, n_jobs, L.data(), p, q, max_positions, db);
+  if (st) return st;
+  // per-job CSR back to the host
+  const auto t2 = clk::now();
+  const gb::Result &r = db.r;
+  gb::DevBackend &be = db.be;
+  const uint32_t J = n_jobs;
+  std::vector<uint32_t> jcount(J), jover(J), jbase(J);
+  auto hp = eng.host_pool();
+  if (!res->row.alloc(hp, ((size_t)r.N + J) * 4) || !res->col.alloc(hp, (size_t)r.M * 4) ||
+      !res->wt.alloc(hp, (size_t)r.M * 4) || !res->att.alloc(hp, (size_t)r.N))
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "host result buffers");
+  be.copy(res->row.p, r.row, ((size_t)r.N + J) * 4);
+  be.copy(res->col.p, r.col, (size_t)r.M * 4);
+  be.copy(res->wt.p, r.wt, (size_t)r.M * 4);
+  be.copy(res->att.p, r.att, (size_t)r.N);
+  be.copy(jcount.data(), r.jcount, (size_t)J * 4);
+  be.copy(jover.data(), r.jover, (size_t)J * 4);
+  be.fetch(jbase.data(), r.jbase, (size_t)J * 4);
+  if (!be.ok()) return fail(GEQ_ERR_CUDA, "device game build: %s", cudaGetErrorString(be.err));
+  res->node_base = jbase;
+  res->n_nodes = jcount;
+  res->edge_base.resize(J);
+  res->n_edges.resize(J);
+  res->over.resize(J);
+  const uint32_t *row = (const uint32_t *)res->row.p;
+  uint64_t eb = 0;
+  for (uint32_t j = 0; j < J; j++) {
+    res->edge_base[j] = (uint32_t)eb;
+    res->n_edges[j] = row[(size_t)jbase[j] + j + jcount[j]];
+    res->over[j] = jover[j] != 0;
+    eb += res->n_edges[j];
+  }
+  res->N = r.N;
+  res->M = r.M;
+  res->levels = r.levels;
+  res->attempts = r.attempts;
+  res->launches = be.launches;
+  res->upload_ms = db.upload_ms;
+  res->build_ms = db.build_ms;
+  res->download_ms = std::chrono::duration<double, std::milli>(clk::now() - t2).count();
+  *out = res.release();
+  return GEQ_OK;
+}
+
+extern "C" uint32_t geq_game_batch_n_jobs(const geq_game_batch *b) { return b ? b->n_jobs : 0; }
+
+extern "C" geq_status geq_game_batch_graph(const geq_game_batch *b, uint32_t job, geq_game_graph *out) {
+  if (!b || !out) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  if (job >= b->n_jobs) return fail(GEQ_ERR_INVALID_INPUT, "job %u out of range", job);
+  if (b->over[job]) return fail(GEQ_ERR_OUT_OF_MEMORY, "job %u: game exceeds the position bound", job);
+  out->conf = geq_energy_conf{6, 3};
+  out->n_vertices = b->n_nodes[job];
+  out->row_offsets = (const uint32_t *)b->row.p + (size_t)b->node_base[job] + job;
+  out->column_indices = (const uint32_t *)b->col.p + b->edge_base[job];
+  out->weights = (const uint32_t *)b->wt.p + b->edge_base[job];
+  out->attacker_pos = (const uint8_t *)b->att.p + b->node_base[job];
+  return GEQ_OK;
+}
+
+extern "C" void geq_game_batch_stats(const geq_game_batch *b, geq_game_batch_info *out) {
+  if (!b || !out) return;
+  out->positions = b->N;
+  out->edges = b->M;
+  out->levels = b->levels;
+  out->kernel_launches = b->launches;
+  out->attempts = b->attempts;
+  out->upload_ms = b->upload_ms;
+  out->build_ms = b->build_ms;
+  out->download_ms = b->download_ms;
+}
+
+extern "C" void geq_game_batch_free(geq_game_batch *b) { delete b; }

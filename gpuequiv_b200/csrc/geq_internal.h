@@ -164,12 +164,25 @@ struct geq_device_games {
 
 namespace geq {
 
+// Games built on the device (device game builder) in the solver's input
+// layout: per game, positions in order with row offsets relative to the game,
+// successor ids local to the game.  Device pointers on the engine's stream.
+struct BuiltGames {
+  uint32_t n_games = 0;
+  const uint32_t *n_nodes = nullptr, *n_edges = nullptr;  // host, per game
+  unsigned long long N = 0, M = 0;
+  const uint32_t *row_rel = nullptr, *col = nullptr, *wt = nullptr;
+  const uint8_t *att = nullptr;
+};
+
 // Engine: owns the CUDA stream, events, pinned staging and the kernels.
 class Engine {
  public:
   static geq_status create(int device, std::unique_ptr<Engine> &out);
   ~Engine();
   geq_status upload(std::vector<GameInput> &games, GamesPtr &out);
+  // games already on the device (BuiltGames), standard reach
+  geq_status upload_built(const BuiltGames &b, GamesPtr &out);
   geq_status solve(DeviceGamesImpl &dg, geq_solve_stats *stats);
   // All positions of all games.
   geq_status download(DeviceGamesImpl &dg, geq_solution &sol);
@@ -197,6 +210,10 @@ class Engine {
                         geq_solve_stats *stats);
   // Node id of game g's first position inside the uploaded batch.
   static uint64_t game_node_base(const DeviceGamesImpl &dg, uint32_t g);
+  // The engine's CUDA stream (a cudaStream_t) and page-locked host pool, for
+  // the other device passes of the library (the device game builder).
+  void *stream_handle() const;
+  std::shared_ptr<HostPool> host_pool() const;
   geq_tuning tuning{};
   int n_sms = 0;
   uint64_t total_mem = 0;
@@ -204,7 +221,18 @@ class Engine {
 
   struct State;
   std::unique_ptr<State> st;
+
+ private:
+  geq_status alloc_work(DeviceGamesImpl &D, bool any_init);
+  geq_status finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out);
 };
+
+// GameBuild::compare (gamebuild.rs:165-170) of jobs (L[j], p[j], q[j]) built
+// by the device game builder and uploaded on eng's stream as standard-reach
+// games; the graphs never pass through the host.
+struct Lts;
+geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *p,
+                            const uint32_t *q, uint64_t max_positions, GamesPtr &out, double *build_ms);
 
 // A large batch split in two halves by positions on engines ea and eb: the
 // upload of the second half overlaps the solve of the first.

@@ -90,38 +90,40 @@ geq_status geq_compare_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *c
     if (!lts[i]) return fail(GEQ_ERR_INVALID_INPUT, "job %u: LTS is NULL", i);
     if (p[i] >= lts[i]->l.n || q[i] >= lts[i]->l.n) return fail(GEQ_ERR_INVALID_INPUT, "job %u: process out of range", i);
   }
-  // host: minimise and build every game (independent -> all host cores)
-  std::vector<GameBuilder> builders(n_jobs);
+  // host: minimise every LTS (independent -> all host cores); the games are
+  // then built on the device and solved there without leaving it
+  std::vector<Lts> reds(minimize ? n_jobs : 0);
+  std::vector<uint32_t> pm(n_jobs), qm(n_jobs);
   std::vector<uint8_t> trivial(n_jobs, 0);
   parallel_for(n_jobs, [&](uint32_t i) {
     const Lts &l = lts[i]->l;
     if (minimize) {
       std::vector<uint64_t> mapping;
-      Lts red;
-      l.minimize(mapping, red);
-      uint32_t pm = (uint32_t)mapping[p[i]], qm = (uint32_t)mapping[q[i]];
-      if (pm == qm) { trivial[i] = 1; return; }  // bisimilar: lib.rs:279-281
-      GameBuilder::compare(red, pm, qm, builders[i]);
+      l.minimize(mapping, reds[i]);
+      pm[i] = (uint32_t)mapping[p[i]];
+      qm[i] = (uint32_t)mapping[q[i]];
+      if (pm[i] == qm[i]) trivial[i] = 1;  // bisimilar: lib.rs:279-281
     } else {
-      GameBuilder::compare(l, p[i], q[i], builders[i]);
+      pm[i] = p[i];
+      qm[i] = q[i];
     }
   });
-  std::vector<GameInput> in;
-  std::vector<uint32_t> job_of;
+  std::vector<const Lts *> L;
+  std::vector<uint32_t> ps, qs;
   for (uint32_t i = 0; i < n_jobs; i++) {
     if (trivial[i]) continue;
-    in.push_back(input_of(builders[i]));
-    job_of.push_back(i);
+    L.push_back(minimize ? &reds[i] : &lts[i]->l);
+    ps.push_back(pm[i]);
+    qs.push_back(qm[i]);
   }
   std::unique_ptr<geq_solution> sol(new geq_solution());
   geq_solution part;
-  if (!in.empty()) {
-    // fix to_reach pointers after the vector settled
-    for (auto &gi : in) gi.to_reach = gi.reach_storage.data();
+  if (!L.empty()) {
     GamesPtr dg;
-    if ((st = e->upload(in, dg))) return st;
+    if ((st = build_and_upload(*e, ctx->device, (uint32_t)L.size(), L.data(), ps.data(), qs.data(), 0, dg, nullptr)))
+      return st;
     if ((st = e->solve(*dg, &sol->stats))) return st;
-    std::vector<uint32_t> first(in.size(), 0), count(in.size(), 1);
+    std::vector<uint32_t> first(L.size(), 0), count(L.size(), 1);
     if ((st = e->download_selected(*dg, first, count, part))) return st;
   }
   // assemble: one game of one position per job

@@ -7,7 +7,7 @@ from typing import Iterable, Sequence
 
 import numpy as np
 
-from ._lib import check, geq_game_graph, geq_position, lib
+from ._lib import check, geq_game_batch_info, geq_game_graph, geq_position, lib
 from .energy import Energy, EnergyArray, EnergyConf
 from .energygame import Context, GameGraph, _lists_from_solution, _stats_of, default_context
 
@@ -251,6 +251,57 @@ class GameBuild:
         check(lib.geq_game_build_compare_multiple(lts.h, _p(pr if pr.size else _Z32, _u32), len(pr), C.byref(h)))
         b = cls(h)
         return b, StartInfo(b.starting_points(), lts.n_vertices())
+
+
+class GameBatch:
+    """GameBuild::compare (gamebuild.rs:165-170) for many (lts, p, q) jobs,
+    built on the device one breadth-first level of all games at a time
+    (geq_game_build_compare_batch).  ``graph(j)`` is job j's GameGraph,
+    identical to ``GameBuild.compare(lts, p, q).game``; a job whose game
+    exceeds ``max_positions`` raises GeqError(OUT_OF_MEMORY) there, as
+    ``GameBuild.compare_bounded`` does."""
+
+    def __init__(self, jobs: Sequence[tuple[TransitionSystem, int, int]], context: Context | None = None,
+                 max_positions: int = 0):
+        ctx = context or default_context()
+        n = len(jobs)
+        hs = (C.c_void_p * max(n, 1))(*[j[0].h.value for j in jobs])
+        ps = np.array([j[1] for j in jobs] or [0], dtype=np.uint32)
+        qs = np.array([j[2] for j in jobs] or [0], dtype=np.uint32)
+        h = C.c_void_p()
+        check(lib.geq_game_build_compare_batch(ctx.h, n, hs, _p(ps, _u32), _p(qs, _u32), int(max_positions),
+                                               C.byref(h)))
+        self.h = h
+        info = geq_game_batch_info()
+        lib.geq_game_batch_stats(h, C.byref(info))
+        self.stats = info.as_dict()
+
+    def __len__(self):
+        return lib.geq_game_batch_n_jobs(self.h)
+
+    def view(self, j: int) -> geq_game_graph:
+        """Borrowed C view of job j's graph (valid while this object lives)."""
+        g = geq_game_graph()
+        check(lib.geq_game_batch_graph(self.h, int(j), C.byref(g)))
+        return g
+
+    def graph(self, j: int) -> GameGraph:
+        g = self.view(j)
+        n = g.n_vertices
+        row = np.ctypeslib.as_array(g.row_offsets, shape=(n + 1,)).copy()
+        m = int(row[-1])
+        col = np.ctypeslib.as_array(g.column_indices, shape=(m,)).copy() if m else np.zeros(0, np.uint32)
+        wt = np.ctypeslib.as_array(g.weights, shape=(m,)).copy() if m else np.zeros(0, np.uint32)
+        att = np.ctypeslib.as_array(g.attacker_pos, shape=(n,)).copy() if n else np.zeros(0, np.uint8)
+        return GameGraph.from_csr(row, col, wt.reshape(-1, 1), att, EnergyConf.STANDARD)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None) and self.h.value:
+                lib.geq_game_batch_free(self.h)
+                self.h = C.c_void_p()
+        except Exception:
+            pass
 
 
 # ---- Equivalence -------------------------------------------------------------

@@ -348,6 +348,31 @@ typedef struct geq_position {
 geq_status geq_game_build_position(const geq_game_build *b, uint32_t idx, geq_position *out);
 void geq_game_build_free(geq_game_build *b);
 
+/* ---- GameBuild on the device ----------------------------------------------
+ * GameBuild::compare (gamebuild.rs:165-170, successors gamepos.rs:17-198) for
+ * n_jobs (lts[j], p[j], q[j]) jobs at once, built on the context's device:
+ * every breadth-first level of all jobs' games is expanded by one group of
+ * kernels.  Each job's game is identical to geq_game_build_compare's (same
+ * position numbering, adjacency order and weights).  A job whose game would
+ * exceed max_positions positions (0 = no bound) is marked and its graph
+ * refused with GEQ_ERR_OUT_OF_MEMORY, as geq_game_build_compare_bounded does. */
+typedef struct geq_game_batch geq_game_batch;
+geq_status geq_game_build_compare_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts,
+                                        const uint32_t *p, const uint32_t *q, uint64_t max_positions,
+                                        geq_game_batch **out);
+uint32_t geq_game_batch_n_jobs(const geq_game_batch *b);
+/* Job's GameGraph (borrowed view, STANDARD conf). */
+geq_status geq_game_batch_graph(const geq_game_batch *b, uint32_t job, geq_game_graph *out);
+typedef struct geq_game_batch_info {
+  uint64_t positions, edges; /* all jobs */
+  uint32_t levels;           /* breadth-first levels of the deepest game */
+  uint32_t kernel_launches;
+  uint32_t attempts;         /* 1 unless a fingerprint collision forced a new hash seed */
+  double upload_ms, build_ms, download_ms; /* host wall time of each phase */
+} geq_game_batch_info;
+void geq_game_batch_stats(const geq_game_batch *b, geq_game_batch_info *out);
+void geq_game_batch_free(geq_game_batch *b);
+
 /* ---- whole algorithm (lib.rs:275-343, src/equivalence.rs) --------------- */
 /* TransitionSystem::compare (minimize != 0) / compare_unminimized: the
  * solution holds one game with a single position: the energies of the start
