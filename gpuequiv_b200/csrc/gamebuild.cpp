@@ -248,10 +248,11 @@ void GameBuilder::compare(const Lts &l, uint32_t p, uint32_t q, GameBuilder &out
   out.build(l);
 }
 
-// Start positions for every ordered pair inside each enabledness class
+// Start pairs for every ordered pair inside each enabledness class
 // (gamebuild.rs:104-133, :176-215).  Classes are visited in order of their
 // first process.
-void GameBuilder::compare_processes(const Lts &l, const uint32_t *procs, uint32_t n, GameBuilder &out) {
+void GameBuilder::start_pairs(const Lts &l, const uint32_t *procs, uint32_t n,
+                              std::vector<std::pair<uint32_t, uint32_t>> &out) {
   std::unordered_map<uint32_t, uint32_t> class_of_set;  // label-set id -> class index
   SetPool labelsets;
   std::vector<std::vector<uint32_t>> classes;
@@ -272,10 +273,17 @@ void GameBuilder::compare_processes(const Lts &l, const uint32_t *procs, uint32_
       classes[it->second].push_back(p);
     }
   }
+  out.clear();
   for (auto &c : classes)
     for (uint32_t p : c)
       for (uint32_t q : c)
-        if (p != q) out.new_node(PosKey{POS_ATTACK, p, out.sets.intern(&q, 1), 0});
+        if (p != q) out.emplace_back(p, q);
+}
+
+void GameBuilder::compare_processes(const Lts &l, const uint32_t *procs, uint32_t n, GameBuilder &out) {
+  std::vector<std::pair<uint32_t, uint32_t>> pairs;
+  start_pairs(l, procs, n, pairs);
+  for (auto &pq : pairs) out.new_node(PosKey{POS_ATTACK, pq.first, out.sets.intern(&pq.second, 1), 0});
   out.build(l);
 }
 

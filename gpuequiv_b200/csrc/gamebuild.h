@@ -49,6 +49,8 @@ struct GameBuilder {
   static void compare(const Lts &l, uint32_t p, uint32_t q, GameBuilder &out);
   static void compare_all(const Lts &l, GameBuilder &out);
   static void compare_processes(const Lts &l, const uint32_t *procs, uint32_t n, GameBuilder &out);
+  static void start_pairs(const Lts &l, const uint32_t *procs, uint32_t n,
+                          std::vector<std::pair<uint32_t, uint32_t>> &out);
 
  private:
   void grow();

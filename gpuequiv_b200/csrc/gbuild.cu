@@ -24,6 +24,13 @@ template <class F>
 __global__ void __launch_bounds__(EACH_T) k_each(uint32_t n, F f) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) f(i);
 }
+// the same with the count read on the device; nothing while *go == 0
+template <class F>
+__global__ void __launch_bounds__(EACH_T) k_each_d(const unsigned long long *np, const unsigned long long *go, F f) {
+  if (!*go) return;
+  const uint32_t n = (uint32_t)*np;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) f(i);
+}
 
 // exclusive scan of a block's values (one per thread); returns the block total
 __device__ __forceinline__ unsigned long long block_scan(unsigned long long x, unsigned long long &total) {
@@ -97,6 +104,303 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_down(const uint32_t *in, uint32
     }
 }
 
+// Three scans at once (the bounds of CountF), same tiling as above.
+struct Scan3 {
+  const uint32_t *in[3];
+  uint32_t *out[3];
+};
+__global__ void __launch_bounds__(SCAN_T) k_scan3_up(Scan3 a, uint32_t n, unsigned long long *part, uint32_t nb) {
+  const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    unsigned long long s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++)
+      if (base + k < n) s += a.in[r][base + k];
+    unsigned long long total;
+    block_scan(s, total);
+    if (threadIdx.x == 0) part[r * nb + blockIdx.x] = total;
+  }
+}
+__global__ void __launch_bounds__(SCAN_T) k_scan3_mid(unsigned long long *part, uint32_t nb, unsigned long long *tot) {
+  for (int r = 0; r < 3; r++) {
+    unsigned long long carry = 0;
+    for (uint32_t b0 = 0; b0 < nb; b0 += SCAN_T) {
+      const uint32_t i = b0 + threadIdx.x;
+      const unsigned long long x = i < nb ? part[r * nb + i] : 0ull;
+      unsigned long long total;
+      const unsigned long long e = block_scan(x, total);
+      if (i < nb) part[r * nb + i] = carry + e;
+      carry += total;
+    }
+    if (threadIdx.x == 0) tot[r] = carry;
+  }
+}
+__global__ void __launch_bounds__(SCAN_T) k_scan3_down(Scan3 a, uint32_t n, const unsigned long long *part,
+                                                       uint32_t nb) {
+  const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    uint32_t v[SCAN_ITEMS];
+    unsigned long long s = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+      v[k] = base + k < n ? a.in[r][base + k] : 0u;
+      s += v[k];
+    }
+    unsigned long long total;
+    unsigned long long e = block_scan(s, total) + part[r * nb + blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++)
+      if (base + k < n) {
+        a.out[r][base + k] = (uint32_t)e;
+        e += v[k];
+      }
+  }
+}
+
+// Scans of R arrays whose length is read on the device: a fixed grid of nb
+// blocks, block b scanning the contiguous chunk b of ceil(n / nb) values tile
+// by tile (reduce, scan of the nb block sums, rescan with the block's carry).
+template <int R>
+__global__ void __launch_bounds__(SCAN_T) k_cscan_up(Scan3 a, const unsigned long long *np, const unsigned long long *go,
+                                                     unsigned long long *part, uint32_t nb) {
+  if (!*go) return;
+  const uint32_t n = (uint32_t)*np, chunk = (n + nb - 1) / nb;
+  const uint32_t lo = min(n, blockIdx.x * chunk), hi = min(n, lo + chunk);
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    unsigned long long s = 0;
+    for (uint32_t base = lo + threadIdx.x * SCAN_ITEMS; base < hi; base += SCAN_TILE)
+#pragma unroll
+      for (int k = 0; k < SCAN_ITEMS; k++)
+        if (base + k < hi) s += a.in[r][base + k];
+    unsigned long long total;
+    block_scan(s, total);
+    if (threadIdx.x == 0) part[r * nb + blockIdx.x] = total;
+  }
+}
+template <int R>
+__global__ void __launch_bounds__(SCAN_T) k_cscan_mid(unsigned long long *part, uint32_t nb, unsigned long long *tot,
+                                                      const unsigned long long *go) {
+  if (!*go) return;
+  for (int r = 0; r < R; r++) {
+    unsigned long long carry = 0;
+    for (uint32_t b0 = 0; b0 < nb; b0 += SCAN_T) {
+      const uint32_t i = b0 + threadIdx.x;
+      const unsigned long long x = i < nb ? part[r * nb + i] : 0ull;
+      unsigned long long total;
+      const unsigned long long e = block_scan(x, total);
+      if (i < nb) part[r * nb + i] = carry + e;
+      carry += total;
+    }
+    if (threadIdx.x == 0) tot[r] = carry;
+  }
+}
+template <int R>
+__global__ void __launch_bounds__(SCAN_T) k_cscan_down(Scan3 a, const unsigned long long *np,
+                                                       const unsigned long long *go, const unsigned long long *part,
+                                                       uint32_t nb) {
+  if (!*go) return;
+  const uint32_t n = (uint32_t)*np, chunk = (n + nb - 1) / nb;
+  const uint32_t lo = min(n, blockIdx.x * chunk), hi = min(n, lo + chunk);
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    unsigned long long carry = part[r * nb + blockIdx.x];
+    for (uint32_t t0 = lo; t0 < hi; t0 += SCAN_TILE) {
+      const uint32_t base = t0 + threadIdx.x * SCAN_ITEMS;
+      uint32_t v[SCAN_ITEMS];
+      unsigned long long s = 0;
+#pragma unroll
+      for (int k = 0; k < SCAN_ITEMS; k++) {
+        v[k] = base + k < hi ? a.in[r][base + k] : 0u;
+        s += v[k];
+      }
+      unsigned long long total;
+      unsigned long long e = block_scan(s, total) + carry;
+#pragma unroll
+      for (int k = 0; k < SCAN_ITEMS; k++)
+        if (base + k < hi) {
+          a.out[r][base + k] = (uint32_t)e;
+          e += v[k];
+        }
+      carry += total;
+    }
+  }
+}
+
+// ---- the warp path for attack positions with many q's ------------------------
+// AttackPosition::successors (gamepos.rs:17-106) by one warp: each label's
+// union Q' is a bitmap over the job's states in shared memory (its set bits in
+// order are the sorted union), the observation moves and the enabledness
+// splits are placed by ballots in the reference's order.  Same output as
+// gen_one.
+constexpr int GH_WARPS = 8;
+constexpr uint32_t GH_BM_WORDS = 1024;  // jobs of up to 32768 states; larger ones: gen_one by lane 0
+constexpr uint32_t FULLMASK = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t lane_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ uint32_t warp_scan_incl(uint32_t x, uint32_t lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULLMASK, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  return x;
+}
+
+__device__ void gen_attack_warp(const View &v, uint32_t i, uint32_t *bm, uint32_t lane) {
+  const Key x = v.nkey[F0(v) + i];
+  const uint32_t j = v.sjob[x.p];
+  const uint32_t sb = v.jsb[j], nw = (v.jsb[j + 1] - sb + 31) / 32;
+  if (nw > GH_BM_WORDS) {
+    if (lane == 0) gen_one(v, i);
+    return;
+  }
+  const uint32_t s0 = v.off_s[i], ns = v.ub_s[i], c0 = v.off_c[i], nc = v.ub_c[i], e0 = v.off_e[i];
+  const uint32_t nq = v.slen[x.a];
+  const uint32_t *Q = v.sdata + v.sstart[x.a];
+  uint32_t *el = v.celem + e0;
+  uint32_t cnt = 0, cc = 0, ecur = 0;
+  uint32_t k = v.soff[x.p];
+  const uint32_t ke = v.soff[x.p + 1];
+  while (k < ke) {
+    const int32_t a = v.slab[k];
+    uint32_t run_end = k + 1;
+    while (run_end < ke && v.slab[run_end] == a) run_end++;
+    for (uint32_t w = lane; w < nw; w += 32) bm[w] = 0u;
+    __syncwarp();
+    for (uint32_t t = lane; t < nq; t += 32) {
+      const uint32_t q = Q[t];
+      for (uint32_t u = label_lower(v, q, a); u < v.soff[q + 1] && v.slab[u] == a; u++) {
+        const uint32_t s = v.stgt[u] - sb;
+        atomicOr(&bm[s >> 5], 1u << (s & 31));
+      }
+    }
+    __syncwarp();
+    uint32_t len = 0;
+    for (uint32_t w0 = 0; w0 < nw; w0 += 32) {
+      const uint32_t w = w0 + lane;
+      uint32_t bits = w < nw ? bm[w] : 0u;
+      const uint32_t c = __popc(bits);
+      const uint32_t incl = warp_scan_incl(c, lane);
+      uint32_t o = ecur + len + incl - c;
+      while (bits) {
+        el[o++] = sb + w * 32 + (uint32_t)(__ffs(bits) - 1);
+        bits &= bits - 1;
+      }
+      len += __shfl_sync(FULLMASK, incl, 31);
+    }
+    if (lane == 0) {
+      v.cstart[c0 + cc] = e0 + ecur;
+      v.clen[c0 + cc] = len;
+    }
+    const uint32_t qref = CAND | (c0 + cc);
+    cc++;
+    for (uint32_t kk = k; kk < run_end; kk += 32) {
+      const uint32_t idx = kk + lane;
+      bool keep = false;
+      uint32_t p2 = 0;
+      if (idx < run_end) {
+        p2 = v.stgt[idx];
+        const uint32_t s = p2 - sb;
+        keep = ((bm[s >> 5] >> (s & 31)) & 1u) == 0u;
+      }
+      const uint32_t bal = __ballot_sync(FULLMASK, keep);
+      if (keep) {
+        const uint32_t pos = s0 + cnt + __popc(bal & lane_lt());
+        v.succ[pos] = Key{K_ATTACK, p2, qref, 0};
+        v.swt[pos] = W_OBS;
+      }
+      cnt += __popc(bal);
+    }
+    ecur += len;
+    k = run_end;
+    __syncwarp();
+  }
+  if (lane == 0) {
+    v.succ[s0 + cnt] = Key{K_DEFEND, x.p, x.a, 0};
+    v.swt[s0 + cnt] = W_CHAL;
+  }
+  cnt++;
+  // enabledness splits: flags per q, then a stable partition per pair
+  uint32_t *b0 = el + ecur, *fl = el + ecur + 3 * nq;
+  uint32_t n1[3] = {0, 0, 0};
+  for (uint32_t t0 = 0; t0 < nq; t0 += 32) {
+    const uint32_t t = t0 + lane;
+    uint32_t f = 0;
+    if (t < nq) {
+      bool sub, sup;
+      compare_enabled(v, x.p, Q[t], sub, sup);
+      f = (sub ? 1u : 0u) | (sup ? 2u : 0u) | ((sub && sup) ? 4u : 0u);
+      fl[t] = f;
+    }
+#pragma unroll
+    for (int pr = 0; pr < 3; pr++) n1[pr] += __popc(__ballot_sync(FULLMASK, t < nq && ((f >> pr) & 1u)));
+  }
+  uint32_t r0[3] = {0, 0, 0}, r1[3] = {0, 0, 0};
+  for (uint32_t t0 = 0; t0 < nq; t0 += 32) {
+    const uint32_t t = t0 + lane;
+    const uint32_t f = t < nq ? fl[t] : 0u;
+    const uint32_t q = t < nq ? Q[t] : 0u;
+#pragma unroll
+    for (int pr = 0; pr < 3; pr++) {
+      const bool pass = ((f >> pr) & 1u) != 0u;
+      const uint32_t bp = __ballot_sync(FULLMASK, t < nq && pass), bf = __ballot_sync(FULLMASK, t < nq && !pass);
+      uint32_t *b = b0 + (uint32_t)pr * nq;
+      if (t < nq) {
+        if (pass) b[nq - n1[pr] + r1[pr] + __popc(bp & lane_lt())] = q;
+        else b[r0[pr] + __popc(bf & lane_lt())] = q;
+      }
+      r0[pr] += __popc(bf);
+      r1[pr] += __popc(bp);
+    }
+  }
+  __syncwarp();
+  uint32_t pushed[3];
+  uint32_t np = 0;
+  for (uint32_t pr = 0; pr < 3; pr++) {
+    const uint32_t nqx = n1[pr], nqs = nq - nqx;
+    if (nqs == 0 || nqx == 0) continue;
+    bool dup = false;  // push_unique: an equal split was pushed already
+    for (uint32_t o = 0; o < np && !dup; o++) {
+      const uint32_t po = pushed[o];
+      if (n1[po] != nqx) continue;
+      bool diff = false;
+      for (uint32_t t = lane; t < nq; t += 32) diff |= b0[po * nq + t] != b0[pr * nq + t];
+      dup = !__any_sync(FULLMASK, diff);
+    }
+    if (dup) continue;
+    if (lane == 0) {
+      v.cstart[c0 + cc] = e0 + ecur + pr * nq;
+      v.clen[c0 + cc] = nqs;
+      v.cstart[c0 + cc + 1] = e0 + ecur + pr * nq + nqs;
+      v.clen[c0 + cc + 1] = nqx;
+      v.succ[s0 + cnt] = Key{K_DEFEND, x.p, CAND | (c0 + cc), CAND | (c0 + cc + 1)};
+      v.swt[s0 + cnt] = W_CHAL;
+    }
+    cc += 2;
+    cnt++;
+    pushed[np++] = pr;
+  }
+  for (uint32_t t = cnt + lane; t < ns; t += 32) v.succ[s0 + t] = Key{K_NONE, 0, 0, 0};
+  for (uint32_t t = cc + lane; t < nc; t += 32) v.clen[c0 + t] = UNSET;
+  if (lane == 0) v.fcnt[i] = cnt;
+}
+
+__global__ void __launch_bounds__(GH_WARPS * 32) k_gen_heavy(View v, const unsigned long long *go) {
+  __shared__ uint32_t bm_all[GH_WARPS][GH_BM_WORDS];
+  if (go && !*go) return;
+  const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const uint32_t nh = v.ctl->n_heavy;
+  for (uint32_t h = blockIdx.x * GH_WARPS + wib; h < nh; h += gridDim.x * GH_WARPS)
+    gen_attack_warp(v, v.hq[h], bm_all[wib], lane);
+}
+
 // Backend of the level loop: stream-ordered allocation, kernels and copies on
 // the context's stream.
 struct DevBackend {
@@ -158,7 +462,97 @@ struct DevBackend {
     k_scan_down<<<nb, SCAN_T, 0, s>>>(in, n, part, out);
     launches += 3;
   }
+  void scan3(const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, uint32_t *o0, uint32_t *o1, uint32_t *o2,
+             uint32_t n, unsigned long long *tot) {
+    const uint32_t nb = std::max<uint32_t>(1, (n + SCAN_TILE - 1) / SCAN_TILE);
+    if (3 * nb > part_cap) {
+      release(part);
+      part_cap = std::max<uint32_t>(3 * nb, 1024);
+      part = (unsigned long long *)alloc((size_t)part_cap * 8);
+      if (!part) {
+        part_cap = 0;
+        note(cudaErrorMemoryAllocation);
+        return;
+      }
+    }
+    const Scan3 a{{i0, i1, i2}, {o0, o1, o2}};
+    k_scan3_up<<<nb, SCAN_T, 0, s>>>(a, n, part, nb);
+    k_scan3_mid<<<1, SCAN_T, 0, s>>>(part, nb, tot);
+    k_scan3_down<<<nb, SCAN_T, 0, s>>>(a, n, part, nb);
+    launches += 3;
+  }
+  void gen_heavy(const View &v, const unsigned long long *go) {
+    if (v.heavy_min == 0xffffffffu) return;
+    k_gen_heavy<<<(unsigned)n_sms * 2, GH_WARPS * 32, 0, s>>>(v, go);
+    launches++;
+  }
+  // ---- device-counted launches (the level loop) ----
+  uint32_t grid_for(uint32_t cap) const {
+    return std::max<uint32_t>(1, std::min<uint32_t>((cap + EACH_T - 1) / EACH_T, (uint32_t)n_sms * 8));
+  }
+  template <class F>
+  void each_d(const unsigned long long *np, uint32_t cap, const unsigned long long *go, const F &f) {
+    k_each_d<<<grid_for(cap), EACH_T, 0, s>>>(np, go, f);
+    launches++;
+  }
+  uint32_t cnb() const { return (uint32_t)n_sms * 2; }
+  bool reserve_part() {
+    if (part_cap >= 3 * cnb()) return true;
+    release(part);
+    part_cap = std::max<uint32_t>(3 * cnb(), 1024);
+    part = (unsigned long long *)alloc((size_t)part_cap * 8);
+    if (!part) {
+      part_cap = 0;
+      note(cudaErrorMemoryAllocation);
+      return false;
+    }
+    return true;
+  }
+  void scan_d(const uint32_t *in, uint32_t *out, const unsigned long long *np, unsigned long long *tot,
+              const unsigned long long *go) {
+    const Scan3 a{{in, in, in}, {out, out, out}};
+    k_cscan_up<1><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
+    k_cscan_mid<1><<<1, SCAN_T, 0, s>>>(part, cnb(), tot, go);
+    k_cscan_down<1><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
+    launches += 3;
+  }
+  void scan3_d(const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, uint32_t *o0, uint32_t *o1, uint32_t *o2,
+               const unsigned long long *np, unsigned long long *tot, const unsigned long long *go) {
+    const Scan3 a{{i0, i1, i2}, {o0, o1, o2}};
+    k_cscan_up<3><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
+    k_cscan_mid<3><<<1, SCAN_T, 0, s>>>(part, cnb(), tot, go);
+    k_cscan_down<3><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
+    launches += 3;
+  }
+  // ---- one level recorded as a CUDA graph ----
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  uint32_t graph_launches = 0, mark = 0;
+  bool has_graph() const { return gexec != nullptr; }
+  void begin_capture() {
+    reserve_part();
+    mark = launches;
+    note(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  }
+  void end_capture() {
+    note(cudaStreamEndCapture(s, &graph));
+    graph_launches = launches - mark;
+    launches = mark;
+    if (err == cudaSuccess) note(cudaGraphInstantiate(&gexec, graph, 0));
+  }
+  void run_graph() {
+    if (!gexec) return;
+    note(cudaGraphLaunch(gexec, s));
+    launches += graph_launches;
+  }
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    gexec = nullptr;
+    graph = nullptr;
+  }
   ~DevBackend() {
+    drop_graph();
     if (part) cudaFreeAsync(part, s);
   }
 };
@@ -184,16 +578,19 @@ struct DeviceBuild {
   }
 };
 
-static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *p,
-                               const uint32_t *q, uint64_t max_positions, DeviceBuild &db) {
+// Job j starts from Attack(p[t], {q[t]}) for t in start_off[j] .. start_off[j+1]-1
+// (local process ids of L[j]), in that order.
+static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L,
+                               const uint32_t *start_off, const uint32_t *p, const uint32_t *q,
+                               uint64_t max_positions, DeviceBuild &db) {
   using clk = std::chrono::steady_clock;
   std::vector<uint64_t> sb(n_jobs + 1, 0), tb(n_jobs + 1, 0);
   for (uint32_t j = 0; j < n_jobs; j++) {
     sb[j + 1] = sb[j] + L[j]->n;
     tb[j + 1] = tb[j] + L[j]->n_transitions();
   }
-  const uint64_t NS = sb[n_jobs], MS = tb[n_jobs];
-  if (NS >= (1ull << 31) || MS >= (1ull << 32) - 1)
+  const uint64_t NS = sb[n_jobs], MS = tb[n_jobs], T = start_off[n_jobs];
+  if (NS >= (1ull << 31) || MS >= (1ull << 32) - 1 || T >= (1ull << 30))
     return fail(GEQ_ERR_INVALID_INPUT, "batch too large: %llu states, %llu transitions", (unsigned long long)NS,
                 (unsigned long long)MS);
   const uint32_t max_pos = max_positions >= (1ull << 31) ? 0u : (uint32_t)max_positions;
@@ -220,7 +617,8 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
   // stage the LTSs: soff | slab | stgt | sjob | p0 | q0
   const auto t0 = clk::now();
   const size_t o_soff = 0, o_slab = o_soff + (NS + 1) * 4, o_stgt = o_slab + MS * 4, o_sjob = o_stgt + MS * 4,
-               o_p0 = o_sjob + NS * 4, o_q0 = o_p0 + (size_t)n_jobs * 4, bytes = o_q0 + (size_t)n_jobs * 4;
+               o_p0 = o_sjob + NS * 4, o_q0 = o_p0 + (size_t)T * 4, o_jsb = o_q0 + (size_t)T * 4,
+               bytes = o_jsb + ((size_t)n_jobs + 1) * 4;
   if (!db.stage.alloc(eng.host_pool(), bytes)) return fail(GEQ_ERR_OUT_OF_MEMORY, "staging %zu bytes", bytes);
   char *hs = (char *)db.stage.p;
   parallel_for(n_jobs, [&](uint32_t j) {
@@ -238,10 +636,14 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
       slab[k] = l.lab_[k];
       stgt[k] = (uint32_t)(sb[j] + l.tgt[k]);
     }
-    ((uint32_t *)(hs + o_p0))[j] = (uint32_t)(sb[j] + p[j]);
-    ((uint32_t *)(hs + o_q0))[j] = (uint32_t)(sb[j] + q[j]);
+    for (uint32_t t = start_off[j]; t < start_off[j + 1]; t++) {
+      ((uint32_t *)(hs + o_p0))[t] = (uint32_t)(sb[j] + p[t]);
+      ((uint32_t *)(hs + o_q0))[t] = (uint32_t)(sb[j] + q[t]);
+    }
+    ((uint32_t *)(hs + o_jsb))[j] = (uint32_t)sb[j];
   });
   ((uint32_t *)(hs + o_soff))[NS] = (uint32_t)MS;
+  ((uint32_t *)(hs + o_jsb))[n_jobs] = (uint32_t)NS;
   db.din = (char *)be.alloc(bytes);
   if (!db.din) return fail(GEQ_ERR_OUT_OF_MEMORY, "device input %zu bytes", bytes);
   be.copy(db.din, hs, bytes);
@@ -249,13 +651,17 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
   in.NS = (uint32_t)NS;
   in.MS = (uint32_t)MS;
   in.n_jobs = n_jobs;
+  in.n_starts = (uint32_t)T;
   in.soff = (const uint32_t *)(db.din + o_soff);
   in.slab = (const int32_t *)(db.din + o_slab);
   in.stgt = (const uint32_t *)(db.din + o_stgt);
   in.sjob = (const uint32_t *)(db.din + o_sjob);
   in.p0 = (const uint32_t *)(db.din + o_p0);
   in.q0 = (const uint32_t *)(db.din + o_q0);
+  in.jsb = (const uint32_t *)(db.din + o_jsb);
   in.max_pos = max_pos;
+  // attack positions with at least this many q's take the warp path
+  in.heavy_min = (eng.tuning.flags & GEQ_TUNE_BUILD_WARP_ALL) ? 1u : 8u;
   const auto t1 = clk::now();
   db.b.reset(new gb::Builder<gb::DevBackend>(be));
   const int rc = db.b->run(in, db.r);
@@ -271,10 +677,11 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
 // GameBuild::compare of every job on the device, handed to the solver as an
 // upload (the graphs never leave the device).  jobs whose game exceeds
 // max_positions (0 = no bound) fail with GEQ_ERR_OUT_OF_MEMORY.
-geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *p,
-                            const uint32_t *q, uint64_t max_positions, GamesPtr &out, double *build_ms) {
+geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *start_off,
+                            const uint32_t *p, const uint32_t *q, uint64_t max_positions, GamesPtr &out,
+                            double *build_ms) {
   DeviceBuild db;
-  geq_status st = device_build(eng, device, n_jobs, L, p, q, max_positions, db);
+  geq_status st = device_build(eng, device, n_jobs, L, start_off, p, q, max_positions, db);
   if (st) return st;
   std::vector<uint32_t> jcount(n_jobs), jm(n_jobs), jover(n_jobs);
   db.be.copy(jcount.data(), db.r.jcount, (size_t)n_jobs * 4);
@@ -330,7 +737,9 @@ extern "C" geq_status geq_game_build_compare_batch(geq_context *ctx, uint32_t n_
   std::unique_ptr<geq_game_batch> res(new geq_game_batch());
   res->n_jobs = n_jobs;
   DeviceBuild db;
-  geq_status st = device_build(eng, ctx->device, n_jobs, L.data(), p, q, max_positions, db);
+  std::vector<uint32_t> start_off(n_jobs + 1);
+  for (uint32_t j = 0; j <= n_jobs; j++) start_off[j] = j;
+  geq_status st = device_build(eng, ctx->device, n_jobs, L.data(), start_off.data(), p, q, max_positions, db);
   if (st) return st;
   // per-job CSR back to the host
   const auto t2 = clk::now();

@@ -28,6 +28,7 @@
 #define __host__
 #define __device__
 #define __forceinline__ inline
+#define __align__(n) alignas(n)
 #endif
 
 namespace geq {
@@ -46,7 +47,7 @@ constexpr uint32_t W_ANS = 4u << 12;                     // [0, 0, 0, Min(3)]
 constexpr uint32_t W_CL1 = 5u;                           // [Min(4)]
 constexpr uint32_t W_CL2 = 6u | (1u << 20);              // [Min(5), 0, 0, 0, 0, -1]
 
-struct Key {
+struct __align__(16) Key {
   uint32_t kind, p, a, b;
 };
 __host__ __device__ __forceinline__ bool key_eq(const Key &x, const Key &y) {
@@ -108,12 +109,32 @@ __host__ __device__ __forceinline__ unsigned long long key_hash(const Key &k, un
   return h ? h : 1ull;
 }
 
+// Counts of the level loop, kept on the device (Totals::t) so that levels
+// run without the host: kernels take their item counts from here.
+enum : int {
+  T_NEW = 0,     // new positions of the level
+  T_S = 1,       // successor slots (upper bound), set words, candidate sets: three in a row
+  T_E = 2,
+  T_C = 3,
+  T_EDGE = 4,    // edges of the level
+  T_N = 5,       // positions of all jobs (final)
+  T_F0 = 6,      // first frontier position
+  T_F = 7,       // frontier size
+  T_NN = 8,      // positions so far
+  T_NE = 9,      // edges so far
+  T_GO = 10,     // 1 while levels may run
+  T_STALL = 11,  // a level stopped for a buffer to grow
+  T_DONE = 12,   // the frontier ran empty
+  T_LEVELS = 13, // levels completed
+  T_COUNT = 16
+};
+
 // Control block on the device.
 struct Ctl {
   uint32_t err;
   uint32_t n_sets;     // interned sets
   uint32_t sdata_top;  // words of set contents
-  uint32_t pad;
+  uint32_t n_heavy;    // this level's attack positions for the warp path
 };
 
 // Every array of a build.  Rebuilt by the host whenever a buffer grows.
@@ -123,6 +144,7 @@ struct View {
   const int32_t *slab;
   const uint32_t *stgt;
   const uint32_t *sjob;  // job of each state
+  const uint32_t *jsb;   // n_jobs + 1: first state of each job
   // interned sets
   uint32_t *sdata, *sstart, *slen;
   uint32_t sdata_cap, sets_cap;
@@ -138,20 +160,22 @@ struct View {
   uint32_t nmask;
   // per job
   uint32_t *jcount, *jfirst, *jover;
-  // level scratch: frontier f0 .. f0+F-1
-  uint32_t f0, F;
+  // level scratch: frontier positions t[T_F0] .. t[T_F0]+t[T_F]-1
+  unsigned long long *t;            // Totals::t on the device
+  uint32_t capF, capS, capE, capC;  // scratch capacities (the level gate checks them)
+  uint32_t scap, ncap;              // hash table sizes
   uint32_t *ub_s, *ub_e, *ub_c;     // upper bounds: successor slots, set words, candidate sets
   uint32_t *off_s, *off_e, *off_c;  // their exclusive scans
   uint32_t *fcnt, *feoff;           // exact successor counts, their scan
+  uint32_t *hq;                     // frontier indices taken by the warp path
+  uint32_t heavy_min;               // |Q| from which an attack position takes the warp path
   Key *succ;
   uint32_t *swt, *sslot, *sres, *snew, *srank;
-  uint32_t S;
   uint32_t *celem, *cstart, *clen, *cslot, *cid;
-  uint32_t C, E;
   // edges in discovery order of their source
   uint32_t *ecol, *ewt;
-  uint32_t n_nodes, n_edges, edges_cap;
-  // start positions: Attack(p0[j], {q0[j]})
+  uint32_t edges_cap;
+  // start positions: Attack(p0[t], {q0[t]}), job-major
   const uint32_t *p0, *q0;
   uint32_t n_jobs;
   uint32_t max_pos;  // 0 = unbounded
@@ -160,6 +184,9 @@ struct View {
 };
 
 __host__ __device__ __forceinline__ uint32_t deg(const View &v, uint32_t s) { return v.soff[s + 1] - v.soff[s]; }
+__host__ __device__ __forceinline__ uint32_t F0(const View &v) { return (uint32_t)v.t[T_F0]; }
+__host__ __device__ __forceinline__ uint32_t NN(const View &v) { return (uint32_t)v.t[T_NN]; }
+__host__ __device__ __forceinline__ uint32_t NE(const View &v) { return (uint32_t)v.t[T_NE]; }
 
 // TransitionSystem::compare_enabled (gamebuild.rs:23-98): (enabled(p) ⊆
 // enabled(q), enabled(p) ⊇ enabled(q)), rows being label-sorted.
@@ -243,7 +270,7 @@ struct StartF {
 struct CountF {
   View v;
   __host__ __device__ void operator()(uint32_t i) const {
-    const Key x = v.nkey[v.f0 + i];
+    const Key x = v.nkey[F0(v) + i];
     uint32_t s = 0, e = 0, c = 0;
     if (!v.jover[v.sjob[x.p]]) {
       if (x.kind == K_ATTACK) {
@@ -256,7 +283,8 @@ struct CountF {
           c = d + 6;
           const uint32_t *Q = v.sdata + v.sstart[x.a];
           for (uint32_t k = 0; k < nq; k++) e += deg(v, Q[k]);
-          e += 3 * nq;
+          e += 4 * nq;  // unions, three split pairs, one word of flags per q (warp path)
+          if (nq >= v.heavy_min) v.hq[at_add(&v.ctl->n_heavy, 1u)] = i;
         }
       } else if (x.kind == K_CLAUSE) {
         s = 2; e = 2; c = 2;
@@ -271,10 +299,9 @@ struct CountF {
 };
 
 // ---- per frontier position: its successors (Position::successors) ----------
-struct GenF {
-  View v;
-  __host__ __device__ void operator()(uint32_t i) const {
-    const Key x = v.nkey[v.f0 + i];
+__host__ __device__ inline void gen_one(const View &v, uint32_t i) {
+  {
+    const Key x = v.nkey[F0(v) + i];
     const uint32_t s0 = v.off_s[i], ns = v.ub_s[i];
     const uint32_t c0 = v.off_c[i], nc = v.ub_c[i];
     const uint32_t e0 = v.off_e[i];
@@ -388,6 +415,19 @@ struct GenF {
     for (uint32_t t = cnt; t < ns; t++) v.succ[s0 + t] = Key{K_NONE, 0, 0, 0};
     for (uint32_t t = cc; t < nc; t++) v.clen[c0 + t] = UNSET;
     v.fcnt[i] = cnt;
+  }
+}
+// whether frontier position i was queued for the warp path by CountF
+__host__ __device__ __forceinline__ bool is_heavy(const View &v, uint32_t i) {
+  const Key x = v.nkey[F0(v) + i];
+  if (x.kind != K_ATTACK || v.jover[v.sjob[x.p]]) return false;
+  const uint32_t nq = v.slen[x.a];
+  return nq != 0 && nq >= v.heavy_min;
+}
+struct GenF {
+  View v;
+  __host__ __device__ void operator()(uint32_t i) const {
+    if (!is_heavy(v, i)) gen_one(v, i);
   }
 };
 
@@ -506,7 +546,7 @@ struct SuccNewF {
   View v;
   __host__ __device__ void operator()(uint32_t s) const {
     if (!v.snew[s]) return;
-    const uint32_t id = v.n_nodes + v.srank[s];
+    const uint32_t id = NN(v) + v.srank[s];
     if (id >= v.nodes_cap) {
       at_or(&v.ctl->err, ERR_RANGE);
       return;
@@ -531,8 +571,8 @@ struct SuccFillF {
 struct EdgeF {
   View v;
   __host__ __device__ void operator()(uint32_t i) const {
-    const uint32_t g = v.f0 + i, n = v.fcnt[i];
-    const unsigned long long e = (unsigned long long)v.n_edges + v.feoff[i];
+    const uint32_t g = F0(v) + i, n = v.fcnt[i];
+    const unsigned long long e = (unsigned long long)NE(v) + v.feoff[i];
     v.nrow[g] = n;
     v.neoff[g] = (uint32_t)e;
     if (e + n > v.edges_cap) {
@@ -552,22 +592,22 @@ struct EdgeF {
 struct LocalAF {
   View v;
   __host__ __device__ void operator()(uint32_t i) const {
-    const uint32_t g = v.n_nodes + i, j = v.sjob[v.nkey[g].p];
+    const uint32_t g = NN(v) + i, j = v.sjob[v.nkey[g].p];
     if (i == 0 || v.sjob[v.nkey[g - 1].p] != j) v.jfirst[j] = g;
   }
 };
 struct LocalBF {
   View v;
   __host__ __device__ void operator()(uint32_t i) const {
-    const uint32_t g = v.n_nodes + i, j = v.sjob[v.nkey[g].p];
+    const uint32_t g = NN(v) + i, j = v.sjob[v.nkey[g].p];
     v.nlocal[g] = v.jcount[j] + (g - v.jfirst[j]);
   }
 };
 struct LocalCF {
   View v;
-  uint32_t cnt;
   __host__ __device__ void operator()(uint32_t i) const {
-    const uint32_t g = v.n_nodes + i, j = v.sjob[v.nkey[g].p];
+    const uint32_t cnt = (uint32_t)v.t[T_NEW];
+    const uint32_t g = NN(v) + i, j = v.sjob[v.nkey[g].p];
     if (i + 1 == cnt || v.sjob[v.nkey[g + 1].p] != j) {
       v.jcount[j] = v.nlocal[g] + 1;
       if (v.max_pos && v.jcount[j] > v.max_pos) v.jover[j] = 1;
@@ -648,12 +688,61 @@ struct RowEndF {
   View v;
   Out o;
   __host__ __device__ void operator()(uint32_t j) const {
-    const uint32_t end = (j + 1 < v.n_jobs) ? o.frow[o.jbase[j + 1]] : v.n_edges;
-    o.row[o.jbase[j] + j + v.jcount[j]] = end - o.frow[o.jbase[j]];
-    o.jm[j] = end - o.frow[o.jbase[j]];
+    // a job without positions (no start pairs) has an empty graph
+    const uint32_t last = o.jbase[j] + v.jcount[j];
+    const uint32_t end = last < NN(v) ? o.frow[last] : NE(v);
+    const uint32_t begin = v.jcount[j] ? o.frow[o.jbase[j]] : end;
+    o.row[o.jbase[j] + j + v.jcount[j]] = end - begin;
+    o.jm[j] = end - begin;
   }
 };
 
+// ---- level bookkeeping on the device (one thread each) ---------------------------
+// Start of a level: done when the frontier is empty; a frontier beyond the
+// scratch capacity stalls the loop until the host has grown the buffers.
+struct LevelStartF {
+  View v;
+  __host__ __device__ void operator()(uint32_t) const {
+    if (!v.t[T_GO]) return;
+    v.ctl->n_heavy = 0;
+    if (v.t[T_F] == 0) {
+      v.t[T_GO] = 0;
+      v.t[T_DONE] = 1;
+    } else if (v.t[T_F] > v.capF) {
+      v.t[T_GO] = 0;
+      v.t[T_STALL] = 1;
+    }
+  }
+};
+// After the bounds' scans and before anything persistent is written: every
+// buffer and table must hold this level, else the level stalls (and is run
+// again after the host grew them).
+struct LevelGateF {
+  View v;
+  __host__ __device__ void operator()(uint32_t) const {
+    if (!v.t[T_GO]) return;
+    const unsigned long long S = v.t[T_S], E = v.t[T_E], C = v.t[T_C], nn = v.t[T_NN], ne = v.t[T_NE];
+    const unsigned long long ns = v.ctl->n_sets, top = v.ctl->sdata_top;
+    const bool fits = S < (1ull << 31) && E < (1ull << 31) && C < (1ull << 31) && S <= v.capS && E <= v.capE &&
+                      C <= v.capC && ns + C <= v.sets_cap && top + E <= v.sdata_cap && 2 * (ns + C) <= v.scap &&
+                      nn + S <= v.nodes_cap && 2 * (nn + S) <= v.ncap && ne + S <= v.edges_cap;
+    if (!fits) {
+      v.t[T_GO] = 0;
+      v.t[T_STALL] = 1;
+    }
+  }
+};
+struct LevelEndF {
+  View v;
+  __host__ __device__ void operator()(uint32_t) const {
+    if (!v.t[T_GO]) return;
+    v.t[T_NN] += v.t[T_NEW];
+    v.t[T_NE] += v.t[T_EDGE];
+    v.t[T_F0] += v.t[T_F];
+    v.t[T_F] = v.t[T_NEW];
+    v.t[T_LEVELS] += 1;
+  }
+};
 
 // ---- the level loop ------------------------------------------------------------
 // Host-side driver over a backend B with
@@ -662,12 +751,17 @@ struct RowEndF {
 //   void fetch(void *host, const void *dev, size_t);      (waits)
 //   template <class F> void each(uint32_t n, const F &);
 //   void scan(const uint32_t *in, uint32_t *out, uint32_t n, unsigned long long *dev_total);
+//   void scan3(in0, in1, in2, out0, out1, out2, n, dev_totals[3]);  (three scans at once)
+//   void gen_heavy(const View &, const unsigned long long *go);  (the positions CountF queued in v.hq)
+//   each_d / scan_d / scan3_d: the same with the item count read on the device
+//     (*n), doing nothing while *go == 0 (a stalled or finished loop);
+//   begin_capture / end_capture / run_graph / has_graph / drop_graph: one
+//     level recorded once and replayed (a CUDA graph on the device).
 //   bool ok();                                             (no backend error so far)
 struct Totals {
   Ctl ctl;
-  unsigned long long t[6];
+  unsigned long long t[T_COUNT];
 };
-enum : int { T_NEW = 0, T_S = 1, T_E = 2, T_C = 3, T_EDGE = 4, T_N = 5 };
 
 // Inputs: all jobs' LTSs in one id space (states of job j contiguous).
 struct Input {
@@ -676,8 +770,11 @@ struct Input {
   const int32_t *slab = nullptr;   // MS
   const uint32_t *stgt = nullptr;  // MS, global ids
   const uint32_t *sjob = nullptr;  // NS
-  const uint32_t *p0 = nullptr, *q0 = nullptr;  // n_jobs, global ids
+  uint32_t n_starts = 0;                         // start positions, job-major
+  const uint32_t *p0 = nullptr, *q0 = nullptr;  // n_starts, global ids
+  const uint32_t *jsb = nullptr;                 // n_jobs + 1: first state of each job
   uint32_t max_pos = 0;
+  uint32_t heavy_min = 0xffffffffu;              // |Q| from which the warp path takes an attack position
 };
 // Output, in backend memory until fetched: per job j, positions
 // jbase[j] .. jbase[j]+jcount[j]-1 and row offsets at row[jbase[j]+j ..].
@@ -770,6 +867,7 @@ class Builder {
     c = capF_; ok = ok && grow(v_.off_c, c, F, 0);
     c = capF_; ok = ok && grow(v_.fcnt, c, F, 0);
     c = capF_; ok = ok && grow(v_.feoff, c, F, 0);
+    c = capF_; ok = ok && grow(v_.hq, c, F, 0);
     capF_ = c;
     return ok;
   }
@@ -859,39 +957,53 @@ class Builder {
     v_.nodes_cap = capNodes_;
     v_.nmask = ncap_ ? ncap_ - 1 : 0;
     v_.edges_cap = capEdges_;
+    v_.capF = capF_;
+    v_.capS = capS_;
+    v_.capE = capE_;
+    v_.capC = capC_;
+    v_.scap = scap_;
+    v_.ncap = ncap_;
+    v_.t = d_tot_ ? d_tot_->t : nullptr;
   }
-  // intern the level's candidate sets and successors; returns false on failure
-  bool intern(uint32_t S, uint32_t C) {
-    sync_view();
-    v_.S = S;
-    v_.C = C;
-    be_.each(C, SetProbeF{v_});
-    be_.each(C, SetNewF{v_});
-    be_.each(C, SetFillF{v_});
-    be_.each(S, SuccProbeF{v_});
-    be_.each(S, SuccFlagF{v_});
-    be_.scan(v_.snew, v_.srank, S, &d_tot_->t[T_NEW]);
-    return true;
-  }
-  void number_new(uint32_t S) {
-    be_.each(S, SuccNewF{v_});
-    be_.each(S, SuccFillF{v_});
-  }
-  void local_ids(uint32_t cnt) {
-    be_.each(cnt, LocalAF{v_});
-    be_.each(cnt, LocalBF{v_});
-    be_.each(cnt, LocalCF{v_, cnt});
+  const unsigned long long *tp(int k) const { return &d_tot_->t[k]; }
+  // One breadth-first level, every count read on the device (no host sync):
+  // bounds, gate, successors, interning, numbering, edges, local ids.
+  void enqueue_level() {
+    const unsigned long long *go = tp(T_GO);
+    be_.each(1, LevelStartF{v_});
+    be_.each_d(tp(T_F), capF_, go, CountF{v_});
+    be_.scan3_d(v_.ub_s, v_.ub_e, v_.ub_c, v_.off_s, v_.off_e, v_.off_c, tp(T_F), &d_tot_->t[T_S], go);
+    be_.each(1, LevelGateF{v_});
+    be_.each_d(tp(T_F), capF_, go, GenF{v_});
+    be_.gen_heavy(v_, go);
+    be_.each_d(tp(T_C), capC_, go, SetProbeF{v_});
+    be_.each_d(tp(T_C), capC_, go, SetNewF{v_});
+    be_.each_d(tp(T_C), capC_, go, SetFillF{v_});
+    be_.each_d(tp(T_S), capS_, go, SuccProbeF{v_});
+    be_.each_d(tp(T_S), capS_, go, SuccFlagF{v_});
+    be_.scan_d(v_.snew, v_.srank, tp(T_S), &d_tot_->t[T_NEW], go);
+    be_.scan_d(v_.fcnt, v_.feoff, tp(T_F), &d_tot_->t[T_EDGE], go);
+    be_.each_d(tp(T_S), capS_, go, SuccNewF{v_});
+    be_.each_d(tp(T_S), capS_, go, SuccFillF{v_});
+    be_.each_d(tp(T_F), capF_, go, EdgeF{v_});
+    be_.each_d(tp(T_NEW), capS_, go, LocalAF{v_});
+    be_.each_d(tp(T_NEW), capS_, go, LocalBF{v_});
+    be_.each_d(tp(T_NEW), capS_, go, LocalCF{v_});
+    be_.each(1, LevelEndF{v_});
   }
 
   int attempt_build(const Input &in, unsigned long long seed, Result &out) {
     v_ = View{};
     capF_ = capS_ = capE_ = capC_ = capNew_ = capSets_ = capSdata_ = capNodes_ = capEdges_ = scap_ = ncap_ = 0;
+    be_.drop_graph();
     v_.soff = in.soff;
     v_.slab = in.slab;
     v_.stgt = in.stgt;
     v_.sjob = in.sjob;
     v_.p0 = in.p0;
     v_.q0 = in.q0;
+    v_.jsb = in.jsb;
+    v_.heavy_min = in.heavy_min;
     v_.n_jobs = in.n_jobs;
     v_.max_pos = in.max_pos;
     v_.seed = seed;
@@ -906,79 +1018,91 @@ class Builder {
     be_.fill(v_.jover, 0, (size_t)J * 4);
     v_.ctl = &d_tot_->ctl;
     // the empty set is set 0
-    if (!ensure_sets(0, 0, (uint64_t)J + 1, (uint64_t)J + 1)) return 1;
+    if (!ensure_sets(0, 0, (uint64_t)in.n_starts + 1, (uint64_t)in.n_starts + 1)) return 1;
     {
       const uint32_t zero = 0;
-      const unsigned long long h = set_hash(nullptr, 0, seed);
-      // set 0: no words; stored by a one-item kernel so the table agrees
       Ctl c0{0, 1, 0, 0};
       be_.copy(v_.sstart, &zero, 4);
       be_.copy(v_.slen, &zero, 4);
       be_.copy(&d_tot_->ctl, &c0, sizeof(Ctl));
-      (void)h;
       sync_view();
       be_.each(1, SetRehashF{v_});
       be_.fetch(&h_tot_, d_tot_, sizeof(Totals));  // also keeps the host copies alive until done
     }
-    // level 0: the start positions Attack(p0[j], {q0[j]})
-    if (!ensure_level(J, J, J) || !ensure_nodes(0, J, 0, 0)) return 1;
+    // level 0: the start positions Attack(p0[t], {q0[t]}), numbered in order
+    const uint32_t T = in.n_starts;
+    if (!ensure_level(T, T, T) || !ensure_nodes(0, T, 0, 0)) return 1;
     sync_view();
-    be_.each(J, StartF{v_});
-    intern(J, J);
+    be_.each(T, StartF{v_});
+    be_.each(T, SetProbeF{v_});
+    be_.each(T, SetNewF{v_});
+    be_.each(T, SetFillF{v_});
+    be_.each(T, SuccProbeF{v_});
+    be_.each(T, SuccFlagF{v_});
+    be_.scan(v_.snew, v_.srank, T, &d_tot_->t[T_NEW]);
     if (!fetch_totals()) return 1;
-    uint32_t newN = (uint32_t)h_tot_.t[T_NEW];
-    sync_view();
-    number_new(J);
-    v_.n_nodes = 0;
-    local_ids(newN);
-    v_.n_nodes = newN;
-    v_.n_edges = 0;
-    v_.f0 = 0;
-    v_.F = newN;
-    uint32_t levels = 0;
-    while (v_.F > 0) {
-      levels++;
-      const uint32_t F = v_.F;
-      if (!ensure_frontier(F)) return 1;
+    const uint32_t newN = (uint32_t)h_tot_.t[T_NEW];
+    be_.each(T, SuccNewF{v_});
+    be_.each(T, SuccFillF{v_});
+    be_.each(newN, LocalAF{v_});
+    be_.each(newN, LocalBF{v_});
+    be_.each(newN, LocalCF{v_});
+    // the level loop from here on runs on the device
+    if (!fetch_totals()) return 1;
+    h_tot_.t[T_NN] = newN;
+    h_tot_.t[T_NE] = 0;
+    h_tot_.t[T_F0] = 0;
+    h_tot_.t[T_F] = newN;
+    h_tot_.t[T_GO] = 1;
+    h_tot_.t[T_STALL] = 0;
+    h_tot_.t[T_DONE] = 0;
+    h_tot_.t[T_LEVELS] = 0;
+    be_.copy(d_tot_, &h_tot_, sizeof(Totals));
+    // first guesses; the gate stalls a level that does not fit and the
+    // buffers grow to its exact needs
+    if (!ensure_frontier(std::max<uint32_t>(newN, 4096)) || !ensure_level(8 * newN + 4096, 8 * newN + 4096, 8 * newN + 4096))
+      return 1;
+    uint32_t batch = 2;
+    for (;;) {
       sync_view();
-      be_.each(F, CountF{v_});
-      be_.scan(v_.ub_s, v_.off_s, F, &d_tot_->t[T_S]);
-      be_.scan(v_.ub_e, v_.off_e, F, &d_tot_->t[T_E]);
-      be_.scan(v_.ub_c, v_.off_c, F, &d_tot_->t[T_C]);
+      if (!be_.has_graph()) {
+        be_.begin_capture();
+        enqueue_level();
+        be_.end_capture();
+      }
+      for (uint32_t k = 0; k < batch; k++) be_.run_graph();
       if (!fetch_totals()) return 1;
       if (h_tot_.ctl.err & ERR_COLLISION) return 3;
       if (h_tot_.ctl.err) return 2;
-      const unsigned long long S = h_tot_.t[T_S], E = h_tot_.t[T_E], C = h_tot_.t[T_C];
-      if (S >= (1ull << 31) || E >= (1ull << 31) || C >= (1ull << 31)) return 2;
-      if ((uint64_t)h_tot_.ctl.sdata_top + E >= (1ull << 32) || (uint64_t)v_.n_nodes + S >= (1ull << 31) ||
-          (uint64_t)v_.n_edges + S >= (1ull << 32))
+      if (h_tot_.t[T_DONE]) break;
+      if (!h_tot_.t[T_STALL]) {
+        batch = std::min<uint32_t>(batch * 2, 64);
+        continue;
+      }
+      // grow to the stalled level's needs (its bounds were counted, or the
+      // frontier itself did not fit) and run it again
+      const unsigned long long F = h_tot_.t[T_F], S = h_tot_.t[T_S], E = h_tot_.t[T_E], C = h_tot_.t[T_C];
+      const unsigned long long nn = h_tot_.t[T_NN], ne = h_tot_.t[T_NE];
+      if (F >= (1ull << 31) || S >= (1ull << 31) || E >= (1ull << 31) || C >= (1ull << 31) ||
+          (uint64_t)h_tot_.ctl.sdata_top + E >= (1ull << 32) || nn + S >= (1ull << 31) || ne + S >= (1ull << 32))
         return 2;
-      if (!ensure_level((uint32_t)S, (uint32_t)E, (uint32_t)C)) return 1;
+      if (!ensure_frontier((uint32_t)F) || !ensure_level((uint32_t)S, (uint32_t)E, (uint32_t)C)) return 1;
       if (!ensure_sets(h_tot_.ctl.n_sets, h_tot_.ctl.sdata_top, C, E)) return 1;
-      if (!ensure_nodes(v_.n_nodes, S, v_.n_edges, S)) return 1;
-      sync_view();
-      v_.S = (uint32_t)S;
-      v_.C = (uint32_t)C;
-      v_.E = (uint32_t)E;
-      be_.each(F, GenF{v_});
-      intern((uint32_t)S, (uint32_t)C);
-      be_.scan(v_.fcnt, v_.feoff, F, &d_tot_->t[T_EDGE]);
-      number_new((uint32_t)S);
-      be_.each(F, EdgeF{v_});
-      if (!fetch_totals()) return 1;
-      newN = (uint32_t)h_tot_.t[T_NEW];
-      const uint32_t L = (uint32_t)h_tot_.t[T_EDGE];
-      local_ids(newN);
-      v_.n_nodes += newN;
-      v_.n_edges += L;
-      v_.f0 += F;
-      v_.F = newN;
+      if (!ensure_nodes((uint32_t)nn, S, (uint32_t)ne, S)) return 1;
+      be_.drop_graph();
+      h_tot_.t[T_GO] = 1;
+      h_tot_.t[T_STALL] = 0;
+      be_.copy(&d_tot_->t[T_GO], &h_tot_.t[T_GO], 2 * sizeof(unsigned long long));
+      batch = 1;
     }
+    be_.drop_graph();
+    v_.t = d_tot_->t;
+    const uint32_t levels = (uint32_t)h_tot_.t[T_LEVELS];
     if (!fetch_totals()) return 1;
     if (h_tot_.ctl.err & ERR_COLLISION) return 3;
     if (h_tot_.ctl.err) return 2;
     // per-job CSR in local ids
-    const uint32_t N = v_.n_nodes, M = v_.n_edges;
+    const uint32_t N = (uint32_t)h_tot_.t[T_NN], M = (uint32_t)h_tot_.t[T_NE];
     Out o{};
     o.jbase = get<uint32_t>((size_t)J + 1);
     o.fperm = get<uint32_t>(N);

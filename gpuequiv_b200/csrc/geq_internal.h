@@ -227,12 +227,15 @@ class Engine {
   geq_status finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out);
 };
 
-// GameBuild::compare (gamebuild.rs:165-170) of jobs (L[j], p[j], q[j]) built
-// by the device game builder and uploaded on eng's stream as standard-reach
-// games; the graphs never pass through the host.
+// The games of jobs L[j] with start positions Attack(p[t], {q[t]}) for t in
+// start_off[j] .. start_off[j+1]-1 (GameBuild::compare with one start,
+// compare_all with the pairs of start_pairs), built by the device game builder
+// and uploaded on eng's stream as standard-reach games; the graphs never pass
+// through the host.
 struct Lts;
-geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *p,
-                            const uint32_t *q, uint64_t max_positions, GamesPtr &out, double *build_ms);
+geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *start_off,
+                            const uint32_t *p, const uint32_t *q, uint64_t max_positions, GamesPtr &out,
+                            double *build_ms);
 
 // A large batch split in two halves by positions on engines ea and eb: the
 // upload of the second half overlaps the solve of the first.

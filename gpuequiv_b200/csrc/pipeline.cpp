@@ -120,7 +120,10 @@ geq_status geq_compare_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *c
   geq_solution part;
   if (!L.empty()) {
     GamesPtr dg;
-    if ((st = build_and_upload(*e, ctx->device, (uint32_t)L.size(), L.data(), ps.data(), qs.data(), 0, dg, nullptr)))
+    std::vector<uint32_t> start_off(L.size() + 1);
+    for (size_t j = 0; j <= L.size(); j++) start_off[j] = (uint32_t)j;
+    if ((st = build_and_upload(*e, ctx->device, (uint32_t)L.size(), L.data(), start_off.data(), ps.data(), qs.data(),
+                               0, dg, nullptr)))
       return st;
     if ((st = e->solve(*dg, &sol->stats))) return st;
     std::vector<uint32_t> first(L.size(), 0), count(L.size(), 1);
@@ -172,20 +175,25 @@ geq_status geq_equivalences(geq_context *ctx, const geq_lts *l, int minimize, ge
     eq->minimized = true;
   }
   eq->n_processes = base->n;
-  GameBuilder b;
-  GameBuilder::compare_all(*base, b);  // gamebuild.rs:200-215
-  for (uint32_t i = 0; i < b.n_starting; i++) {
-    const PosKey &k = b.nodes[i];
-    eq->starts.emplace_back(k.p, b.sets.ptr(k.a)[0]);
-  }
-  if (b.n_starting) {
-    std::vector<GameInput> in{input_of(b)};
-    in[0].to_reach = in[0].reach_storage.data();
+  // GameBuild::compare_all (gamebuild.rs:200-215): the start pairs on the
+  // host, the game built on the device
+  std::vector<uint32_t> all(base->n);
+  for (uint32_t i = 0; i < base->n; i++) all[i] = i;
+  GameBuilder::start_pairs(*base, all.data(), base->n, eq->starts);
+  const uint32_t n_starting = (uint32_t)eq->starts.size();
+  if (n_starting) {
+    std::vector<uint32_t> sp(n_starting), sq(n_starting), start_off{0, n_starting};
+    for (uint32_t i = 0; i < n_starting; i++) {
+      sp[i] = eq->starts[i].first;
+      sq[i] = eq->starts[i].second;
+    }
+    const Lts *L[1] = {base};
     GamesPtr dg;
-    if ((st = e->upload(in, dg))) return st;
+    if ((st = build_and_upload(*e, ctx->device, 1, L, start_off.data(), sp.data(), sq.data(), 0, dg, nullptr)))
+      return st;
     if ((st = e->solve(*dg, nullptr))) return st;
     geq_solution part;
-    std::vector<uint32_t> first{0}, count{b.n_starting};
+    std::vector<uint32_t> first{0}, count{n_starting};
     if ((st = e->download_selected(*dg, first, count, part))) return st;
     eq->offsets.assign(part.offsets.begin(), part.offsets.end());
     eq->data = std::move(part.data);

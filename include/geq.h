@@ -289,6 +289,7 @@ typedef struct geq_tuning {
 #define GEQ_TUNE_PROFILE 8u       /* time every round-kernel launch (implies no graphs) */
 #define GEQ_TUNE_NO_THREAD_PATH 16u /* no lane-per-position path (cross-check) */
 #define GEQ_TUNE_NO_SPLIT 32u     /* a large batch on one engine, not as two pipelined halves */
+#define GEQ_TUNE_BUILD_WARP_ALL 64u /* device GameBuild: every attack position by the warp path (cross-check) */
 geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t);
 void geq_context_get_tuning(const geq_context *ctx, geq_tuning *t);
 

@@ -87,6 +87,37 @@ def test_batched_workload_vs_host(geq, ctx):
         assert_same(arrays(g), arrays(geq.GameBuild.compare(red, p, q).game), f"seed {rows[k][0]}")
 
 
+def test_warp_path_vs_host(geq, ctx):
+    """Every attack position through the warp path (bitmap unions, ballot
+    placement), on random LTSs with much nondeterminism and on a slice of the
+    batched workload."""
+    from gpuequiv_b200._lib import TUNE_BUILD_WARP_ALL
+    from gpuequiv_b200 import synth
+    rng = np.random.default_rng(11)
+    jobs = []
+    for _ in range(48):
+        n = int(rng.integers(2, 40))
+        lts = geq.TransitionSystem(random_lts(rng, n, int(rng.integers(1, 4)), int(rng.integers(n, 4 * n + 1))))
+        jobs.append((lts, int(rng.integers(0, lts.n_vertices())), int(rng.integers(0, lts.n_vertices()))))
+    for seed, _, _ in synth.batched_manifest()["jobs"][1::64]:
+        src, dst, lab, p, q = synth.batched_lts(seed)
+        red, mp = geq.TransitionSystem.from_arrays(src, dst, lab).bisimilar_minimize()
+        jobs.append((red, int(mp[p]), int(mp[q])))
+    try:
+        ctx.set_tuning(flags=TUNE_BUILD_WARP_ALL)
+        b = geq.GameBatch(jobs, context=ctx, max_positions=300_000)
+    finally:
+        ctx.set_tuning(flags=0)
+    for j, (lts, p, q) in enumerate(jobs):
+        try:
+            host = geq.GameBuild.compare_bounded(lts, p, q, 300_000)
+        except geq.GeqError:
+            with pytest.raises(geq.GeqError):
+                b.graph(j)
+            continue
+        assert_same(arrays(b.graph(j)), arrays(host.game), f"job {j}")
+
+
 def test_position_bound(geq, ctx):
     """Jobs beyond max_positions are refused exactly when compare_bounded refuses."""
     rng = np.random.default_rng(7)
