@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--no-stress", dest="stress", action="store_false", help="skip the stress-game leg")
     ap.add_argument("--solve-only", action="store_true",
                     help="build, upload and solve only (the command profiled with ncu)")
+    ap.add_argument("--build-only", action="store_true",
+                    help="one device GameBuild of the batch's minimised LTSs only (profiled with ncu)")
     return ap.parse_args()
 
 
@@ -317,9 +319,9 @@ def run_serving(ctx, graphs, lam: float, seconds: float, seed: int) -> dict:
 # ---- arms -----------------------------------------------------------------------
 def run_lts_pipeline(ctx, seeds, graphs, args, d: Dist) -> dict:
     """compare_batch over the batch's LTSs: the whole LTS -> energies path
-    (minimisation on the host cores, GameBuild on the device, batched solve,
-    start-position energies read back), against the host GameBuild of the
-    same minimised LTSs on all host cores."""
+    (minimisation and GameBuild on the device, batched solve, start-position
+    energies read back), beside the device GameBuild alone and the host
+    GameBuild of the same minimised LTSs on all host cores."""
     from concurrent.futures import ThreadPoolExecutor
 
     import gpuequiv_b200 as geq
@@ -357,7 +359,7 @@ def run_lts_pipeline(ctx, seeds, graphs, args, d: Dist) -> dict:
     with ThreadPoolExecutor(max_workers=threads) as ex:
         list(ex.map(lambda j: geq.GameBuild.compare(*j), reds))
     host_build_ms = (time.perf_counter() - t) * 1e3
-    return {"workload": "compare_batch over the same 4096 LTSs (unminimised): host minimisation, device GameBuild, "
+    return {"workload": "compare_batch over the same 4096 LTSs (unminimised): device minimisation, device GameBuild, "
                         "batched solve, start energies read back",
             "games_s": d.sum(len(jobs)) / pipe_s, "ms_per_step": pipe_s * 1e3,
             "device_build_ms": float(np.median(dev_build)), "build_levels": b.stats["levels"],
@@ -391,9 +393,36 @@ def run_reference(args, d: Dist):
     }), flush=True)
 
 
+def run_build_only(args, d: Dist):
+    """One device GameBuild of the batch (GameBuild::compare of every job's
+    minimised LTS), nothing else on the device: the command profiled for the
+    builder's launch list."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import gpuequiv_b200 as geq
+    synth = synth_mod()
+    seeds, _ = batched_seeds(args.jobs, d.rank)
+
+    def prep(seed):
+        src, dst, lab, p, q = synth.batched_lts(seed)
+        red, mp = geq.TransitionSystem.from_arrays(src, dst, lab).bisimilar_minimize()
+        return red, int(mp[p]), int(mp[q])
+
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        jobs = list(ex.map(prep, seeds))
+    ctx = geq.Context(d.local_rank)
+    b = geq.GameBatch(jobs, context=ctx)
+    if d.rank == 0:
+        print(json.dumps({"build_only": True, "jobs": len(jobs), "stats": b.stats}), flush=True)
+    del b
+    ctx.close()
+
+
 def run_ours(args, d: Dist):
     import gpuequiv_b200 as geq
     from gpuequiv_b200._lib import TUNE_PROFILE
+    if args.build_only:
+        return run_build_only(args, d)
     ctx = geq.Context(d.local_rank)
     seeds, rows = batched_seeds(args.jobs, d.rank)
     t = time.perf_counter()

@@ -11,11 +11,11 @@ from .energy import (Energy, EnergyArray, EnergyConf, Upd, Update, UpdateArray, 
 from .energygame import (Context, DeviceGames, EnergyGame, GameGraph, c_views, default_context, run_batch,
                          run_batch_raw, run_static)
 from .lts import (Equivalence, EquivalenceRelation, GameBatch, GameBuild, Position, StartInfo,
-                  TransitionSystem, compare_batch)
+                  TransitionSystem, compare_batch, signature_refinement_batch)
 
 __all__ = [
     "GeqError", "library_path", "Energy", "EnergyArray", "EnergyConf", "Upd", "Update", "UpdateArray",
     "std_equivalences", "update", "Context", "DeviceGames", "EnergyGame", "GameGraph", "default_context",
     "run_batch", "run_batch_raw", "run_static", "c_views", "Equivalence", "EquivalenceRelation", "GameBatch", "GameBuild", "Position", "StartInfo",
-    "TransitionSystem", "compare_batch",
+    "TransitionSystem", "compare_batch", "signature_refinement_batch",
 ]

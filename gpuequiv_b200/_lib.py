@@ -153,6 +153,7 @@ _SIGS = {
     "geq_lts_transitions": ([vp, u64p, u32p, i32p], None),
     "geq_lts_signature_refinement": ([vp, u64p, u64p], C.c_int),
     "geq_lts_bisimilar_minimize": ([vp, C.POINTER(vp), u64p], C.c_int),
+    "geq_lts_signature_refinement_batch": ([vp, C.c_uint32, C.POINTER(vp), u64p, u64p], C.c_int),
     "geq_lts_free": ([vp], None),
     "geq_game_build_compare": ([vp, C.c_uint32, C.c_uint32, C.POINTER(vp)], C.c_int),
     "geq_game_build_compare_all": ([vp, C.POINTER(vp)], C.c_int),

@@ -9,6 +9,7 @@
 #include <mutex>
 
 #include "gbuild.cuh"
+#include "refine.cuh"
 #include "geq_internal.h"
 #include "lts.h"
 
@@ -567,22 +568,39 @@ namespace geq {
 struct DeviceBuild {
   gb::DevBackend be;
   std::unique_ptr<gb::Builder<gb::DevBackend>> b;
+  std::unique_ptr<rf::Refiner<gb::DevBackend>> rf;
   gb::Result r;
   char *din = nullptr;
+  uint32_t *dstarts = nullptr;
   HostBuf stage;
-  double upload_ms = 0, build_ms = 0;
+  double upload_ms = 0, build_ms = 0, minimize_ms = 0;
   ~DeviceBuild() {
     b.reset();
+    rf.reset();
     be.release(din);
+    be.release(dstarts);
     cudaStreamSynchronize(be.s);
   }
 };
 
+static geq_status refine_status(int rc, gb::DevBackend &be) {
+  if (!be.ok()) return fail(GEQ_ERR_CUDA, "device minimisation: %s", cudaGetErrorString(be.err));
+  if (rc == 1) return fail(GEQ_ERR_OUT_OF_MEMORY, "device minimisation: out of device memory");
+  if (rc == 3) return fail(GEQ_ERR_INTERNAL, "device minimisation: fingerprint collisions under four hash seeds");
+  return GEQ_OK;
+}
+
 // Job j starts from Attack(p[t], {q[t]}) for t in start_off[j] .. start_off[j+1]-1
 // (local process ids of L[j]), in that order.
+// With `trivial` set, the LTSs are first minimised on the device (signature
+// refinement, then the minimised systems written in place of the originals)
+// and a one-start job whose two processes fall into one class gets no game
+// (the bisimilar short cut of lib.rs:279-281): trivial[j] = 1.  With `stop`
+// set, only the LTSs are staged (for the refinement entry point).
 static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L,
                                const uint32_t *start_off, const uint32_t *p, const uint32_t *q,
-                               uint64_t max_positions, DeviceBuild &db) {
+                               uint64_t max_positions, DeviceBuild &db, std::vector<uint8_t> *trivial = nullptr,
+                               gb::Input *staged = nullptr) {
   using clk = std::chrono::steady_clock;
   std::vector<uint64_t> sb(n_jobs + 1, 0), tb(n_jobs + 1, 0);
   for (uint32_t j = 0; j < n_jobs; j++) {
@@ -662,9 +680,54 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
   in.max_pos = max_pos;
   // attack positions with at least this many q's take the warp path
   in.heavy_min = (eng.tuning.flags & GEQ_TUNE_BUILD_WARP_ALL) ? 1u : 8u;
+  if (staged) {
+    *staged = in;
+    db.upload_ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+    return GEQ_OK;
+  }
+  gb::Input bin = in;
+  if (trivial) {
+    const auto tm = clk::now();
+    db.rf.reset(new rf::Refiner<gb::DevBackend>(be));
+    int rrc = db.rf->run(in);
+    uint32_t *rp0 = nullptr, *rq0 = nullptr;
+    if (rrc == 0) rrc = db.rf->reduce(in, bin, rp0, rq0);
+    geq_status rst = refine_status(rrc, be);
+    if (rst) return rst;
+    // the bisimilar short cut, decided on the host from the mapped starts
+    std::vector<uint32_t> mp((size_t)T), mq((size_t)T);
+    be.copy(mp.data(), rp0, (size_t)T * 4);
+    be.fetch(mq.data(), rq0, (size_t)T * 4);
+    if (!be.ok()) return fail(GEQ_ERR_CUDA, "device minimisation: %s", cudaGetErrorString(be.err));
+    trivial->assign(n_jobs, 0);
+    std::vector<uint32_t> keep;
+    keep.reserve(2 * (size_t)T);
+    for (uint32_t j = 0; j < n_jobs; j++) {
+      const uint32_t t0j = start_off[j], t1j = start_off[j + 1];
+      if (t1j - t0j == 1 && mp[t0j] == mq[t0j]) {
+        (*trivial)[j] = 1;
+        continue;
+      }
+      for (uint32_t t = t0j; t < t1j; t++) keep.push_back(t);
+    }
+    const uint32_t K = (uint32_t)keep.size();
+    std::vector<uint32_t> hst(2 * (size_t)K + 1);
+    for (uint32_t k = 0; k < K; k++) {
+      hst[k] = mp[keep[k]];
+      hst[K + k] = mq[keep[k]];
+    }
+    db.dstarts = (uint32_t *)be.alloc(((size_t)2 * K + 1) * 4);
+    if (!db.dstarts) return fail(GEQ_ERR_OUT_OF_MEMORY, "device start positions");
+    be.copy(db.dstarts, hst.data(), ((size_t)2 * K + 1) * 4);
+    bin.p0 = db.dstarts;
+    bin.q0 = db.dstarts + K;
+    bin.n_starts = K;
+    be.fetch(hst.data(), db.dstarts, 4);  // the host copy above is done
+    db.minimize_ms = std::chrono::duration<double, std::milli>(clk::now() - tm).count();
+  }
   const auto t1 = clk::now();
   db.b.reset(new gb::Builder<gb::DevBackend>(be));
-  const int rc = db.b->run(in, db.r);
+  const int rc = db.b->run(bin, db.r);
   db.upload_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   db.build_ms = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
   if (!be.ok()) return fail(GEQ_ERR_CUDA, "device game build: %s", cudaGetErrorString(be.err));
@@ -679,9 +742,9 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
 // max_positions (0 = no bound) fail with GEQ_ERR_OUT_OF_MEMORY.
 geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *start_off,
                             const uint32_t *p, const uint32_t *q, uint64_t max_positions, GamesPtr &out,
-                            double *build_ms) {
+                            double *build_ms, std::vector<uint8_t> *trivial) {
   DeviceBuild db;
-  geq_status st = device_build(eng, device, n_jobs, L, start_off, p, q, max_positions, db);
+  geq_status st = device_build(eng, device, n_jobs, L, start_off, p, q, max_positions, db, trivial);
   if (st) return st;
   std::vector<uint32_t> jcount(n_jobs), jm(n_jobs), jover(n_jobs);
   db.be.copy(jcount.data(), db.r.jcount, (size_t)n_jobs * 4);
@@ -691,11 +754,23 @@ geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts 
   for (uint32_t j = 0; j < n_jobs; j++)
     if (jover[j]) return fail(GEQ_ERR_OUT_OF_MEMORY, "job %u: game exceeds %llu positions", j,
                               (unsigned long long)max_positions);
-  if (build_ms) *build_ms = db.upload_ms + db.build_ms;
+  if (build_ms) *build_ms = db.upload_ms + db.minimize_ms + db.build_ms;
+  // jobs without positions (no start pairs, or the bisimilar short cut) add
+  // nothing to the arrays: the games are the other jobs, in order
+  std::vector<uint32_t> gn, gm;
+  for (uint32_t j = 0; j < n_jobs; j++)
+    if (jcount[j]) {
+      gn.push_back(jcount[j]);
+      gm.push_back(jm[j]);
+    }
+  if (gn.empty()) {
+    out.reset();
+    return GEQ_OK;
+  }
   BuiltGames bg;
-  bg.n_games = n_jobs;
-  bg.n_nodes = jcount.data();
-  bg.n_edges = jm.data();
+  bg.n_games = (uint32_t)gn.size();
+  bg.n_nodes = gn.data();
+  bg.n_edges = gm.data();
   bg.N = db.r.N;
   bg.M = db.r.M;
   bg.row_rel = db.r.rrel;
@@ -781,6 +856,33 @@ extern "C" geq_status geq_game_build_compare_batch(geq_context *ctx, uint32_t n_
   res->build_ms = db.build_ms;
   res->download_ms = std::chrono::duration<double, std::milli>(clk::now() - t2).count();
   *out = res.release();
+  return GEQ_OK;
+}
+
+extern "C" geq_status geq_lts_signature_refinement_batch(geq_context *ctx, uint32_t n_lts, const geq_lts *const *lts,
+                                                         uint64_t *partitions, uint64_t *n_classes) {
+  if (!ctx || !ctx->engine) return fail(GEQ_ERR_INVALID_INPUT, "context is NULL");
+  if (!lts || !partitions || !n_classes) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  if (n_lts == 0) return fail(GEQ_ERR_INVALID_INPUT, "no systems");
+  std::vector<const Lts *> L(n_lts);
+  for (uint32_t j = 0; j < n_lts; j++) {
+    if (!lts[j]) return fail(GEQ_ERR_INVALID_INPUT, "system %u is NULL", j);
+    L[j] = &lts[j]->l;
+  }
+  std::vector<uint32_t> start_off(n_lts + 1, 0);
+  DeviceBuild db;
+  gb::Input in;
+  geq_status st = device_build(*ctx->engine, ctx->device, n_lts, L.data(), start_off.data(), nullptr, nullptr, 0, db,
+                               nullptr, &in);
+  if (st) return st;
+  db.rf.reset(new rf::Refiner<gb::DevBackend>(db.be));
+  if ((st = refine_status(db.rf->run(in), db.be))) return st;
+  std::vector<uint32_t> part(in.NS), cnt(n_lts);
+  db.be.copy(part.data(), db.rf->partition(), (size_t)in.NS * 4);
+  db.be.fetch(cnt.data(), db.rf->counts(), (size_t)n_lts * 4);
+  if (!db.be.ok()) return fail(GEQ_ERR_CUDA, "device minimisation: %s", cudaGetErrorString(db.be.err));
+  for (uint32_t i = 0; i < in.NS; i++) partitions[i] = part[i];
+  for (uint32_t j = 0; j < n_lts; j++) n_classes[j] = cnt[j];
   return GEQ_OK;
 }
 

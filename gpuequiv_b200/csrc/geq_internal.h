@@ -233,9 +233,13 @@ class Engine {
 // and uploaded on eng's stream as standard-reach games; the graphs never pass
 // through the host.
 struct Lts;
+// With `trivial` set the LTSs are minimised on the device first and a
+// one-start job whose processes are bisimilar gets no game (trivial[j] = 1);
+// the games of out are the jobs with positions, in order (out is empty when
+// there are none).
 geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *start_off,
                             const uint32_t *p, const uint32_t *q, uint64_t max_positions, GamesPtr &out,
-                            double *build_ms);
+                            double *build_ms, std::vector<uint8_t> *trivial = nullptr);
 
 // A large batch split in two halves by positions on engines ea and eb: the
 // upload of the second half overlaps the solve of the first.

@@ -30,22 +30,6 @@ geq_status engine_of(geq_context *ctx, Engine *&e) {
   return GEQ_OK;
 }
 
-GameInput input_of(const GameBuilder &b) {
-  GameInput gi;
-  gi.g.conf = geq_energy_conf{6, 3};
-  gi.g.n_vertices = (uint32_t)b.nodes.size();
-  gi.g.row_offsets = b.row.data();
-  gi.g.column_indices = b.col.data();
-  gi.g.weights = b.wt.data();
-  gi.g.attacker_pos = b.attacker.data();
-  // EnergyGame::standard_reach (energygame.rs:347-352)
-  for (uint32_t v = 0; v < gi.g.n_vertices; v++)
-    if (!b.attacker[v] && b.row[v + 1] == b.row[v]) gi.reach_storage.push_back(v);
-  gi.to_reach = gi.reach_storage.data();
-  gi.n_reach = (uint32_t)gi.reach_storage.size();
-  return gi;
-}
-
 // EnergyArray::test_equivalence (energy.rs:307-318) for STANDARD energies.
 bool holds(const uint32_t *e, uint64_t n, uint32_t eq) {
   for (uint64_t k = 0; k < n; k++) {
@@ -90,44 +74,26 @@ geq_status geq_compare_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *c
     if (!lts[i]) return fail(GEQ_ERR_INVALID_INPUT, "job %u: LTS is NULL", i);
     if (p[i] >= lts[i]->l.n || q[i] >= lts[i]->l.n) return fail(GEQ_ERR_INVALID_INPUT, "job %u: process out of range", i);
   }
-  // host: minimise every LTS (independent -> all host cores); the games are
-  // then built on the device and solved there without leaving it
-  std::vector<Lts> reds(minimize ? n_jobs : 0);
-  std::vector<uint32_t> pm(n_jobs), qm(n_jobs);
+  // everything on the device: the LTSs staged once, minimised (signature
+  // refinement), the bisimilar short cut decided, the games built and solved
+  std::vector<const Lts *> L(n_jobs);
+  std::vector<uint32_t> start_off(n_jobs + 1);
+  for (uint32_t i = 0; i < n_jobs; i++) L[i] = &lts[i]->l;
+  for (uint32_t i = 0; i <= n_jobs; i++) start_off[i] = i;
   std::vector<uint8_t> trivial(n_jobs, 0);
-  parallel_for(n_jobs, [&](uint32_t i) {
-    const Lts &l = lts[i]->l;
-    if (minimize) {
-      std::vector<uint64_t> mapping;
-      l.minimize(mapping, reds[i]);
-      pm[i] = (uint32_t)mapping[p[i]];
-      qm[i] = (uint32_t)mapping[q[i]];
-      if (pm[i] == qm[i]) trivial[i] = 1;  // bisimilar: lib.rs:279-281
-    } else {
-      pm[i] = p[i];
-      qm[i] = q[i];
-    }
-  });
-  std::vector<const Lts *> L;
-  std::vector<uint32_t> ps, qs;
-  for (uint32_t i = 0; i < n_jobs; i++) {
-    if (trivial[i]) continue;
-    L.push_back(minimize ? &reds[i] : &lts[i]->l);
-    ps.push_back(pm[i]);
-    qs.push_back(qm[i]);
-  }
   std::unique_ptr<geq_solution> sol(new geq_solution());
   geq_solution part;
-  if (!L.empty()) {
+  if (n_jobs) {
     GamesPtr dg;
-    std::vector<uint32_t> start_off(L.size() + 1);
-    for (size_t j = 0; j <= L.size(); j++) start_off[j] = (uint32_t)j;
-    if ((st = build_and_upload(*e, ctx->device, (uint32_t)L.size(), L.data(), start_off.data(), ps.data(), qs.data(),
-                               0, dg, nullptr)))
+    if ((st = build_and_upload(*e, ctx->device, n_jobs, L.data(), start_off.data(), p, q, 0, dg, nullptr,
+                               minimize ? &trivial : nullptr)))
       return st;
-    if ((st = e->solve(*dg, &sol->stats))) return st;
-    std::vector<uint32_t> first(L.size(), 0), count(L.size(), 1);
-    if ((st = e->download_selected(*dg, first, count, part))) return st;
+    if (dg) {
+      if ((st = e->solve(*dg, &sol->stats))) return st;
+      const uint32_t n_games = (uint32_t)(std::count(trivial.begin(), trivial.end(), 0));
+      std::vector<uint32_t> first(n_games, 0), count(n_games, 1);
+      if ((st = e->download_selected(*dg, first, count, part))) return st;
+    }
   }
   // assemble: one game of one position per job
   sol->energy_size = 1;

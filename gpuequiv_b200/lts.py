@@ -125,6 +125,24 @@ class TransitionSystem:
         return Equivalence._compute(self, False, context)
 
 
+def signature_refinement_batch(systems: Sequence[TransitionSystem], context: Context | None = None):
+    """TransitionSystem::signature_refinement (lib.rs:444-464) of many systems
+    at once on the device; returns [(partition, n_classes)] like
+    ``TransitionSystem.signature_refinement``."""
+    ctx = context or default_context()
+    n = len(systems)
+    hs = (C.c_void_p * max(n, 1))(*[s.h.value for s in systems])
+    sizes = [s.n_vertices() for s in systems]
+    part = np.zeros(max(sum(sizes), 1), dtype=np.uint64)
+    cnt = np.zeros(max(n, 1), dtype=np.uint64)
+    check(lib.geq_lts_signature_refinement_batch(ctx.h, n, hs, _p(part, _u64), _p(cnt, _u64)))
+    out, o = [], 0
+    for k, m in enumerate(sizes):
+        out.append((part[o:o + m].copy(), int(cnt[k])))
+        o += m
+    return out
+
+
 def compare_batch(jobs: Sequence[tuple[TransitionSystem, int, int]], context: Context | None = None,
                   minimize: bool = True, return_stats: bool = False):
     """TransitionSystem::compare for many (lts, p, q) jobs, all games solved in

@@ -316,6 +316,12 @@ geq_status geq_lts_signature_refinement(const geq_lts *l, uint64_t *partition,
                                         uint64_t *n_classes);
 /* TransitionSystem::bisimilar_minimize (lib.rs:413-432). */
 geq_status geq_lts_bisimilar_minimize(const geq_lts *l, geq_lts **reduced, uint64_t *mapping);
+/* TransitionSystem::signature_refinement (lib.rs:444-464) of n_lts systems at
+ * once on the context's device: partitions holds each system's per-process
+ * class ids in turn (sum of the process counts), n_classes one count per
+ * system; both identical to geq_lts_signature_refinement's. */
+geq_status geq_lts_signature_refinement_batch(geq_context *ctx, uint32_t n_lts, const geq_lts *const *lts,
+                                              uint64_t *partitions, uint64_t *n_classes);
 void geq_lts_free(geq_lts *l);
 
 /* ---- GameBuild (src/gamebuild.rs) --------------------------------------- */
@@ -377,7 +383,8 @@ void geq_game_batch_free(geq_game_batch *b);
 /* ---- whole algorithm (lib.rs:275-343, src/equivalence.rs) --------------- */
 /* TransitionSystem::compare (minimize != 0) / compare_unminimized: the
  * solution holds one game with a single position: the energies of the start
- * position Attack(p, {q}). */
+ * position Attack(p, {q}).  Minimisation, game construction and solving all
+ * run on the device. */
 geq_status geq_compare(geq_context *ctx, const geq_lts *l, uint32_t p, uint32_t q, int minimize,
                        geq_solution **out);
 /* compare() for many (lts, p, q) jobs; every game solved in one batch.  The
