@@ -260,9 +260,11 @@ def profile_traffic_ratio():
     return None
 
 
-def run_serving(ctx, graphs, lam: float, seconds: float, seed: int) -> dict:
-    """Poisson arrivals of single-game requests (drawn from `graphs`) into the
-    serving loop; latency = submit -> result in the caller's hands."""
+def run_serving(ctx, graphs, lam: float, seconds: float, seed: int, queries=False) -> dict:
+    """Poisson arrivals of single requests (drawn from `graphs`) into the
+    serving loop; latency = submit -> result in the caller's hands.  With
+    `queries`, the items are (lts, p, q) equivalence queries (minimised, built
+    and solved on the device), else game graphs."""
     import queue
     import threading
 
@@ -274,11 +276,12 @@ def run_serving(ctx, graphs, lam: float, seconds: float, seed: int) -> dict:
     t_sub = np.zeros(n)
     t_done = np.zeros(n)
     with Server(ctx) as srv:
+        submit = (lambda item: srv.submit_compare(*item)) if queries else srv.submit
         # warm the pipelines (CUDA graphs, device and host pools): single
         # requests, then a burst
         for g in graphs[:32]:
-            srv.poll(srv.submit(g))
-        for t in [srv.submit(g) for g in graphs[:512]]:
+            srv.poll(submit(g))
+        for t in [submit(g) for g in graphs[:512]]:
             srv.poll(t)
         q: "queue.Queue" = queue.Queue()
 
@@ -301,7 +304,7 @@ def run_serving(ctx, graphs, lam: float, seconds: float, seed: int) -> dict:
             if wait > 0:
                 time.sleep(wait)
             t_sub[i] = time.perf_counter()
-            q.put((i, srv.submit(graphs[pick[i]])))
+            q.put((i, submit(graphs[pick[i]])))
         for _ in pollers:
             q.put(None)
         for th in pollers:
@@ -359,7 +362,7 @@ def run_lts_pipeline(ctx, seeds, graphs, args, d: Dist) -> dict:
     with ThreadPoolExecutor(max_workers=threads) as ex:
         list(ex.map(lambda j: geq.GameBuild.compare(*j), reds))
     host_build_ms = (time.perf_counter() - t) * 1e3
-    return {"workload": "compare_batch over the same 4096 LTSs (unminimised): device minimisation, device GameBuild, "
+    return jobs, {"workload": "compare_batch over the same 4096 LTSs (unminimised): device minimisation, device GameBuild, "
                         "batched solve, start energies read back",
             "games_s": d.sum(len(jobs)) / pipe_s, "ms_per_step": pipe_s * 1e3,
             "device_build_ms": float(np.median(dev_build)), "build_levels": b.stats["levels"],
@@ -496,7 +499,7 @@ def run_ours(args, d: Dist):
 
     # ---- LTS -> verdict: compare_batch from the unminimised LTSs (host
     # minimisation, games built on the device, solved, start energies back) ----
-    lts_pipe = run_lts_pipeline(ctx, seeds, graphs, args, d)
+    lts_jobs, lts_pipe = run_lts_pipeline(ctx, seeds, graphs, args, d)
 
     # ---- plain CUDA: one call per game (sample) ----
     idx = sample_indices(len(graphs), args.plain_sample)
@@ -514,6 +517,11 @@ def run_ours(args, d: Dist):
     rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
     for k, lam in enumerate(rates):
         serving.append(run_serving(ctx, graphs, lam, args.serve_seconds, seed=100 + k + 1000 * d.rank))
+    # the same arrivals as equivalence queries on the LTSs themselves
+    serving_q = []
+    for k, lam in enumerate(rates):
+        serving_q.append(run_serving(ctx, lts_jobs, lam, args.serve_seconds, seed=100 + k + 1000 * d.rank,
+                                     queries=True))
 
     # ---- stress configuration: one 2M-position / 10M-edge game, resident ----
     stress = None
@@ -573,7 +581,10 @@ def run_ours(args, d: Dist):
             "stress": stress,
             "serving": {"workload": "Poisson arrivals of single compare(p,q) games drawn from this batch "
                                     "(LTS 20-5000 states), geq_server with 2 pipelines, 150 GB admission budget",
-                        "runs": serving},
+                        "runs": serving,
+                        "queries": {"workload": "the same Poisson arrivals as compare(p, q) queries on the batch's "
+                                                "unminimised LTSs (geq_server_submit_compare: minimisation, "
+                                                "GameBuild and solve on the device)", "runs": serving_q}},
             "gpu_launches": int(launches),
             "clocks": ck,
             "solve_stats": {k: st_last[k] for k in ("rounds", "positions_computed", "edges_relaxed",

@@ -142,6 +142,7 @@ _SIGS = {
     "geq_device_games_free": ([vp], None),
     "geq_server_create": ([vp, C.POINTER(geq_server_config), C.POINTER(vp)], C.c_int),
     "geq_server_submit": ([vp, C.POINTER(geq_game_graph), C.POINTER(C.c_uint64)], C.c_int),
+    "geq_server_submit_compare": ([vp, vp, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)], C.c_int),
     "geq_server_poll": ([vp, C.c_uint64, C.c_int32, C.POINTER(vp)], C.c_int),
     "geq_server_get_stats": ([vp, C.POINTER(geq_server_stats)], None),
     "geq_server_destroy": ([vp], None),

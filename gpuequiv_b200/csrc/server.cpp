@@ -5,9 +5,11 @@
 // batch in flight (continuous batching over alternating pipelines).
 //
 // A request is one game with standard initialisation, as EnergyGame::run
-// after EnergyGame::standard_reach (energygame.rs:347-352, :379-383).  Inside
-// a batch every game keeps its own positions and frontier, so each result is
-// the result of solving that game alone.
+// after EnergyGame::standard_reach (energygame.rs:347-352, :379-383), or one
+// TransitionSystem::compare query (lib.rs:275-283) that is minimised, built
+// and solved on the device with the other queries of its batch.  Inside a
+// batch every game keeps its own positions and frontier, so each result is
+// the result of solving that game or query alone.
 
 #include <chrono>
 #include <condition_variable>
@@ -20,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include "geq_internal.h"
+#include "lts.h"
 
 namespace geq {
 namespace {
@@ -30,9 +33,18 @@ namespace {
 // power-of-two blocks, plus the fixed minimum arena.
 constexpr uint64_t BATCH_BASE_BYTES = 32ull << 20;
 uint64_t game_footprint(uint64_t n, uint64_t m) { return 2 * (70 * n + 12 * m) + 4096; }
+// A compare query's game is not known before it is built: estimated at 16
+// positions and 64 edges per state and transition of its LTS, plus the
+// builder's and the minimisation's per-state and per-transition arrays.
+uint64_t compare_footprint(uint64_t n, uint64_t m) {
+  return game_footprint(16 * (n + m) + 64, 64 * (n + m) + 256) + 64 * (n + m);
+}
 
 struct Request {
   uint64_t ticket = 0;
+  int kind = 0;  // 0: a game (geq_server_submit), 1: a compare query (geq_server_submit_compare)
+  Lts lts;
+  uint32_t p = 0, q = 0;
   geq_energy_conf conf{};
   uint32_t n = 0;
   std::vector<uint32_t> row, col, wt, reach;
@@ -81,6 +93,63 @@ std::unique_ptr<geq_solution> split_one(const geq_solution &all, uint32_t g) {
   s->data.assign(d, d + words * all.energy_size);
   s->stats = all.stats;
   return s;
+}
+
+// Compare queries of a batch: minimised, built and solved together on the
+// device (the path of geq_compare_batch); each request gets the energies of
+// its start position.  On failure of several, each is retried alone.
+void run_compares(Engine &e, int device, std::vector<Request *> &batch) {
+  const uint32_t n = (uint32_t)batch.size();
+  std::vector<const Lts *> L(n);
+  std::vector<uint32_t> p(n), q(n), start_off(n + 1);
+  for (uint32_t i = 0; i < n; i++) {
+    L[i] = &batch[i]->lts;
+    p[i] = batch[i]->p;
+    q[i] = batch[i]->q;
+  }
+  for (uint32_t i = 0; i <= n; i++) start_off[i] = i;
+  std::vector<uint8_t> trivial;
+  GamesPtr dg;
+  geq_solution part;
+  geq_status st = build_and_upload(e, device, n, L.data(), start_off.data(), p.data(), q.data(), 0, dg, nullptr,
+                                   &trivial);
+  if (!st && dg) st = e.solve(*dg, &part.stats);
+  if (!st && dg) {
+    const uint32_t games = (uint32_t)std::count(trivial.begin(), trivial.end(), 0);
+    std::vector<uint32_t> first(games, 0), count(games, 1);
+    st = e.download_selected(*dg, first, count, part);
+  }
+  dg.reset();
+  if (st) {
+    if (n > 1) {
+      for (Request *r : batch) {
+        std::vector<Request *> one{r};
+        run_compares(e, device, one);
+      }
+      return;
+    }
+    batch[0]->st = st;
+    batch[0]->err = geq_last_error();
+    return;
+  }
+  uint32_t k = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    std::unique_ptr<geq_solution> sol(new geq_solution());
+    sol->energy_size = 1;
+    sol->n_vertices.assign(1, 1);
+    sol->offsets_base.assign(1, 0);
+    sol->data_base.assign(1, 0);
+    sol->stats = part.stats;
+    if (trivial[i]) {
+      sol->offsets = {0, 0};  // bisimilar: lib.rs:279-281
+    } else {
+      const uint64_t cnt = part.offsets[part.offsets_base[k] + 1];
+      sol->offsets = {0, cnt};
+      sol->data.assign(part.data.begin() + part.data_base[k], part.data.begin() + part.data_base[k] + cnt);
+      k++;
+    }
+    batch[i]->sol = std::move(sol);
+  }
 }
 
 // Upload, solve and download one batch on engine `e`; on failure of a batch
@@ -166,7 +235,12 @@ void pipeline(geq_server *s, Engine *e) {
       s->stats.queued = s->queue.size();
       if (fp > s->stats.max_batch_footprint) s->stats.max_batch_footprint = fp;
     }
-    run_batch(*e, batch);
+    {
+      std::vector<Request *> games, compares;
+      for (Request *r : batch) (r->kind ? compares : games).push_back(r);
+      if (!games.empty()) run_batch(*e, games);
+      if (!compares.empty()) run_compares(*e, s->device, compares);
+    }
     {
       std::lock_guard<std::mutex> lk(s->mu);
       for (Request *r : batch) {
@@ -232,6 +306,34 @@ geq_status geq_server_submit(geq_server *s, const geq_game_graph *graph, uint64_
     return fail(GEQ_ERR_OUT_OF_MEMORY, "game of %llu positions needs ~%llu device bytes, a pipeline may use %llu",
                 (unsigned long long)n, (unsigned long long)(BATCH_BASE_BYTES + r->footprint),
                 (unsigned long long)s->budget);
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stop) return fail(GEQ_ERR_BUSY, "server is shutting down");
+    if (s->queue.size() >= s->cfg.max_queued) return fail(GEQ_ERR_BUSY, "%llu requests queued",
+                                                          (unsigned long long)s->queue.size());
+    r->ticket = s->next_ticket++;
+    *ticket = r->ticket;
+    s->queue.push_back(r.get());
+    s->reqs.emplace(r->ticket, std::move(r));
+    s->stats.submitted++;
+    s->stats.queued = s->queue.size();
+  }
+  s->cv_work.notify_one();
+  return GEQ_OK;
+}
+
+geq_status geq_server_submit_compare(geq_server *s, const geq_lts *lts, uint32_t p, uint32_t q, uint64_t *ticket) {
+  if (!s || !lts || !ticket) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  if (p >= lts->l.n || q >= lts->l.n) return fail(GEQ_ERR_INVALID_INPUT, "process out of range");
+  std::unique_ptr<Request> r(new Request());
+  r->kind = 1;
+  r->lts = lts->l;
+  r->p = p;
+  r->q = q;
+  r->footprint = compare_footprint(lts->l.n, lts->l.n_transitions());
+  if (BATCH_BASE_BYTES + r->footprint > s->budget)
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "query of %u processes needs ~%llu device bytes, a pipeline may use %llu",
+                lts->l.n, (unsigned long long)(BATCH_BASE_BYTES + r->footprint), (unsigned long long)s->budget);
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) return fail(GEQ_ERR_BUSY, "server is shutting down");

@@ -18,7 +18,8 @@ TIMEOUT = 4  # GEQ_ERR_TIMEOUT
 
 
 class Server:
-    """geq_server: ``submit(graph) -> ticket``, ``poll(ticket, timeout_ms)``."""
+    """geq_server: ``submit(graph)`` / ``submit_compare(lts, p, q) -> ticket``,
+    ``poll(ticket, timeout_ms)``."""
 
     def __init__(self, context: Context | None = None, n_pipelines: int = 0, max_batch_games: int = 0,
                  max_wait_us: int = 0, hbm_budget_bytes: int = 0, max_queued: int = 0):
@@ -33,6 +34,14 @@ class Server:
         t = C.c_uint64()
         view = graph.c_view()
         check(lib.geq_server_submit(self.h, C.byref(view), C.byref(t)))
+        return t.value
+
+    def submit_compare(self, lts, p: int, q: int) -> int:
+        """Queue one ``TransitionSystem.compare(p, q)`` query (the LTS is
+        copied); its result is the start position's energies, as
+        ``lts.compare(p, q)``."""
+        t = C.c_uint64()
+        check(lib.geq_server_submit_compare(self.h, lts.h, int(p), int(q), C.byref(t)))
         return t.value
 
     def poll(self, ticket: int, timeout_ms: int = -1):

@@ -265,6 +265,13 @@ geq_status geq_server_create(geq_context *ctx, const geq_server_config *cfg, geq
  * malformed graph (the same checks as geq_energy_game_run); a game whose
  * estimated footprint alone exceeds a pipeline's budget: GEQ_ERR_OUT_OF_MEMORY. */
 geq_status geq_server_submit(geq_server *srv, const geq_game_graph *graph, uint64_t *ticket);
+/* Queue one equivalence query TransitionSystem::compare(p, q) (lib.rs:275-283;
+ * the LTS is copied).  The queries of a batch are minimised, built and solved
+ * together on the device; the solution equals geq_compare's: one game of one
+ * position, the energies of Attack(p, {q}) (none for bisimilar processes).
+ * Admission uses an estimate of the game from the LTS's size. */
+geq_status geq_server_submit_compare(geq_server *srv, const struct geq_lts *lts, uint32_t p, uint32_t q,
+                                     uint64_t *ticket);
 /* Wait up to timeout_ms (< 0: forever) for request `ticket`.  GEQ_OK: *out
  * is its solution (one game; free with geq_solution_free) and the ticket is
  * retired.  GEQ_ERR_TIMEOUT: not finished yet (poll again).  Any other

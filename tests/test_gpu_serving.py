@@ -115,3 +115,46 @@ def test_unknown_ticket_and_busy(geq, ctx):
         with pytest.raises(GeqError) as e:
             srv.poll(12345, timeout_ms=0)
         assert e.value.name == "INVALID_INPUT"
+
+
+def test_compare_queries_alone_equal_in_the_mix(geq, ctx):
+    """LTS equivalence queries (geq_server_submit_compare) mixed with game
+    requests: each query's energies equal compare() of the query alone and
+    the oracle's TransitionSystem::compare; bisimilar pairs give no energies."""
+    from gpuequiv_b200 import synth
+    from gpuequiv_b200.serving import Server
+    from helpers import random_lts
+    from oracle import ora
+    queries, oracle_of = [], {}
+    for seed, npos, _ in synth.batched_manifest()["jobs"][:400]:
+        if npos <= 20_000 and len(queries) < 96:
+            src, dst, lab, p, q = synth.batched_lts(seed)
+            queries.append((geq.TransitionSystem.from_arrays(src, dst, lab), int(p), int(q)))
+    rng = np.random.default_rng(31)
+    for k in range(24):
+        n = int(rng.integers(2, 10))
+        edges = random_lts(rng, n, 2, int(rng.integers(n, 2 * n + 1)))
+        lts = geq.TransitionSystem(edges)
+        p = int(rng.integers(0, lts.n_vertices()))
+        q = p if k % 6 == 0 else int(rng.integers(0, lts.n_vertices()))
+        oracle_of[len(queries)] = ora.compare(ora.Lts.from_edges(edges), p, q)
+        queries.append((lts, p, q))
+    alone = [sorted(int(x) for x in np.asarray(geq.compare_batch([qq], context=ctx)[0].array).reshape(-1))
+             for qq in queries]
+    games = _games(geq, 16)
+    with Server(ctx, n_pipelines=2, max_wait_us=1000) as srv:
+        tickets = []
+        for i, (lts, p, q) in enumerate(queries):
+            tickets.append(srv.submit_compare(lts, p, q))
+            if i % 8 == 0:
+                srv.submit(games[(i // 8) % len(games)])
+        got = []
+        for t in tickets:
+            offs, data, _ = srv.poll(t, timeout_ms=120_000)
+            assert len(offs) == 2
+            got.append(sorted(int(x) for x in data[int(offs[0]):int(offs[1])]))
+        st = srv.stats()
+    assert got == alone
+    for i, ref in oracle_of.items():
+        assert got[i] == sorted(int(x) for x in np.asarray(ref).reshape(-1)), i
+    assert st["failed"] == 0
