@@ -834,7 +834,8 @@ class Builder {
   template <class T>
   bool grow(T *&p, uint32_t &cap, uint64_t need, uint64_t keep) {
     if (need <= cap) return true;
-    const uint64_t nc = std::max<uint64_t>(need + need / 2, 1024);
+    uint64_t nc = std::max<uint64_t>(2 * need, 1024);  // doubling: few stalls of the level loop
+    if (nc > 0xffffffffull) nc = need;
     if (nc > 0xffffffffull) return false;
     T *q = get<T>(nc);
     if (!q) return false;
@@ -1060,9 +1061,16 @@ class Builder {
     be_.copy(d_tot_, &h_tot_, sizeof(Totals));
     // first guesses; the gate stalls a level that does not fit and the
     // buffers grow to its exact needs
-    if (!ensure_frontier(std::max<uint32_t>(newN, 4096)) || !ensure_level(8 * newN + 4096, 8 * newN + 4096, 8 * newN + 4096))
-      return 1;
-    uint32_t batch = 2;
+    {
+      const uint64_t guess = 8ull * newN + 4096;
+      if (!ensure_frontier(std::max<uint32_t>(newN, 4096)) ||
+          !ensure_level((uint32_t)guess, (uint32_t)guess, (uint32_t)guess) ||
+          !ensure_sets(h_tot_.ctl.n_sets, h_tot_.ctl.sdata_top, guess, guess) || !ensure_nodes(newN, guess, 0, guess))
+        return 1;
+    }
+    uint32_t batch = 4;
+    unsigned long long last_stall = ~0ull;
+    uint32_t same_stall = 0;
     for (;;) {
       sync_view();
       if (!be_.has_graph()) {
@@ -1080,7 +1088,11 @@ class Builder {
         continue;
       }
       // grow to the stalled level's needs (its bounds were counted, or the
-      // frontier itself did not fit) and run it again
+      // frontier itself did not fit) and run it again; a level that stalls
+      // again after its buffers grew would be a defect: give up
+      if (h_tot_.t[T_LEVELS] == last_stall && ++same_stall > 2) return 2;
+      if (h_tot_.t[T_LEVELS] != last_stall) same_stall = 0;
+      last_stall = h_tot_.t[T_LEVELS];
       const unsigned long long F = h_tot_.t[T_F], S = h_tot_.t[T_S], E = h_tot_.t[T_E], C = h_tot_.t[T_C];
       const unsigned long long nn = h_tot_.t[T_NN], ne = h_tot_.t[T_NE];
       if (F >= (1ull << 31) || S >= (1ull << 31) || E >= (1ull << 31) || C >= (1ull << 31) ||
