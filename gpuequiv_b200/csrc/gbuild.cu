@@ -731,7 +731,12 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
   db.upload_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   db.build_ms = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
   if (!be.ok()) return fail(GEQ_ERR_CUDA, "device game build: %s", cudaGetErrorString(be.err));
-  if (rc == 1) return fail(GEQ_ERR_OUT_OF_MEMORY, "device game build: out of device memory");
+  if (rc == 1)
+    return fail(GEQ_ERR_OUT_OF_MEMORY,
+                "device game build: out of device memory (a request of %llu could not be met; %llu positions, "
+                "%llu edges after %llu levels)",
+                (unsigned long long)db.b->short_, (unsigned long long)db.b->reached_positions(),
+                (unsigned long long)db.b->reached_edges(), (unsigned long long)db.b->reached_levels());
   if (rc == 2) return fail(GEQ_ERR_INVALID_INPUT, "device game build: game beyond 2^31 positions or 2^32 edges");
   if (rc == 3) return fail(GEQ_ERR_INTERNAL, "device game build: fingerprint collisions under four hash seeds");
   return GEQ_OK;

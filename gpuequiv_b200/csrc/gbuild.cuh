@@ -801,6 +801,13 @@ class Builder {
     return 3;
   }
   // device buffers of the result stay owned by the builder until it dies
+  // After a failure: the request that could not be met (elements or bytes),
+  // and the positions / edges / levels reached.
+  uint64_t short_ = 0;
+  uint64_t reached_positions() const { return h_tot_.t[T_NN]; }
+  uint64_t reached_edges() const { return h_tot_.t[T_NE]; }
+  uint64_t reached_levels() const { return h_tot_.t[T_LEVELS]; }
+
  private:
   B &be_;
   struct Buf {
@@ -836,9 +843,19 @@ class Builder {
     if (need <= cap) return true;
     uint64_t nc = std::max<uint64_t>(2 * need, 1024);  // doubling: few stalls of the level loop
     if (nc > 0xffffffffull) nc = need;
-    if (nc > 0xffffffffull) return false;
+    if (nc > 0xffffffffull) {
+      short_ = need;
+      return false;
+    }
     T *q = get<T>(nc);
-    if (!q) return false;
+    if (!q) {  // no room for headroom: exactly what is needed
+      nc = need;
+      q = get<T>(nc);
+    }
+    if (!q) {
+      short_ = need * sizeof(T);
+      return false;
+    }
     if (p && keep) be_.copy(q, p, keep * sizeof(T));
     put(p);
     p = q;
@@ -860,52 +877,61 @@ class Builder {
   bool ensure_frontier(uint32_t F) {
     uint32_t c;
     bool ok = true;
-    c = capF_; ok = ok && grow(v_.ub_s, c, F, 0);
-    c = capF_; ok = ok && grow(v_.ub_e, c, F, 0);
-    c = capF_; ok = ok && grow(v_.ub_c, c, F, 0);
-    c = capF_; ok = ok && grow(v_.off_s, c, F, 0);
-    c = capF_; ok = ok && grow(v_.off_e, c, F, 0);
-    c = capF_; ok = ok && grow(v_.off_c, c, F, 0);
-    c = capF_; ok = ok && grow(v_.fcnt, c, F, 0);
-    c = capF_; ok = ok && grow(v_.feoff, c, F, 0);
-    c = capF_; ok = ok && grow(v_.hq, c, F, 0);
-    capF_ = c;
+    uint32_t m_capF_ = 0xffffffffu;
+    c = capF_; ok = ok && grow(v_.ub_s, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    c = capF_; ok = ok && grow(v_.ub_e, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    c = capF_; ok = ok && grow(v_.ub_c, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    c = capF_; ok = ok && grow(v_.off_s, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    c = capF_; ok = ok && grow(v_.off_e, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    c = capF_; ok = ok && grow(v_.off_c, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    c = capF_; ok = ok && grow(v_.fcnt, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    c = capF_; ok = ok && grow(v_.feoff, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    c = capF_; ok = ok && grow(v_.hq, c, F, 0); m_capF_ = std::min(m_capF_, c);
+    capF_ = m_capF_;
     return ok;
   }
   bool ensure_level(uint32_t S, uint32_t E, uint32_t C) {
     bool ok = true;
     uint32_t c;
-    c = capS_; ok = ok && grow(v_.succ, c, S, 0);
-    c = capS_; ok = ok && grow(v_.swt, c, S, 0);
-    c = capS_; ok = ok && grow(v_.sslot, c, S, 0);
-    c = capS_; ok = ok && grow(v_.sres, c, S, 0);
-    c = capS_; ok = ok && grow(v_.snew, c, S, 0);
-    c = capS_; ok = ok && grow(v_.srank, c, S, 0);
-    capS_ = c;
-    c = capE_; ok = ok && grow(v_.celem, c, E, 0);
-    capE_ = c;
-    c = capC_; ok = ok && grow(v_.cstart, c, C, 0);
-    c = capC_; ok = ok && grow(v_.clen, c, C, 0);
-    c = capC_; ok = ok && grow(v_.cslot, c, C, 0);
-    c = capC_; ok = ok && grow(v_.cid, c, C, 0);
-    capC_ = c;
+    uint32_t m_capS_ = 0xffffffffu;
+    c = capS_; ok = ok && grow(v_.succ, c, S, 0); m_capS_ = std::min(m_capS_, c);
+    c = capS_; ok = ok && grow(v_.swt, c, S, 0); m_capS_ = std::min(m_capS_, c);
+    c = capS_; ok = ok && grow(v_.sslot, c, S, 0); m_capS_ = std::min(m_capS_, c);
+    c = capS_; ok = ok && grow(v_.sres, c, S, 0); m_capS_ = std::min(m_capS_, c);
+    c = capS_; ok = ok && grow(v_.snew, c, S, 0); m_capS_ = std::min(m_capS_, c);
+    c = capS_; ok = ok && grow(v_.srank, c, S, 0); m_capS_ = std::min(m_capS_, c);
+    capS_ = m_capS_;
+    uint32_t m_capE_ = 0xffffffffu;
+    c = capE_; ok = ok && grow(v_.celem, c, E, 0); m_capE_ = std::min(m_capE_, c);
+    capE_ = m_capE_;
+    uint32_t m_capC_ = 0xffffffffu;
+    c = capC_; ok = ok && grow(v_.cstart, c, C, 0); m_capC_ = std::min(m_capC_, c);
+    c = capC_; ok = ok && grow(v_.clen, c, C, 0); m_capC_ = std::min(m_capC_, c);
+    c = capC_; ok = ok && grow(v_.cslot, c, C, 0); m_capC_ = std::min(m_capC_, c);
+    c = capC_; ok = ok && grow(v_.cid, c, C, 0); m_capC_ = std::min(m_capC_, c);
+    capC_ = m_capC_;
     return ok;
   }
   // set store and table for `extra` more sets of at most `words` words
   bool ensure_sets(uint32_t n_sets, uint32_t top, uint64_t extra, uint64_t words) {
     bool ok = true;
     uint32_t c;
-    c = capSdata_; ok = ok && grow(v_.sdata, c, top + words, top);
-    capSdata_ = c;
-    c = capSets_; ok = ok && grow(v_.sstart, c, n_sets + extra, n_sets);
-    c = capSets_; ok = ok && grow(v_.slen, c, n_sets + extra, n_sets);
-    capSets_ = c;
+    uint32_t m_capSdata_ = 0xffffffffu;
+    c = capSdata_; ok = ok && grow(v_.sdata, c, top + words, top); m_capSdata_ = std::min(m_capSdata_, c);
+    capSdata_ = m_capSdata_;
+    uint32_t m_capSets_ = 0xffffffffu;
+    c = capSets_; ok = ok && grow(v_.sstart, c, n_sets + extra, n_sets); m_capSets_ = std::min(m_capSets_, c);
+    c = capSets_; ok = ok && grow(v_.slen, c, n_sets + extra, n_sets); m_capSets_ = std::min(m_capSets_, c);
+    capSets_ = m_capSets_;
     if (!ok) return false;
     const uint64_t need = 2 * ((uint64_t)n_sets + extra);
     if (need <= scap_) return true;
     uint64_t cap = 1024;
-    while (cap < 2 * need) cap <<= 1;
-    if (cap > (1ull << 31)) return false;
+    while (cap < 2 * need && cap < (1ull << 31)) cap <<= 1;  // load <= 1/4, at most 2^31 slots
+    if (cap < need) {
+      short_ = need;
+      return false;
+    }
     put(v_.stab); put(v_.sval); put(v_.sclaim);
     v_.stab = get<unsigned long long>(cap);
     v_.sval = get<uint32_t>(cap);
@@ -923,20 +949,25 @@ class Builder {
   bool ensure_nodes(uint32_t n_nodes, uint64_t extra, uint32_t n_edges, uint64_t extra_edges) {
     bool ok = true;
     uint32_t c;
-    c = capNodes_; ok = ok && grow(v_.nkey, c, n_nodes + extra, n_nodes);
-    c = capNodes_; ok = ok && grow(v_.nlocal, c, n_nodes + extra, n_nodes);
-    c = capNodes_; ok = ok && grow(v_.nrow, c, n_nodes + extra, n_nodes);
-    c = capNodes_; ok = ok && grow(v_.neoff, c, n_nodes + extra, n_nodes);
-    capNodes_ = c;
-    c = capEdges_; ok = ok && grow(v_.ecol, c, (uint64_t)n_edges + extra_edges, n_edges);
-    c = capEdges_; ok = ok && grow(v_.ewt, c, (uint64_t)n_edges + extra_edges, n_edges);
-    capEdges_ = c;
+    uint32_t m_capNodes_ = 0xffffffffu;
+    c = capNodes_; ok = ok && grow(v_.nkey, c, n_nodes + extra, n_nodes); m_capNodes_ = std::min(m_capNodes_, c);
+    c = capNodes_; ok = ok && grow(v_.nlocal, c, n_nodes + extra, n_nodes); m_capNodes_ = std::min(m_capNodes_, c);
+    c = capNodes_; ok = ok && grow(v_.nrow, c, n_nodes + extra, n_nodes); m_capNodes_ = std::min(m_capNodes_, c);
+    c = capNodes_; ok = ok && grow(v_.neoff, c, n_nodes + extra, n_nodes); m_capNodes_ = std::min(m_capNodes_, c);
+    capNodes_ = m_capNodes_;
+    uint32_t m_capEdges_ = 0xffffffffu;
+    c = capEdges_; ok = ok && grow(v_.ecol, c, (uint64_t)n_edges + extra_edges, n_edges); m_capEdges_ = std::min(m_capEdges_, c);
+    c = capEdges_; ok = ok && grow(v_.ewt, c, (uint64_t)n_edges + extra_edges, n_edges); m_capEdges_ = std::min(m_capEdges_, c);
+    capEdges_ = m_capEdges_;
     if (!ok) return false;
     const uint64_t need = 2 * ((uint64_t)n_nodes + extra);
     if (need <= ncap_) return true;
     uint64_t cap = 1024;
-    while (cap < 2 * need) cap <<= 1;
-    if (cap > (1ull << 31)) return false;
+    while (cap < 2 * need && cap < (1ull << 31)) cap <<= 1;  // load <= 1/4, at most 2^31 slots
+    if (cap < need) {
+      short_ = need;
+      return false;
+    }
     put(v_.ntab); put(v_.nval); put(v_.nclaim);
     v_.ntab = get<unsigned long long>(cap);
     v_.nval = get<uint32_t>(cap);
