@@ -393,6 +393,13 @@ __device__ void gen_attack_warp(const View &v, uint32_t i, uint32_t *bm, uint32_
   if (lane == 0) v.fcnt[i] = cnt;
 }
 
+// End of one level inside the graph's WHILE node: run the next level while
+// the loop may go on, at most ctr[1] levels per graph launch (ctr[0] counts).
+__global__ void k_level_cond(cudaGraphConditionalHandle h, const unsigned long long *go, uint32_t *ctr) {
+  const uint32_t k = ++ctr[0];
+  cudaGraphSetConditional(h, (*go != 0ull && k < ctr[1]) ? 1u : 0u);
+}
+
 __global__ void __launch_bounds__(GH_WARPS * 32) k_gen_heavy(View v, const unsigned long long *go) {
   __shared__ uint32_t bm_all[GH_WARPS][GH_BM_WORDS];
   if (go && !*go) return;
@@ -525,35 +532,60 @@ struct DevBackend {
     k_cscan_down<3><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
     launches += 3;
   }
-  // ---- one level recorded as a CUDA graph ----
-  cudaGraph_t graph = nullptr;
+  // ---- the level loop as a CUDA graph: a WHILE node whose body is one
+  // recorded level followed by k_level_cond, so that one launch runs levels
+  // until the loop stops (frontier empty, a stall) or the launch's limit ----
+  cudaGraph_t graph = nullptr, body = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  cudaGraphConditionalHandle cond = 0;
+  uint32_t *d_loop = nullptr;  // [levels run in this launch, limit]
+  uint32_t h_loop[2] = {0, 0};
   uint32_t graph_launches = 0, mark = 0;
   bool has_graph() const { return gexec != nullptr; }
   void begin_capture() {
     reserve_part();
+    if (!d_loop) d_loop = (uint32_t *)alloc(2 * sizeof(uint32_t));
+    if (!d_loop) note(cudaErrorMemoryAllocation);
     mark = launches;
-    note(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    note(cudaGraphCreate(&graph, 0));
+    note(cudaGraphConditionalHandleCreate(&cond, graph, 1u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = cond;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    note(cudaGraphAddNode(&node, graph, nullptr, 0, &np));
+    body = np.conditional.phGraph_out[0];
+    note(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   }
-  void end_capture() {
-    note(cudaStreamEndCapture(s, &graph));
+  void end_capture(const unsigned long long *go) {
+    k_level_cond<<<1, 1, 0, s>>>(cond, go, d_loop);
+    note(cudaStreamEndCapture(s, &body));
     graph_launches = launches - mark;
     launches = mark;
     if (err == cudaSuccess) note(cudaGraphInstantiate(&gexec, graph, 0));
   }
-  void run_graph() {
+  // up to `limit` levels in one launch
+  void run_graph(uint32_t limit) {
     if (!gexec) return;
+    h_loop[0] = 0;
+    h_loop[1] = limit;
+    note(cudaMemcpyAsync(d_loop, h_loop, sizeof(h_loop), cudaMemcpyHostToDevice, s));
     note(cudaGraphLaunch(gexec, s));
-    launches += graph_launches;
   }
+  // kernel launches of the levels that ran
+  void note_levels(unsigned long long levels) { launches += (uint32_t)(levels * graph_launches); }
   void drop_graph() {
     if (gexec) cudaGraphExecDestroy(gexec);
-    if (graph) cudaGraphDestroy(graph);
+    if (graph) cudaGraphDestroy(graph);  // the WHILE node's body with it
     gexec = nullptr;
     graph = nullptr;
+    body = nullptr;
   }
   ~DevBackend() {
     drop_graph();
+    if (d_loop) cudaFreeAsync(d_loop, s);
     if (part) cudaFreeAsync(part, s);
   }
 };
@@ -679,7 +711,7 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
   in.jsb = (const uint32_t *)(db.din + o_jsb);
   in.max_pos = max_pos;
   // attack positions with at least this many q's take the warp path
-  in.heavy_min = (eng.tuning.flags & GEQ_TUNE_BUILD_WARP_ALL) ? 1u : 8u;
+  in.heavy_min = (eng.tuning.flags & GEQ_TUNE_BUILD_WARP_ALL) ? 1u : 4u;
   if (staged) {
     *staged = in;
     db.upload_ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();

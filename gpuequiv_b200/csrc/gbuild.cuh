@@ -700,27 +700,27 @@ struct RowEndF {
 // ---- level bookkeeping on the device (one thread each) ---------------------------
 // Start of a level: done when the frontier is empty; a frontier beyond the
 // scratch capacity stalls the loop until the host has grown the buffers.
+__host__ __device__ inline void level_start(const View &v) {
+  v.ctl->n_heavy = 0;
+  if (v.t[T_F] == 0) {
+    v.t[T_GO] = 0;
+    v.t[T_DONE] = 1;
+  } else if (v.t[T_F] > v.capF) {
+    v.t[T_GO] = 0;
+    v.t[T_STALL] = 1;
+  }
+}
 struct LevelStartF {
   View v;
   __host__ __device__ void operator()(uint32_t) const {
-    if (!v.t[T_GO]) return;
-    v.ctl->n_heavy = 0;
-    if (v.t[T_F] == 0) {
-      v.t[T_GO] = 0;
-      v.t[T_DONE] = 1;
-    } else if (v.t[T_F] > v.capF) {
-      v.t[T_GO] = 0;
-      v.t[T_STALL] = 1;
-    }
+    if (v.t[T_GO]) level_start(v);
   }
 };
 // After the bounds' scans and before anything persistent is written: every
 // buffer and table must hold this level, else the level stalls (and is run
 // again after the host grew them).
-struct LevelGateF {
-  View v;
-  __host__ __device__ void operator()(uint32_t) const {
-    if (!v.t[T_GO]) return;
+__host__ __device__ inline void level_gate(const View &v) {
+  {
     const unsigned long long S = v.t[T_S], E = v.t[T_E], C = v.t[T_C], nn = v.t[T_NN], ne = v.t[T_NE];
     const unsigned long long ns = v.ctl->n_sets, top = v.ctl->sdata_top;
     const bool fits = S < (1ull << 31) && E < (1ull << 31) && C < (1ull << 31) && S <= v.capS && E <= v.capE &&
@@ -731,16 +731,24 @@ struct LevelGateF {
       v.t[T_STALL] = 1;
     }
   }
+}
+struct LevelGateF {
+  View v;
+  __host__ __device__ void operator()(uint32_t) const {
+    if (v.t[T_GO]) level_gate(v);
+  }
 };
+__host__ __device__ inline void level_end(const View &v) {
+  v.t[T_NN] += v.t[T_NEW];
+  v.t[T_NE] += v.t[T_EDGE];
+  v.t[T_F0] += v.t[T_F];
+  v.t[T_F] = v.t[T_NEW];
+  v.t[T_LEVELS] += 1;
+}
 struct LevelEndF {
   View v;
   __host__ __device__ void operator()(uint32_t) const {
-    if (!v.t[T_GO]) return;
-    v.t[T_NN] += v.t[T_NEW];
-    v.t[T_NE] += v.t[T_EDGE];
-    v.t[T_F0] += v.t[T_F];
-    v.t[T_F] = v.t[T_NEW];
-    v.t[T_LEVELS] += 1;
+    if (v.t[T_GO]) level_end(v);
   }
 };
 
@@ -755,8 +763,10 @@ struct LevelEndF {
 //   void gen_heavy(const View &, const unsigned long long *go);  (the positions CountF queued in v.hq)
 //   each_d / scan_d / scan3_d: the same with the item count read on the device
 //     (*n), doing nothing while *go == 0 (a stalled or finished loop);
-//   begin_capture / end_capture / run_graph / has_graph / drop_graph: one
-//     level recorded once and replayed (a CUDA graph on the device).
+//   begin_capture / end_capture(go) / run_graph(limit) / note_levels /
+//     has_graph / drop_graph: one level recorded once and run repeatedly
+//     (on the device a CUDA graph WHILE node: up to `limit` levels per launch,
+//     stopping as soon as *go == 0).
 //   bool ok();                                             (no backend error so far)
 struct Totals {
   Ctl ctl;
@@ -1099,7 +1109,9 @@ class Builder {
           !ensure_sets(h_tot_.ctl.n_sets, h_tot_.ctl.sdata_top, guess, guess) || !ensure_nodes(newN, guess, 0, guess))
         return 1;
     }
-    uint32_t batch = 4;
+    // levels per graph launch: the loop stops by itself when the frontier
+    // runs empty or a level stalls; the limit only bounds one launch
+    const uint32_t batch = 4096;
     unsigned long long last_stall = ~0ull;
     uint32_t same_stall = 0;
     for (;;) {
@@ -1107,15 +1119,17 @@ class Builder {
       if (!be_.has_graph()) {
         be_.begin_capture();
         enqueue_level();
-        be_.end_capture();
+        be_.end_capture(tp(T_GO));
       }
-      for (uint32_t k = 0; k < batch; k++) be_.run_graph();
+      const unsigned long long levels_before = h_tot_.t[T_LEVELS];
+      be_.run_graph(batch);  // up to `batch` levels, fewer when the loop stops
       if (!fetch_totals()) return 1;
+      be_.note_levels(h_tot_.t[T_LEVELS] - levels_before + (h_tot_.t[T_STALL] ? 1 : 0));
       if (h_tot_.ctl.err & ERR_COLLISION) return 3;
       if (h_tot_.ctl.err) return 2;
       if (h_tot_.t[T_DONE]) break;
       if (!h_tot_.t[T_STALL]) {
-        batch = std::min<uint32_t>(batch * 2, 64);
+        if (h_tot_.t[T_LEVELS] == levels_before) return 2;  // no progress without a stall: a defect
         continue;
       }
       // grow to the stalled level's needs (its bounds were counted, or the
@@ -1136,7 +1150,6 @@ class Builder {
       h_tot_.t[T_GO] = 1;
       h_tot_.t[T_STALL] = 0;
       be_.copy(&d_tot_->t[T_GO], &h_tot_.t[T_GO], 2 * sizeof(unsigned long long));
-      batch = 1;
     }
     be_.drop_graph();
     v_.t = d_tot_->t;
