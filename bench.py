@@ -57,6 +57,9 @@ def parse():
                     help="build, upload and solve only (the command profiled with ncu)")
     ap.add_argument("--build-only", action="store_true",
                     help="one device GameBuild of the batch's minimised LTSs only (profiled with ncu)")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="with --build-only: levels as plain launches (ncu does not profile kernels of a graph "
+                         "with conditional nodes)")
     return ap.parse_args()
 
 
@@ -414,6 +417,9 @@ def run_build_only(args, d: Dist):
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         jobs = list(ex.map(prep, seeds))
     ctx = geq.Context(d.local_rank)
+    if args.no_graph:
+        from gpuequiv_b200._lib import TUNE_NO_GRAPH
+        ctx.set_tuning(flags=TUNE_NO_GRAPH)
     b = geq.GameBatch(jobs, context=ctx)
     if d.rank == 0:
         print(json.dumps({"build_only": True, "jobs": len(jobs), "stats": b.stats}), flush=True)

@@ -105,61 +105,11 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_down(const uint32_t *in, uint32
     }
 }
 
-// Three scans at once (the bounds of CountF), same tiling as above.
+// Three arrays scanned in one pass (the bounds of CountF).
 struct Scan3 {
   const uint32_t *in[3];
   uint32_t *out[3];
 };
-__global__ void __launch_bounds__(SCAN_T) k_scan3_up(Scan3 a, uint32_t n, unsigned long long *part, uint32_t nb) {
-  const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
-#pragma unroll
-  for (int r = 0; r < 3; r++) {
-    unsigned long long s = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++)
-      if (base + k < n) s += a.in[r][base + k];
-    unsigned long long total;
-    block_scan(s, total);
-    if (threadIdx.x == 0) part[r * nb + blockIdx.x] = total;
-  }
-}
-__global__ void __launch_bounds__(SCAN_T) k_scan3_mid(unsigned long long *part, uint32_t nb, unsigned long long *tot) {
-  for (int r = 0; r < 3; r++) {
-    unsigned long long carry = 0;
-    for (uint32_t b0 = 0; b0 < nb; b0 += SCAN_T) {
-      const uint32_t i = b0 + threadIdx.x;
-      const unsigned long long x = i < nb ? part[r * nb + i] : 0ull;
-      unsigned long long total;
-      const unsigned long long e = block_scan(x, total);
-      if (i < nb) part[r * nb + i] = carry + e;
-      carry += total;
-    }
-    if (threadIdx.x == 0) tot[r] = carry;
-  }
-}
-__global__ void __launch_bounds__(SCAN_T) k_scan3_down(Scan3 a, uint32_t n, const unsigned long long *part,
-                                                       uint32_t nb) {
-  const uint32_t base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
-#pragma unroll
-  for (int r = 0; r < 3; r++) {
-    uint32_t v[SCAN_ITEMS];
-    unsigned long long s = 0;
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++) {
-      v[k] = base + k < n ? a.in[r][base + k] : 0u;
-      s += v[k];
-    }
-    unsigned long long total;
-    unsigned long long e = block_scan(s, total) + part[r * nb + blockIdx.x];
-#pragma unroll
-    for (int k = 0; k < SCAN_ITEMS; k++)
-      if (base + k < n) {
-        a.out[r][base + k] = (uint32_t)e;
-        e += v[k];
-      }
-  }
-}
-
 // Scans of R arrays whose length is read on the device: a fixed grid of nb
 // blocks, block b scanning the contiguous chunk b of ceil(n / nb) values tile
 // by tile (reduce, scan of the nb block sums, rescan with the block's carry).
@@ -470,25 +420,6 @@ struct DevBackend {
     k_scan_down<<<nb, SCAN_T, 0, s>>>(in, n, part, out);
     launches += 3;
   }
-  void scan3(const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, uint32_t *o0, uint32_t *o1, uint32_t *o2,
-             uint32_t n, unsigned long long *tot) {
-    const uint32_t nb = std::max<uint32_t>(1, (n + SCAN_TILE - 1) / SCAN_TILE);
-    if (3 * nb > part_cap) {
-      release(part);
-      part_cap = std::max<uint32_t>(3 * nb, 1024);
-      part = (unsigned long long *)alloc((size_t)part_cap * 8);
-      if (!part) {
-        part_cap = 0;
-        note(cudaErrorMemoryAllocation);
-        return;
-      }
-    }
-    const Scan3 a{{i0, i1, i2}, {o0, o1, o2}};
-    k_scan3_up<<<nb, SCAN_T, 0, s>>>(a, n, part, nb);
-    k_scan3_mid<<<1, SCAN_T, 0, s>>>(part, nb, tot);
-    k_scan3_down<<<nb, SCAN_T, 0, s>>>(a, n, part, nb);
-    launches += 3;
-  }
   void gen_heavy(const View &v, const unsigned long long *go) {
     if (v.heavy_min == 0xffffffffu) return;
     k_gen_heavy<<<(unsigned)n_sms * 2, GH_WARPS * 32, 0, s>>>(v, go);
@@ -541,9 +472,11 @@ struct DevBackend {
   uint32_t *d_loop = nullptr;  // [levels run in this launch, limit]
   uint32_t h_loop[2] = {0, 0};
   uint32_t graph_launches = 0, mark = 0;
+  bool plain = false;  // levels as plain launches, one per host sync (profilers see every kernel)
   bool has_graph() const { return gexec != nullptr; }
   void begin_capture() {
     reserve_part();
+    if (plain) return;  // the level that "capture" enqueues runs as it is
     if (!d_loop) d_loop = (uint32_t *)alloc(2 * sizeof(uint32_t));
     if (!d_loop) note(cudaErrorMemoryAllocation);
     mark = launches;
@@ -560,6 +493,7 @@ struct DevBackend {
     note(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   }
   void end_capture(const unsigned long long *go) {
+    if (plain) return;
     k_level_cond<<<1, 1, 0, s>>>(cond, go, d_loop);
     note(cudaStreamEndCapture(s, &body));
     graph_launches = launches - mark;
@@ -664,6 +598,9 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
   gb::DevBackend &be = db.be;
   be.s = (cudaStream_t)eng.stream_handle();
   be.n_sms = eng.n_sms;
+  // GEQ_TUNE_NO_GRAPH: levels as plain launches (ncu does not profile the
+  // kernels of a graph with conditional nodes)
+  be.plain = (eng.tuning.flags & GEQ_TUNE_NO_GRAPH) != 0;
   // stage the LTSs: soff | slab | stgt | sjob | p0 | q0
   const auto t0 = clk::now();
   const size_t o_soff = 0, o_slab = o_soff + (NS + 1) * 4, o_stgt = o_slab + MS * 4, o_sjob = o_stgt + MS * 4,

@@ -292,7 +292,7 @@ typedef struct geq_tuning {
 } geq_tuning;
 #define GEQ_TUNE_FORCE_GENERIC 1u /* generic codec even for STANDARD (cross-check) */
 #define GEQ_TUNE_FORCE_LARGE 2u   /* bypass the register paths (cross-check) */
-#define GEQ_TUNE_NO_GRAPH 4u      /* launch rounds one by one instead of graphs */
+#define GEQ_TUNE_NO_GRAPH 4u      /* launch rounds (and GameBuild levels) one by one instead of graphs */
 #define GEQ_TUNE_PROFILE 8u       /* time every round-kernel launch (implies no graphs) */
 #define GEQ_TUNE_NO_THREAD_PATH 16u /* no lane-per-position path (cross-check) */
 #define GEQ_TUNE_NO_SPLIT 32u     /* a large batch on one engine, not as two pipelined halves */

@@ -69,8 +69,10 @@ def test_random_vs_oracle(geq, ctx, seed):
         assert_same(g, arrays(geq.GameBuild.compare(lts, p, q).game), f"job {j}")
 
 
-def test_batched_workload_vs_host(geq, ctx):
-    """Minimised LTSs of the batched configuration (every 32nd accepted seed)."""
+@pytest.mark.parametrize("flags", [0, 4], ids=["graph_loop", "plain_launches"])
+def test_batched_workload_vs_host(geq, ctx, flags):
+    """Minimised LTSs of the batched configuration (every 32nd accepted seed),
+    with the level loop in a CUDA graph and as plain launches (GEQ_TUNE_NO_GRAPH)."""
     from gpuequiv_b200 import synth
     rows = synth.batched_manifest()["jobs"][::32]
     jobs = []
@@ -78,7 +80,11 @@ def test_batched_workload_vs_host(geq, ctx):
         src, dst, lab, p, q = synth.batched_lts(seed)
         red, mp = geq.TransitionSystem.from_arrays(src, dst, lab).bisimilar_minimize()
         jobs.append((red, int(mp[p]), int(mp[q]), npos))
-    b = geq.GameBatch([j[:3] for j in jobs], context=ctx)
+    try:
+        ctx.set_tuning(flags=flags)
+        b = geq.GameBatch([j[:3] for j in jobs], context=ctx)
+    finally:
+        ctx.set_tuning(flags=0)
     assert b.stats["attempts"] == 1
     assert b.stats["positions"] == sum(j[3] for j in jobs)
     for k, (red, p, q, npos) in enumerate(jobs):
