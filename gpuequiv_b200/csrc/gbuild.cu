@@ -1,7 +1,13 @@
-// gbuild.cu - the device game builder (gbuild.cuh) on the CUDA stream of a
-// context: GameBuild::compare (src/gamebuild.rs:165-170) for a batch of
-// (LTS, p, q) jobs, one breadth-first level per group of launches, results
-// copied back as one CSR game graph per job.
+// gbuild.cu - the device game builder (gbuild.cuh) and the device
+// minimisation (refine.cuh) on the CUDA stream of a context:
+// GameBuild::compare (src/gamebuild.rs:165-170) for a batch of (LTS, p, q)
+// jobs, one breadth-first level per pass over the level kernels (all levels
+// inside one CUDA graph WHILE node), results either copied back as one CSR
+// game graph per job (geq_game_build_compare_batch) or handed to the solver
+// on the device (build_and_upload, used by geq_compare_batch, the serving
+// loop's queries and geq_equivalences); and
+// TransitionSystem::signature_refinement of many systems at once
+// (geq_lts_signature_refinement_batch).
 #include <cuda_runtime.h>
 
 #include <chrono>
