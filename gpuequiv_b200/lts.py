@@ -9,7 +9,7 @@ import numpy as np
 
 from ._lib import check, geq_game_batch_info, geq_game_graph, geq_position, lib
 from .energy import Energy, EnergyArray, EnergyConf
-from .energygame import Context, GameGraph, _lists_from_solution, _stats_of, default_context
+from .energygame import Context, GameGraph, _stats_of, default_context
 
 _u32 = C.POINTER(C.c_uint32)
 _i32 = C.POINTER(C.c_int32)
@@ -155,10 +155,19 @@ def compare_batch(jobs: Sequence[tuple[TransitionSystem, int, int]], context: Co
     sol = C.c_void_p()
     check(lib.geq_compare_batch(ctx.h, n, hs, _p(ps, _u32), _p(qs, _u32), 1 if minimize else 0, C.byref(sol)))
     try:
-        out = [_lists_from_solution(sol, i, EnergyConf.STANDARD)[0] for i in range(n)]
+        # all games' lists at once: game i has one position, offsets (0, count_i)
+        po, pd = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+        no, nw = C.c_uint64(), C.c_uint64()
+        check(lib.geq_solution_flat(sol, C.byref(po), C.byref(no), C.byref(pd), C.byref(nw)))
+        offs = np.ctypeslib.as_array(po, shape=(no.value,)).astype(np.int64) if no.value else np.zeros(0, np.int64)
+        data = np.ctypeslib.as_array(pd, shape=(nw.value,)).copy() if nw.value else np.zeros(0, np.uint32)
         stats = _stats_of(sol)
     finally:
         lib.geq_solution_free(sol)
+    base = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(offs[1::2][:n], out=base[1:])
+    bl = base.tolist()
+    out = [EnergyArray(data[bl[i]:bl[i + 1]].reshape(-1, 1), EnergyConf.STANDARD) for i in range(n)]
     return (out, stats) if return_stats else out
 
 
