@@ -166,7 +166,10 @@ _SIGS = {
     "geq_game_build_free": ([vp], None),
     "geq_game_build_compare_batch": ([vp, C.c_uint32, C.POINTER(vp), u32p, u32p, C.c_uint64, C.POINTER(vp)],
                                      C.c_int),
+    "geq_game_build_starts_batch": ([vp, C.c_uint32, C.POINTER(vp), u32p, u32p, u32p, C.c_uint64, C.POINTER(vp)],
+                                    C.c_int),
     "geq_game_batch_n_jobs": ([vp], C.c_uint32),
+    "geq_game_batch_n_starting_points": ([vp, C.c_uint32], C.c_uint32),
     "geq_game_batch_graph": ([vp, C.c_uint32, C.POINTER(geq_game_graph)], C.c_int),
     "geq_game_batch_stats": ([vp, C.POINTER(geq_game_batch_info)], None),
     "geq_game_batch_free": ([vp], None),

@@ -766,7 +766,7 @@ using namespace geq;
 
 struct geq_game_batch {
   uint32_t n_jobs = 0;
-  std::vector<uint32_t> node_base, edge_base, n_nodes, n_edges;
+  std::vector<uint32_t> node_base, edge_base, n_nodes, n_edges, n_starts;
   std::vector<uint8_t> over;
   HostBuf row, col, wt, att;
   uint64_t N = 0, M = 0;
@@ -774,27 +774,49 @@ struct geq_game_batch {
   double upload_ms = 0, build_ms = 0, download_ms = 0;
 };
 
+static geq_status build_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts, const uint32_t *start_off,
+                              const uint32_t *p, const uint32_t *q, uint64_t max_positions, geq_game_batch **out);
+
 extern "C" geq_status geq_game_build_compare_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts,
                                                    const uint32_t *p, const uint32_t *q, uint64_t max_positions,
                                                    geq_game_batch **out) {
+  if (!out || !lts || !p || !q) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  std::vector<uint32_t> start_off(n_jobs + 1);
+  for (uint32_t j = 0; j <= n_jobs; j++) start_off[j] = j;
+  return build_batch(ctx, n_jobs, lts, start_off.data(), p, q, max_positions, out);
+}
+
+extern "C" geq_status geq_game_build_starts_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts,
+                                                  const uint32_t *start_off, const uint32_t *p, const uint32_t *q,
+                                                  uint64_t max_positions, geq_game_batch **out) {
+  if (!out || !lts || !start_off) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  if (n_jobs && start_off[0] != 0) return fail(GEQ_ERR_INVALID_INPUT, "start_off[0] must be 0");
+  for (uint32_t j = 0; j < n_jobs; j++)
+    if (start_off[j + 1] < start_off[j]) return fail(GEQ_ERR_INVALID_INPUT, "start_off must not decrease");
+  if (n_jobs && start_off[n_jobs] && (!p || !q)) return fail(GEQ_ERR_INVALID_INPUT, "NULL start arrays");
+  return build_batch(ctx, n_jobs, lts, start_off, p, q, max_positions, out);
+}
+
+static geq_status build_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts, const uint32_t *start_off,
+                              const uint32_t *p, const uint32_t *q, uint64_t max_positions, geq_game_batch **out) {
   using clk = std::chrono::steady_clock;
   if (!ctx || !ctx->engine) return fail(GEQ_ERR_INVALID_INPUT, "context is NULL");
-  if (!out || !lts || !p || !q) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
   *out = nullptr;
   if (n_jobs == 0) return fail(GEQ_ERR_INVALID_INPUT, "no jobs");
   std::vector<const Lts *> L(n_jobs);
   for (uint32_t j = 0; j < n_jobs; j++) {
     if (!lts[j]) return fail(GEQ_ERR_INVALID_INPUT, "job %u: LTS is NULL", j);
     L[j] = &lts[j]->l;
-    if (p[j] >= L[j]->n || q[j] >= L[j]->n) return fail(GEQ_ERR_INVALID_INPUT, "job %u: process out of range", j);
+    for (uint32_t t = start_off[j]; t < start_off[j + 1]; t++)
+      if (p[t] >= L[j]->n || q[t] >= L[j]->n) return fail(GEQ_ERR_INVALID_INPUT, "job %u: process out of range", j);
   }
   Engine &eng = *ctx->engine;
   std::unique_ptr<geq_game_batch> res(new geq_game_batch());
   res->n_jobs = n_jobs;
+  res->n_starts.resize(n_jobs);
+  for (uint32_t j = 0; j < n_jobs; j++) res->n_starts[j] = start_off[j + 1] - start_off[j];
   DeviceBuild db;
-  std::vector<uint32_t> start_off(n_jobs + 1);
-  for (uint32_t j = 0; j <= n_jobs; j++) start_off[j] = j;
-  geq_status st = device_build(eng, ctx->device, n_jobs, L.data(), start_off.data(), p, q, max_positions, db);
+  geq_status st = device_build(eng, ctx->device, n_jobs, L.data(), start_off, p, q, max_positions, db);
   if (st) return st;
   // per-job CSR back to the host
   const auto t2 = clk::now();
@@ -891,6 +913,10 @@ extern "C" void geq_game_batch_stats(const geq_game_batch *b, geq_game_batch_inf
   out->upload_ms = b->upload_ms;
   out->build_ms = b->build_ms;
   out->download_ms = b->download_ms;
+}
+
+extern "C" uint32_t geq_game_batch_n_starting_points(const geq_game_batch *b, uint32_t job) {
+  return b && job < b->n_jobs ? b->n_starts[job] : 0;
 }
 
 extern "C" void geq_game_batch_free(geq_game_batch *b) { delete b; }

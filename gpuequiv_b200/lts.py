@@ -298,10 +298,54 @@ class GameBatch:
         h = C.c_void_p()
         check(lib.geq_game_build_compare_batch(ctx.h, n, hs, _p(ps, _u32), _p(qs, _u32), int(max_positions),
                                                C.byref(h)))
+        self._adopt(h)
+
+    def _adopt(self, h):
         self.h = h
         info = geq_game_batch_info()
         lib.geq_game_batch_stats(h, C.byref(info))
         self.stats = info.as_dict()
+
+    @classmethod
+    def with_starts(cls, systems: Sequence[TransitionSystem], starts: Sequence[Sequence[tuple[int, int]]],
+                    context: Context | None = None, max_positions: int = 0) -> "GameBatch":
+        """Job j is the game of systems[j] from the start positions
+        Attack(p, {q}) for (p, q) in starts[j], numbered in that order (the
+        start layout of GameBuild::compare_multiple / compare_all,
+        gamebuild.rs:176-215); geq_game_build_starts_batch."""
+        ctx = context or default_context()
+        n = len(systems)
+        hs = (C.c_void_p * max(n, 1))(*[s.h.value for s in systems])
+        off = np.zeros(n + 1, dtype=np.uint32)
+        np.cumsum([len(x) for x in starts], out=off[1:])
+        flat = [pq for x in starts for pq in x]
+        ps = np.array([pq[0] for pq in flat] or [0], dtype=np.uint32)
+        qs = np.array([pq[1] for pq in flat] or [0], dtype=np.uint32)
+        h = C.c_void_p()
+        check(lib.geq_game_build_starts_batch(ctx.h, n, hs, _p(off, _u32), _p(ps, _u32), _p(qs, _u32),
+                                              int(max_positions), C.byref(h)))
+        b = cls.__new__(cls)
+        b._adopt(h)
+        return b
+
+    @classmethod
+    def compare_all(cls, systems: Sequence[TransitionSystem], context: Context | None = None,
+                    max_positions: int = 0) -> "GameBatch":
+        """GameBuild::compare_all (gamebuild.rs:200-215) of each system on the
+        device: every ordered pair of distinct processes with the same enabled
+        labels, classes in order of their first process."""
+        starts = []
+        for lts in systems:
+            off, _, lb = lts.inner()
+            classes: dict = {}
+            for p in range(lts.n_vertices()):
+                key = tuple(sorted(set(int(x) for x in lb[int(off[p]):int(off[p + 1])])))
+                classes.setdefault(key, []).append(p)
+            starts.append([(p, q) for c in classes.values() for p in c for q in c if p != q])
+        return cls.with_starts(systems, starts, context, max_positions)
+
+    def n_starting_points(self, j: int) -> int:
+        return lib.geq_game_batch_n_starting_points(self.h, int(j))
 
     def __len__(self):
         return lib.geq_game_batch_n_jobs(self.h)

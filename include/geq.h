@@ -374,7 +374,18 @@ typedef struct geq_game_batch geq_game_batch;
 geq_status geq_game_build_compare_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts,
                                         const uint32_t *p, const uint32_t *q, uint64_t max_positions,
                                         geq_game_batch **out);
+/* The same with any start positions: job j starts from Attack(p[t], {q[t]}) for
+ * t in start_off[j] .. start_off[j+1]-1 (start_off has n_jobs + 1 entries,
+ * start_off[0] = 0), numbered 0.. in that order, as GameBuild::new_node does
+ * for compare_multiple / compare_all (gamebuild.rs:176-215; the start pairs of
+ * compare_all are every ordered pair of distinct processes inside each
+ * enabledness class, classes in order of their first process).  The start
+ * positions of one job must be distinct. */
+geq_status geq_game_build_starts_batch(geq_context *ctx, uint32_t n_jobs, const geq_lts *const *lts,
+                                       const uint32_t *start_off, const uint32_t *p, const uint32_t *q,
+                                       uint64_t max_positions, geq_game_batch **out);
 uint32_t geq_game_batch_n_jobs(const geq_game_batch *b);
+uint32_t geq_game_batch_n_starting_points(const geq_game_batch *b, uint32_t job);
 /* Job's GameGraph (borrowed view, STANDARD conf). */
 geq_status geq_game_batch_graph(const geq_game_batch *b, uint32_t job, geq_game_graph *out);
 typedef struct geq_game_batch_info {

@@ -156,3 +156,26 @@ def test_bad_input(geq, ctx):
     assert ei.value.status == 3
     with pytest.raises(geq.GeqError):
         geq.GameBatch([], context=ctx)
+
+
+def test_compare_all_vs_host(geq, ctx):
+    """GameBuild::compare_all on the device (many start positions per job)
+    against the host builder and the oracle: same start numbering, CSR and
+    weights."""
+    rng = np.random.default_rng(21)
+    systems, edges_of = [], []
+    for _ in range(12):
+        n = int(rng.integers(2, 9))
+        edges = random_lts(rng, n, 2, int(rng.integers(n, 2 * n + 1)))
+        systems.append(geq.TransitionSystem(edges))
+        edges_of.append(edges)
+    systems.append(geq.TransitionSystem(G.EXAMPLE_LTS))
+    edges_of.append(G.EXAMPLE_LTS)
+    b = geq.GameBatch.compare_all(systems, context=ctx, max_positions=2_000_000)
+    for j, lts in enumerate(systems):
+        host, info = geq.GameBuild.compare_all(lts)
+        assert b.n_starting_points(j) == host.n_starting_points
+        assert_same(arrays(b.graph(j)), arrays(host.game), f"job {j}")
+        ob = ora.Build.compare_all(ora.Lts.from_edges(edges_of[j]))
+        assert ob.n_starting == host.n_starting_points
+        assert_same(arrays(b.graph(j)), (ob.row, ob.col, ob.wt, ob.attacker), f"job {j} (oracle)")
