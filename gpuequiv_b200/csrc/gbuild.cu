@@ -13,6 +13,7 @@
 #include <chrono>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
 
 #include "gbuild.cuh"
 #include "refine.cuh"
@@ -702,7 +703,19 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
   }
   const auto t1 = clk::now();
   db.b.reset(new gb::Builder<gb::DevBackend>(be));
+  // start from the capacities the previous build on this stream ended with
+  static std::mutex hint_mu;
+  static std::unordered_map<void *, gb::Builder<gb::DevBackend>::Caps> hints;
+  {
+    std::lock_guard<std::mutex> g(hint_mu);
+    auto it = hints.find((void *)be.s);
+    if (it != hints.end()) db.b->hint = it->second;
+  }
   const int rc = db.b->run(bin, db.r);
+  if (rc == 0) {
+    std::lock_guard<std::mutex> g(hint_mu);
+    hints[(void *)be.s] = db.b->used;
+  }
   db.upload_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
   db.build_ms = std::chrono::duration<double, std::milli>(clk::now() - t1).count();
   if (!be.ok()) return fail(GEQ_ERR_CUDA, "device game build: %s", cudaGetErrorString(be.err));

@@ -809,6 +809,13 @@ class Builder {
     }
     return 3;
   }
+  // Capacities to start from (a hint, e.g. those of the previous build on
+  // the same stream: a serving loop's batches then rarely stall for buffers)
+  // and those a successful build ended with.
+  struct Caps {
+    uint32_t F = 0, S = 0, E = 0, C = 0, sets = 0, sdata = 0, nodes = 0, edges = 0;
+  };
+  Caps hint, used;
   // device buffers of the result stay owned by the builder until it dies
   // After a failure: the request that could not be met (elements or bytes),
   // and the positions / edges / levels reached.
@@ -824,6 +831,7 @@ class Builder {
     size_t bytes = 0;
   };
   std::vector<Buf> bufs_;
+  bool exact_ = false;
   template <class T>
   T *get(size_t n) {
     const size_t b = (n ? n : 1) * sizeof(T);
@@ -850,7 +858,9 @@ class Builder {
   template <class T>
   bool grow(T *&p, uint32_t &cap, uint64_t need, uint64_t keep) {
     if (need <= cap) return true;
-    uint64_t nc = std::max<uint64_t>(2 * need, 1024);  // doubling: few stalls of the level loop
+    // doubling: few stalls of the level loop (exact while capacities from a
+    // hint are applied, so that hints do not grow from build to build)
+    uint64_t nc = exact_ ? need : std::max<uint64_t>(2 * need, 1024);
     if (nc > 0xffffffffull) nc = need;
     if (nc > 0xffffffffull) {
       short_ = need;
@@ -945,7 +955,10 @@ class Builder {
     v_.stab = get<unsigned long long>(cap);
     v_.sval = get<uint32_t>(cap);
     v_.sclaim = get<uint32_t>(cap);
-    if (!v_.stab || !v_.sval || !v_.sclaim) return false;
+    if (!v_.stab || !v_.sval || !v_.sclaim) {
+      short_ = cap * 16;
+      return false;
+    }
     be_.fill(v_.stab, 0, cap * 8);
     be_.fill(v_.sval, 0xff, cap * 4);
     be_.fill(v_.sclaim, 0xff, cap * 4);
@@ -981,7 +994,10 @@ class Builder {
     v_.ntab = get<unsigned long long>(cap);
     v_.nval = get<uint32_t>(cap);
     v_.nclaim = get<uint32_t>(cap);
-    if (!v_.ntab || !v_.nval || !v_.nclaim) return false;
+    if (!v_.ntab || !v_.nval || !v_.nclaim) {
+      short_ = cap * 16;
+      return false;
+    }
     be_.fill(v_.ntab, 0, cap * 8);
     be_.fill(v_.nval, 0xff, cap * 4);
     be_.fill(v_.nclaim, 0xff, cap * 4);
@@ -1103,10 +1119,17 @@ class Builder {
     // buffers grow to its exact needs
     {
       const uint64_t guess = 8ull * newN + 4096;
-      if (!ensure_frontier(std::max<uint32_t>(newN, 4096)) ||
-          !ensure_level((uint32_t)guess, (uint32_t)guess, (uint32_t)guess) ||
-          !ensure_sets(h_tot_.ctl.n_sets, h_tot_.ctl.sdata_top, guess, guess) || !ensure_nodes(newN, guess, 0, guess))
-        return 1;
+      auto mx = [&](uint32_t h) { return (uint32_t)std::max<uint64_t>(guess, h); };
+      const uint32_t n_sets = h_tot_.ctl.n_sets, top = h_tot_.ctl.sdata_top;
+      exact_ = true;
+      const bool ok =
+          ensure_frontier(std::max<uint32_t>(std::max<uint32_t>(newN, 4096), hint.F)) &&
+          ensure_level(mx(hint.S), mx(hint.E), mx(hint.C)) &&
+          ensure_sets(n_sets, top, std::max<uint64_t>(guess, hint.sets > n_sets ? hint.sets - n_sets : 0),
+                      std::max<uint64_t>(guess, hint.sdata > top ? hint.sdata - top : 0)) &&
+          ensure_nodes(newN, std::max<uint64_t>(guess, hint.nodes > newN ? hint.nodes - newN : 0), 0, mx(hint.edges));
+      exact_ = false;
+      if (!ok) return 1;
     }
     // levels per graph launch: the loop stops by itself when the frontier
     // runs empty or a level stalls; the limit only bounds one launch
@@ -1181,6 +1204,7 @@ class Builder {
     be_.each(J, RowEndF{v_, o});
     if (!fetch_totals()) return 1;
     if (h_tot_.t[T_N] != N || h_tot_.t[T_EDGE] != M || h_tot_.ctl.err) return 2;
+    used = Caps{capF_, capS_, capE_, capC_, capSets_, capSdata_, capNodes_, capEdges_};
     out.N = N;
     out.M = M;
     out.levels = levels;
