@@ -1122,14 +1122,19 @@ class Builder {
       auto mx = [&](uint32_t h) { return (uint32_t)std::max<uint64_t>(guess, h); };
       const uint32_t n_sets = h_tot_.ctl.n_sets, top = h_tot_.ctl.sdata_top;
       exact_ = true;
-      const bool ok =
+      bool ok =
           ensure_frontier(std::max<uint32_t>(std::max<uint32_t>(newN, 4096), hint.F)) &&
           ensure_level(mx(hint.S), mx(hint.E), mx(hint.C)) &&
           ensure_sets(n_sets, top, std::max<uint64_t>(guess, hint.sets > n_sets ? hint.sets - n_sets : 0),
                       std::max<uint64_t>(guess, hint.sdata > top ? hint.sdata - top : 0)) &&
           ensure_nodes(newN, std::max<uint64_t>(guess, hint.nodes > newN ? hint.nodes - newN : 0), 0, mx(hint.edges));
       exact_ = false;
+      if (!ok)  // the hint asked for more than the device has now: start small
+        ok = ensure_frontier(std::max<uint32_t>(newN, 4096)) &&
+             ensure_level((uint32_t)guess, (uint32_t)guess, (uint32_t)guess) &&
+             ensure_sets(n_sets, top, guess, guess) && ensure_nodes(newN, guess, 0, guess);
       if (!ok) return 1;
+      short_ = 0;
     }
     // levels per graph launch: the loop stops by itself when the frontier
     // runs empty or a level stalls; the limit only bounds one launch
