@@ -280,6 +280,18 @@ class GameBuild:
         return b, StartInfo(b.starting_points(), lts.n_vertices())
 
 
+def compare_all_starts(lts: TransitionSystem) -> list[tuple[int, int]]:
+    """Start pairs of GameBuild::compare_all (gamebuild.rs:104-133, :200-215):
+    every ordered pair of distinct processes with the same set of enabled
+    labels, the classes in order of their first process."""
+    off, _, lb = lts.inner()
+    classes: dict = {}
+    for p in range(lts.n_vertices()):
+        key = tuple(sorted(set(int(x) for x in lb[int(off[p]):int(off[p + 1])])))
+        classes.setdefault(key, []).append(p)
+    return [(p, q) for c in classes.values() for p in c for q in c if p != q]
+
+
 class GameBatch:
     """GameBuild::compare (gamebuild.rs:165-170) for many (lts, p, q) jobs,
     built on the device one breadth-first level of all games at a time
@@ -334,15 +346,7 @@ class GameBatch:
         """GameBuild::compare_all (gamebuild.rs:200-215) of each system on the
         device: every ordered pair of distinct processes with the same enabled
         labels, classes in order of their first process."""
-        starts = []
-        for lts in systems:
-            off, _, lb = lts.inner()
-            classes: dict = {}
-            for p in range(lts.n_vertices()):
-                key = tuple(sorted(set(int(x) for x in lb[int(off[p]):int(off[p + 1])])))
-                classes.setdefault(key, []).append(p)
-            starts.append([(p, q) for c in classes.values() for p in c for q in c if p != q])
-        return cls.with_starts(systems, starts, context, max_positions)
+        return cls.with_starts(systems, [compare_all_starts(lts) for lts in systems], context, max_positions)
 
     def n_starting_points(self, j: int) -> int:
         return lib.geq_game_batch_n_starting_points(self.h, int(j))

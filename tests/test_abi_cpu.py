@@ -185,6 +185,23 @@ def test_gamebuild_compare_all_vs_oracle(geq, seed):
     assert np.array_equal(b.game.column_indices, ob.col)
 
 
+@pytest.mark.parametrize("seed", range(5))
+def test_compare_all_start_pairs(geq, seed):
+    """The start pairs the device build of compare_all is given
+    (lts.compare_all_starts) are the host builder's start positions, in order,
+    and the oracle's."""
+    from gpuequiv_b200.lts import compare_all_starts
+    rng = np.random.default_rng(90 + seed)
+    edges = random_lts(rng, int(rng.integers(5, 30)), 3, int(rng.integers(10, 60)))
+    lts = geq.TransitionSystem(edges)
+    pairs = compare_all_starts(lts)
+    b, _ = geq.GameBuild.compare_all(lts)
+    starts = [(int(x[1]), tuple(int(v) for v in x[2])) for x in b.nodes[:b.n_starting_points]]
+    assert [(p, (q,)) for p, q in pairs] == starts
+    ob = ora.Build.compare_all(ora.Lts.from_edges(edges))
+    assert [(p, (q,)) for p, q in pairs] == [(pos[1], pos[2]) for pos in ob.positions[:ob.n_starting]]
+
+
 def test_gamebuild_bounded(geq):
     lts = geq.TransitionSystem(G.EXAMPLE_LTS)
     with pytest.raises(geq.GeqError) as e:
