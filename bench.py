@@ -365,12 +365,23 @@ def run_lts_pipeline(ctx, seeds, graphs, args, d: Dist) -> dict:
     with ThreadPoolExecutor(max_workers=threads) as ex:
         list(ex.map(lambda j: geq.GameBuild.compare(*j), reds))
     host_build_ms = (time.perf_counter() - t) * 1e3
+    # the plain form: one compare() call per query (every 32nd job)
+    sample = jobs[::32]
+    for j in sample[:8]:
+        geq.compare_batch([j], context=ctx)
+    t = time.perf_counter()
+    for j in sample:
+        geq.compare_batch([j], context=ctx)
+    plain_q = len(sample) / (time.perf_counter() - t)
     return jobs, {"workload": "compare_batch over the same 4096 LTSs (unminimised): device minimisation, device GameBuild, "
                         "batched solve, start energies read back",
             "games_s": d.sum(len(jobs)) / pipe_s, "ms_per_step": pipe_s * 1e3,
             "device_build_ms": float(np.median(dev_build)), "build_levels": b.stats["levels"],
             "build_kernel_launches": b.stats["kernel_launches"],
-            "host_build_ms_all_cores": host_build_ms, "host_threads": threads}
+            "host_build_ms_all_cores": host_build_ms, "host_threads": threads,
+            "plain_per_query": {"value": plain_q, "unit": UNIT,
+                                "sample": f"{len(sample)} jobs (every 32nd), one compare() call each"},
+            "batched_vs_plain_per_query": (d.sum(len(jobs)) / pipe_s) / plain_q if plain_q else None}
 
 
 def run_reference(args, d: Dist):
