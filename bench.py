@@ -49,9 +49,17 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--plain-sample", type=int, default=256)
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch shape)")
-    ap.add_argument("--serve-rates", default="1000,5000",
-                    help="Poisson arrival rates (req/s) of the serving leg; empty: no serving leg")
-    ap.add_argument("--serve-seconds", type=float, default=3.0, help="arrivals per serving rate (s)")
+    ap.add_argument("--serve-rates", default="5000,20000",
+                    help="Poisson arrival rates (req/s) of the game-request serving leg; empty: none")
+    ap.add_argument("--query-rates", default="200,1000,5000",
+                    help="Poisson arrival rates (req/s) of the serving configuration (equivalence queries on LTSs "
+                         "of 20-20,000 states); empty: none")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrivals per serving rate (s)")
+    ap.add_argument("--saturation-seconds", type=float, default=6.0,
+                    help="closed-loop saturation run of each serving leg (s); 0: none")
+    ap.add_argument("--query-bound", type=int, default=200_000,
+                    help="position bound of a served query's game (larger games are refused)")
+    ap.add_argument("--query-pool", type=int, default=2048, help="distinct queries the arrivals draw from")
     ap.add_argument("--no-stress", dest="stress", action="store_false", help="skip the stress-game leg")
     ap.add_argument("--solve-only", action="store_true",
                     help="build, upload and solve only (the command profiled with ncu)")
@@ -222,22 +230,55 @@ def build_games_oracle(seeds):
     return games
 
 
+def canonical(offsets, data):
+    """Every position's list sorted: (offsets, data) ordered by (position, word)."""
+    o = np.asarray(offsets, np.int64)
+    dd = np.asarray(data, np.uint32)
+    seg = np.repeat(np.arange(len(o) - 1), np.diff(o))
+    return o, dd[np.lexsort((dd, seg))]
+
+
 def sample_indices(n: int, k: int):
     return list(range(0, n, max(1, n // k)))[:k]
 
 
-def oracle_rate(games, threads: int, budget_s: float):
-    """Solve games with the oracle until the budget is spent; games/s."""
+def build_games_oracle_parallel(seeds, threads: int):
+    """build_games_oracle on host threads (the oracle's calls release the GIL)."""
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        return [g for part in ex.map(build_games_oracle, [[s] for s in seeds]) for g in part]
+
+
+def oracle_solve(games, threads: int):
+    """One oracle solve of every game: `threads` threads share one work
+    counter, largest games first.  Returns (games/s, seconds, solutions)."""
     from oracle import ora
-    done, t0 = 0, time.perf_counter()
-    chunk = max(1, threads * 4)
-    while done < len(games):
-        ora.run_games_parallel(games[done:done + chunk], threads=threads)
-        done = min(len(games), done + chunk)
-        if time.perf_counter() - t0 > budget_s:
-            break
+    t0 = time.perf_counter()
+    sols = ora.solve_games(games, threads=threads, largest_first=True)
     dt = time.perf_counter() - t0
-    return done / dt, done, dt
+    return len(games) / dt, dt, sols
+
+
+def workload_config(rows, world: int) -> dict:
+    """The `config` object of both arms (same workload, same keys)."""
+    pos = sum(r[1] for r in rows)
+    edges = sum(r[2] for r in rows)
+    in_bytes = sum(4 * (r[1] + 1) + 8 * r[2] + r[1] for r in rows)  # row, col, wt, attacker flags
+    return {
+        "workload": f"batched: {len(rows)} seeded LTS compare(p,q) spectroscopy games per GPU "
+                    f"(states log-uniform 20-5000, 2-16 labels, 1.5-5 transitions/state; games <= 200k positions)",
+        "games_per_gpu": len(rows), "positions_per_gpu": int(pos), "edges_per_gpu": int(edges),
+        "l2": f"inputs larger than L2 ({in_bytes / 1e6:.0f} MB of game graph per GPU)",
+        "parallelism": f"replicas x{world}",
+    }
+
+
+# DRAM bytes per algorithmic byte of the round kernels (k_round + k_round_big):
+# dram__bytes_read.sum + dram__bytes_write.sum over all their launches in one
+# ncu capture of the 1,024-job batch (--solve-only --jobs 1024), divided by
+# the algorithmic bytes those launches counted.  Traffic grows with the work
+# of a launch, so the full-size figure is this ratio x its algorithmic bytes.
+DRAM_PER_ALGORITHMIC_BYTE = 1.77
 
 
 def peak_hbm():
@@ -249,77 +290,231 @@ def peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profile_traffic_ratio():
-    """DRAM bytes per algorithmic byte of k_round, from the committed ncu
-    summary (all round launches of a smaller case of the same workload)."""
-    p = os.path.join(ROOT, "profiles", "k_round_batched.md")
-    try:
-        with open(p) as f:
-            for line in f:
-                if line.strip().startswith("dram_per_algorithmic_byte:"):
-                    return float(line.split(":", 1)[1].strip())
-    except OSError:
-        pass
-    return None
+class Load:
+    """Drives a geq_server from host threads through the C ABI: arrival i
+    submits item pick[i] (a game view or an (lts, p, q) query) at its arrival
+    time (open loop) or as soon as a previous request of its thread finished
+    (closed loop, `outstanding` requests in flight).  Latency = submit ->
+    the request's solution in the caller's hands (geq_server_poll returned)."""
 
+    def __init__(self, srv, items, queries: bool, threads: int = 4):
+        from gpuequiv_b200._lib import lib
+        self.lib, self.h, self.items, self.queries, self.threads = lib, srv.h, items, queries, threads
 
-def run_serving(ctx, graphs, lam: float, seconds: float, seed: int, queries=False) -> dict:
-    """Poisson arrivals of single requests (drawn from `graphs`) into the
-    serving loop; latency = submit -> result in the caller's hands.  With
-    `queries`, the items are (lts, p, q) equivalence queries (minimised, built
-    and solved on the device), else game graphs."""
-    import queue
-    import threading
+    def _submit(self, item):
+        import ctypes as C
+        t = C.c_uint64()
+        if self.queries:
+            lts, p, q = item
+            st = self.lib.geq_server_submit_compare(self.h, lts.h, p, q, C.byref(t))
+        else:
+            st = self.lib.geq_server_submit(self.h, C.byref(item), C.byref(t))
+        if st:
+            raise RuntimeError(f"submit failed: status {st}")
+        return t.value
 
-    from gpuequiv_b200.serving import Server
-    rng = np.random.default_rng(seed)
-    n = max(1, int(lam * seconds))
-    arrivals = np.cumsum(rng.exponential(1.0 / lam, n))
-    pick = rng.integers(0, len(graphs), n)
-    t_sub = np.zeros(n)
-    t_done = np.zeros(n)
-    with Server(ctx) as srv:
-        submit = (lambda item: srv.submit_compare(*item)) if queries else srv.submit
-        # warm the pipelines (CUDA graphs, device and host pools): single
-        # requests, then a burst
-        for g in graphs[:32]:
-            srv.poll(submit(g))
-        for t in [submit(g) for g in graphs[:512]]:
-            srv.poll(t)
-        q: "queue.Queue" = queue.Queue()
+    def _poll(self, ticket):
+        import ctypes as C
+        sol = C.c_void_p()
+        st = self.lib.geq_server_poll(self.h, ticket, -1, C.byref(sol))
+        if st == 0:
+            self.lib.geq_solution_free(sol)
+        return st
 
-        def poller():
+    def open_loop(self, arrivals, pick):
+        import queue
+        import threading
+        n = len(arrivals)
+        t_sub, t_done, status = np.zeros(n), np.zeros(n), np.zeros(n, np.int32)
+        t0 = time.perf_counter() + 0.05
+
+        def submitter(k, q):
+            for i in range(k, n, self.threads):
+                wait = t0 + arrivals[i] - time.perf_counter()
+                if wait > 0:
+                    time.sleep(wait)
+                t_sub[i] = time.perf_counter()
+                q.put((i, self._submit(self.items[pick[i]])))
+            q.put(None)
+
+        def poller(q):
             while True:
-                item = q.get()
-                if item is None:
+                x = q.get()
+                if x is None:
                     return
-                i, t = item
-                srv.poll(t)
+                i, t = x
+                status[i] = self._poll(t)
                 t_done[i] = time.perf_counter()
 
-        pollers = [threading.Thread(target=poller) for _ in range(4)]
-        for th in pollers:
-            th.start()
-        st0 = srv.stats()
+        qs = [queue.Queue() for _ in range(self.threads)]
+        th = [threading.Thread(target=submitter, args=(k, qs[k])) for k in range(self.threads)]
+        th += [threading.Thread(target=poller, args=(qs[k],)) for k in range(self.threads)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        return t_sub, t_done, status, t0
+
+    def closed_loop(self, pick, outstanding: int, seconds: float):
+        import collections
+        import threading
+        per = max(1, outstanding // self.threads)
+        lat, stat, done_at = [], [], []
+        lock = threading.Lock()
         t0 = time.perf_counter()
-        for i in range(n):
-            wait = t0 + arrivals[i] - time.perf_counter()
-            if wait > 0:
-                time.sleep(wait)
-            t_sub[i] = time.perf_counter()
-            q.put((i, submit(graphs[pick[i]])))
-        for _ in pollers:
-            q.put(None)
-        for th in pollers:
-            th.join()
-        st = srv.stats()
-    lat = (t_done - t_sub) * 1e3
-    span = t_done.max() - t0
-    batches = st["batches"] - st0["batches"]
-    return {"lambda_req_s": lam, "requests": n, "seconds": round(float(span), 3),
-            "throughput_games_s": n / span, "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
-            "batches": int(batches), "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches)}
+        t_end = t0 + seconds
+
+        def worker(k):
+            rng = np.random.default_rng(k)
+            fifo = collections.deque()
+            my_lat, my_stat, my_done = [], [], []
+            while True:
+                while len(fifo) < per and time.perf_counter() < t_end:
+                    fifo.append((time.perf_counter(), self._submit(self.items[pick[int(rng.integers(len(pick)))]])))
+                if not fifo:
+                    break
+                ts, t = fifo.popleft()
+                st = self._poll(t)
+                now = time.perf_counter()
+                my_lat.append((now - ts) * 1e3)
+                my_stat.append(st)
+                my_done.append(now)
+            with lock:
+                lat.extend(my_lat)
+                stat.extend(my_stat)
+                done_at.extend(my_done)
+
+        th = [threading.Thread(target=worker, args=(k,)) for k in range(self.threads)]
+        for x in th:
+            x.start()
+        for x in th:
+            x.join()
+        return np.array(lat), np.array(stat, np.int32), np.array(done_at), t0
+
+
+def _lat_summary(lat_ms, status, span_s):
+    ok = status == 0
+    refused = int((status == 2).sum())  # GEQ_ERR_OUT_OF_MEMORY: the game exceeds the position bound
+    failed = int((~ok).sum()) - refused
+    l = lat_ms[ok] if ok.any() else np.zeros(1)
+    return {"requests": int(len(status)), "served": int(ok.sum()), "refused": refused, "failed": failed,
+            "refusal_rate": refused / max(1, len(status)), "seconds": round(float(span_s), 3),
+            "throughput_games_s": float(ok.sum() / span_s) if span_s > 0 else None,
+            "p50_ms": float(np.percentile(l, 50)), "p99_ms": float(np.percentile(l, 99)), "mean_ms": float(l.mean())}
+
+
+def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, saturation_s: float,
+                max_game_positions: int = 0, outstanding: int = 8192) -> dict:
+    """One server: open-loop Poisson arrivals at each rate, then a closed-loop
+    saturation run (`outstanding` requests kept in flight)."""
+    from gpuequiv_b200.serving import Server
+    rng = np.random.default_rng(seed)
+    out = {"runs": [], "saturation": None}
+    with Server(ctx, max_game_positions=max_game_positions) as srv:
+        load = Load(srv, items, queries)
+        # warm the pipelines (CUDA graphs, device and host pools): single
+        # requests, then a burst
+        warm = np.arange(min(len(items), 512))
+        load.open_loop(np.zeros(min(32, len(warm))), warm[:32])
+        load.open_loop(np.zeros(len(warm)), warm)
+        for lam in rates:
+            n = max(1, int(rng.poisson(lam * seconds)))
+            arrivals = np.sort(rng.uniform(0, seconds, n))
+            pick = rng.integers(0, len(items), n)
+            st0 = srv.stats()
+            t_sub, t_done, status, t0 = load.open_loop(arrivals, pick)
+            st = srv.stats()
+            r = _lat_summary((t_done - t_sub) * 1e3, status, t_done.max() - t0)
+            batches = st["batches"] - st0["batches"]
+            r.update({"lambda_req_s": lam, "batches": int(batches),
+                      "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches)})
+            out["runs"].append(r)
+        if saturation_s > 0:
+            pick = np.arange(len(items))
+            st0 = srv.stats()
+            lat, status, done_at, t0 = load.closed_loop(pick, outstanding, saturation_s)
+            st = srv.stats()
+            r = _lat_summary(lat, status, done_at.max() - t0)
+            batches = st["batches"] - st0["batches"]
+            r.update({"outstanding": outstanding, "batches": int(batches),
+                      "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches)})
+            out["saturation"] = r
+    return out
+
+
+def within_bound(job, bound: int) -> bool:
+    """The game of compare(p, q) (after minimisation) has at most `bound`
+    positions (host GameBuild with the bound)."""
+    import gpuequiv_b200 as geq
+    lts, p, q = job
+    red, mp = lts.bisimilar_minimize()
+    if mp[p] == mp[q]:
+        return True
+    try:
+        geq.GameBuild.compare_bounded(red, int(mp[p]), int(mp[q]), bound)
+        return True
+    except geq.GeqError:
+        return False
+
+
+def serving_queries(n_pool: int, seed: int = 7):
+    """A pool of equivalence queries with the serving configuration's
+    distribution: each a seeded LTS of log-uniform 20-20,000 states (other
+    parameters as the batched configuration) and one pair p != q."""
+    import gpuequiv_b200 as geq
+    synth = synth_mod()
+    _, seeds = synth.serving_trace(seed, n_pool, 1.0)
+    out = []
+    for s in seeds[:n_pool]:
+        src, dst, lab, p, q = synth.batched_lts(int(s), smax=20_000)
+        out.append((geq.TransitionSystem.from_arrays(src, dst, lab), int(p), int(q)))
+    return out
+
+
+def run_small(ctx, seeds, check: bool) -> dict:
+    """The small configuration: TransitionSystem::equivalences() (minimise ->
+    compare_all game -> solve -> verdicts) of seeded 40-state LTSs, one call
+    per LTS.  With `check` (the CPU baseline leg) the oracle computes the same
+    equivalences on one thread: its time is the baseline, and every start
+    pair's energies and the 13 standard relations are compared."""
+    import gpuequiv_b200 as geq
+    synth = synth_mod()
+    systems = [synth.small_lts(s) for s in seeds]
+    ltss = [geq.TransitionSystem.from_arrays(*x) for x in systems]
+    for lts in ltss[:5]:
+        lts.equivalences(ctx)
+    t = time.perf_counter()
+    eqs = [lts.equivalences(ctx) for lts in ltss]
+    dt = time.perf_counter() - t
+    out = {"workload": f"small: seeds {seeds[0]}..{seeds[-1]}, 40 states, 4 labels, 120 transitions (tau p 0.2), "
+                       f"equivalences() per LTS (minimisation, compare_all game, solve, verdicts)",
+           "games_s": len(ltss) / dt, "ms_per_game": dt / len(ltss) * 1e3}
+    if not check:
+        return out
+    from oracle import ora
+    t = time.perf_counter()
+    oeqs = [ora.equivalences(ora.Lts.from_arrays(*x)) for x in systems]
+    odt = time.perf_counter() - t
+    names = geq.std_equivalences.names()
+    bad = []
+    for k, (eq, oeq, lts) in enumerate(zip(eqs, oeqs, ltss)):
+        n = lts.n_vertices()
+        ok = True
+        for p in range(n):
+            for q in range(n):
+                a, b = eq.energies(p, q), oeq.energies_of(p, q)
+                if (a is None) != (b is None) or (a is not None and sorted(int(x) for x in a.array.reshape(-1)) !=
+                                                  sorted(int(x) for x in np.asarray(b).reshape(-1))):
+                    ok = False
+        for name in names:
+            r, o = eq.relation(geq.std_equivalences.get(name)), oeq.relation(geq.std_equivalences._T[name])
+            ok = ok and r.count_classes() == o.count_classes()
+        if not ok:
+            bad.append(int(seeds[k]))
+    out.update({"cpu_baseline": {"value": len(systems) / odt, "unit": UNIT, "cores": 1, "kind": "port",
+                                 "sample": f"the same {len(systems)} LTSs, oracle equivalences(), 1 thread"},
+                "parity_checked": len(systems), "parity_mismatches": len(bad), "mismatched_seeds": bad[:16]})
+    return out
 
 
 # ---- arms -----------------------------------------------------------------------
@@ -385,26 +580,42 @@ def run_lts_pipeline(ctx, seeds, graphs, args, d: Dist) -> dict:
 
 
 def run_reference(args, d: Dist):
+    """The reference's path on the host cores: the oracle (the reference's
+    Rust/wgpu code cannot run here) builds every job's game with its own
+    GameBuild and solves it with its EnergyGame::run on all host threads,
+    the threads sharing one work counter, largest games first.  A step is one
+    solve of the whole batch -- or, when K steps of it would not end within a
+    few minutes, of every s-th job (a sample with the batch's size mix)."""
     if d.rank != 0:
         return
     seeds, rows = batched_seeds(args.jobs, 0)
-    idx = sample_indices(len(seeds), 512)
-    games = build_games_oracle([seeds[i] for i in idx])
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        oracle_rate(games[:threads], threads, 5.0)
+    t = time.perf_counter()
+    games = build_games_oracle_parallel(seeds, threads)
+    build_s = time.perf_counter() - t
+    # warm-up: one solve of the whole batch (it also sizes the steps), the
+    # others on a small sample
+    _, full_s, _ = oracle_solve(games, threads)
+    for _ in range(max(0, args.warmup - 1)):
+        oracle_solve(games[::64], threads)
+    stride = 1
+    while stride < 64 and args.steps * full_s / stride > 150.0:
+        stride *= 2
+    step_games = games[::stride]
     rates = []
     for _ in range(args.steps):
-        r, n, dt = oracle_rate(games, threads, max(5.0, 60.0 / max(args.steps, 1)))
-        rates.append((r, n, dt))
+        r, dt, _ = oracle_solve(step_games, threads)
+        rates.append((r, dt))
     value = float(np.median([r[0] for r in rates]))
-    sample = (f"{rates[0][1]} of {len(games)} games (every {max(1, len(seeds) // 512)}th job of the "
-              f"{len(seeds)}-job batch) per step, oracle EnergyGame::run on {threads} threads")
+    sample = (f"{len(step_games)} of the {len(games)} games per step" +
+              (f" (every {stride}th job)" if stride > 1 else " (the whole batch)") +
+              f", oracle GameBuild (untimed, {build_s:.1f} s) + EnergyGame::run on {threads} threads, "
+              f"one shared work counter, largest games first")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median([r[2] for r in rates]) * 1e3),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median([r[1] for r in rates]) * 1e3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"batched: {len(seeds)} seeded LTS compare(p,q) spectroscopy games"},
+        "config": workload_config(rows, d.world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -485,6 +696,10 @@ def run_ours(args, d: Dist):
     step_ms = d.max(dev_ms / args.steps)
     total_games = d.sum(len(graphs))
     value = total_games / (step_ms / 1e3)
+    # the lists of the last timed solve: checked against the oracle below,
+    # and the byte floor of the solve from them
+    res_offs, res_data = dg.download_raw()
+    b_min = sum(geq.b_min(g, o) for g, o in zip(graphs, res_offs))
 
     # ---- roofline of the round kernel (one profiled solve, not timed) ----
     ctx.set_tuning(flags=TUNE_PROFILE)
@@ -495,9 +710,8 @@ def run_ours(args, d: Dist):
     k_ms = st_prof["round_kernel_ms"]
     k_launch = max(1, st_prof["round_kernel_launches"])
     achieved = st_prof["algorithmic_bytes"] / (k_ms / 1e3) / 1e9 if k_ms > 0 else None
-    ratio = profile_traffic_ratio()
     alg_per_launch = st_prof["algorithmic_bytes"] / k_launch
-    traffic = ratio * alg_per_launch if ratio else None
+    traffic = DRAM_PER_ALGORITHMIC_BYTE * alg_per_launch
 
     # ---- e2e: host buffers through the C ABI (geq_energy_game_run_batch) ----
     views = geq.c_views(graphs)
@@ -529,16 +743,41 @@ def run_ours(args, d: Dist):
     plain_s = time.perf_counter() - t
     plain_rate = len(idx) / plain_s  # every k-th job: the batch's size mix
 
-    # ---- serving loop: Poisson arrivals of single games (not part of value) ----
-    serving = []
+    # ---- serving loop (not part of value) ----
+    # game requests drawn from this batch: Poisson arrivals, then saturation
     rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
-    for k, lam in enumerate(rates):
-        serving.append(run_serving(ctx, graphs, lam, args.serve_seconds, seed=100 + k + 1000 * d.rank))
-    # the same arrivals as equivalence queries on the LTSs themselves
-    serving_q = []
-    for k, lam in enumerate(rates):
-        serving_q.append(run_serving(ctx, lts_jobs, lam, args.serve_seconds, seed=100 + k + 1000 * d.rank,
-                                     queries=True))
+    serving = None
+    if rates or args.saturation_seconds > 0:
+        serving = run_serving(ctx, views, False, rates, args.serve_seconds, 100 + 1000 * d.rank,
+                              args.saturation_seconds)
+        sat = serving["saturation"]
+        serving["saturation_vs_plain"] = sat["throughput_games_s"] / plain_rate if sat and plain_rate else None
+    # the serving configuration: equivalence queries on LTSs of 20-20,000
+    # states (minimised, built and solved on the device), games above the
+    # position bound refused
+    qrates = [float(x) for x in args.query_rates.split(",") if x.strip()]
+    serving_q = None
+    if qrates or args.saturation_seconds > 0:
+        pool = serving_queries(args.query_pool, seed=7 + 1000 * d.rank)
+        serving_q = run_serving(ctx, pool, True, qrates, args.serve_seconds, 200 + 1000 * d.rank,
+                                args.saturation_seconds, max_game_positions=args.query_bound,
+                                outstanding=2048)
+        # the plain form on the same distribution: one compare() call per
+        # query, for queries whose game is within the bound
+        acc = [j for j in pool[::max(1, len(pool) // 96)][:96] if within_bound(j, args.query_bound)][:64]
+        for j in acc[:8]:
+            geq.compare_batch([j], context=ctx)
+        t = time.perf_counter()
+        for j in acc:
+            geq.compare_batch([j], context=ctx)
+        plain_q = len(acc) / (time.perf_counter() - t) if acc else None
+        serving_q["plain_per_query"] = {"value": plain_q, "unit": UNIT,
+                                        "sample": f"{len(acc)} pool queries within the bound, one compare() each"}
+        sat = serving_q["saturation"]
+        serving_q["saturation_vs_plain"] = (sat["throughput_games_s"] / plain_q) if sat and plain_q else None
+
+    # ---- small configuration: equivalences() of 100 seeded 40-state LTSs ----
+    small = run_small(ctx, list(range(100)), check=d.rank == 0)
 
     # ---- stress configuration: one 2M-position / 10M-edge game, resident ----
     stress = None
@@ -549,59 +788,92 @@ def run_ours(args, d: Dist):
         for _ in range(2):
             sdg.solve()
         sts = [sdg.solve() for _ in range(3)]
+        s_offs, _ = sdg.download_raw()
+        s_bmin = geq.b_min(sg, s_offs[0])
+        del s_offs
+        flags0 = ctx.tuning()["flags"]
+        ctx.set_tuning(flags=flags0 | TUNE_PROFILE)
+        s_prof = sdg.solve()
+        ctx.set_tuning(flags=flags0)
         sdg.close()
         sms = float(np.median([x["device_ms"] for x in sts]))
+        s_ach = s_prof["algorithmic_bytes"] / (s_prof["round_kernel_ms"] / 1e3) / 1e9 if s_prof["round_kernel_ms"] else None
         stress = {"workload": "stress: 2,000,000 positions (60 % attackers), 10,000,000 edges, seed 2, standard reach",
                   "solve_ms": sms, "edges_relaxed": sts[0]["edges_relaxed"],
                   "positions_computed": sts[0]["positions_computed"], "rounds": sts[0]["rounds"],
-                  "edges_relaxed_per_s": sts[0]["edges_relaxed"] / (sms / 1e3)}
+                  "edges_relaxed_per_s": sts[0]["edges_relaxed"] / (sms / 1e3),
+                  "roofline": {"bound": "hbm", "achieved": s_ach, "peak": peak, "unit": "GB/s",
+                               "frac": s_ach / peak if s_ach else None, "peak_kind": peak_kind,
+                               "kernel": "k_round + k_round_big (all rounds of one solve)",
+                               "algorithmic_bytes_per_solve": s_prof["algorithmic_bytes"],
+                               "round_kernel_ms_per_solve": s_prof["round_kernel_ms"],
+                               "round_kernel_launches": s_prof["round_kernel_launches"],
+                               "b_min": s_bmin, "b_min_over_algorithmic_bytes": s_bmin / s_prof["algorithmic_bytes"]}}
 
-    # ---- CPU baseline: the oracle on one host thread (rank 0, N=1) ----
-    cpu = None
-    if d.rank == 0 and d.world == 1:
+    # ---- CPU baseline: the oracle on one host thread (rank 0, N=1), on every
+    # 16th job; its lists are the check of the timed solve's lists ----
+    cpu, parity = None, None
+    if d.rank == 0:
         cidx = sample_indices(len(seeds), 256)
-        cg = build_games_oracle([seeds[i] for i in cidx])
-        r, n, dt = oracle_rate(cg, 1, args.cpu_seconds)
-        cpu = {"value": r, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{n} games (every {max(1, len(seeds) // 256)}th job of the batch, in order) in {dt:.1f} s, "
-                         f"oracle EnergyGame::run, 1 thread"}
+        cg = build_games_oracle_parallel([seeds[i] for i in cidx], os.cpu_count() or 4)
+        threads = 1 if d.world == 1 else (os.cpu_count() or 4)
+        r, dt, sols = oracle_solve(cg, threads)
+        if d.world == 1:
+            cpu = {"value": r, "unit": UNIT, "cores": 1, "kind": "port",
+                   "sample": f"{len(cg)} games (every {max(1, len(seeds) // 256)}th job of the batch) in {dt:.1f} s, "
+                             f"oracle EnergyGame::run, 1 thread"}
+        bad = []
+        for i, sol in zip(cidx, sols):
+            same = (len(res_offs[i]) == len(sol.offsets) and
+                    all(np.array_equal(a, b) for a, b in zip(canonical(res_offs[i], res_data[i]),
+                                                             canonical(sol.offsets, sol.data))))
+            if not same:
+                bad.append(int(i))
+        parity = {"parity_checked": len(cidx), "parity_mismatches": len(bad), "mismatched_jobs": bad[:16],
+                  "what": "every position's list (as a set) of the last timed solve against the oracle's "
+                          "GameBuild + EnergyGame::run, every 16th job"}
+    del res_offs, res_data
 
     if d.rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": d.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {
-                "workload": f"batched: {len(graphs)} seeded LTS compare(p,q) spectroscopy games per GPU "
-                            f"(states log-uniform 20-5000, 2-16 labels, 1.5-5 transitions/state; games <= 200k positions)",
-                "games_per_gpu": len(graphs), "positions_per_gpu": pos, "edges_per_gpu": edges,
-                "host_build_s": round(build_s, 2),
-                "l2": f"inputs larger than L2 ({in_bytes / 1e6:.0f} MB of game graph per GPU)",
-                "parallelism": f"replicas x{d.world}",
-            },
+            "config": workload_config(rows, d.world),
+            "host_build_s": round(build_s, 2),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "traffic_source": "ncu DRAM bytes per algorithmic byte of all round-kernel launches (k_round + "
-                                           "k_round_big) of the 1024-job case (profiles/k_round_batched.md) x "
+                         "traffic_source": f"ncu DRAM bytes per algorithmic byte ({DRAM_PER_ALGORITHMIC_BYTE}) of all "
+                                           "round-kernel launches (k_round + k_round_big) of the 1024-job case x "
                                            "algorithmic bytes per full-size round",
+                         "b_min": b_min, "b_min_over_algorithmic_bytes": b_min / st_prof["algorithmic_bytes"],
+                         "b_min_note": "schedule-independent floor 4(n+1) + 8m + n + sum_v 4|A*_v|(1+indeg v) "
+                                       "from the final lists",
                          "algorithmic_bytes_per_launch": alg_per_launch,
                          "kernel": "k_round + k_round_big (one round)", "peak_kind": peak_kind,
                          "algorithmic_bytes_per_solve": st_prof["algorithmic_bytes"],
                          "round_kernel_ms_per_solve": k_ms, "round_kernel_launches": k_launch},
             "cpu_baseline": cpu,
+            **(parity or {}),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(in_bytes),
                     "d2h_bytes_per_step": int(out_bytes)},
             "plain_cuda": {"value": plain_rate, "unit": UNIT, "sample": f"{len(idx)} games (every "
                            f"{max(1, len(graphs) // len(idx))}th job), one geq_energy_game_run call each"},
             "batched_vs_plain": value / plain_rate if plain_rate else None,
             "lts_pipeline": lts_pipe,
+            "small": small,
             "stress": stress,
-            "serving": {"workload": "Poisson arrivals of single compare(p,q) games drawn from this batch "
-                                    "(LTS 20-5000 states), geq_server with 2 pipelines, 150 GB admission budget",
-                        "runs": serving,
-                        "queries": {"workload": "the same Poisson arrivals as compare(p, q) queries on the batch's "
-                                                "unminimised LTSs (geq_server_submit_compare: minimisation, "
-                                                "GameBuild and solve on the device)", "runs": serving_q}},
+            "serving": {"workload": "game requests (geq_server_submit) drawn from this batch's games: Poisson "
+                                    "arrivals, then a closed loop of 8192 requests in flight (saturation); "
+                                    "geq_server with 2 pipelines, 150 GB admission budget; latency = submit -> "
+                                    "lists in the caller's hands",
+                        **(serving or {}),
+                        "queries": {"workload": f"serving configuration: Poisson arrivals of compare(p, q) queries "
+                                                f"on seeded LTSs of log-uniform 20-20,000 states (pool of "
+                                                f"{args.query_pool}), geq_server_submit_compare (minimisation, "
+                                                f"GameBuild, solve on the device), games above "
+                                                f"{args.query_bound} positions refused; then a closed loop of 2048 "
+                                                f"queries in flight", **(serving_q or {})}},
             "gpu_launches": int(launches),
             "clocks": ck,
             "solve_stats": {k: st_last[k] for k in ("rounds", "positions_computed", "edges_relaxed",
@@ -612,6 +884,11 @@ def run_ours(args, d: Dist):
         }
         print(json.dumps(line), flush=True)
     ctx.close()
+    if parity and parity["parity_mismatches"]:
+        raise SystemExit(f"parity: {parity['parity_mismatches']} of {parity['parity_checked']} checked jobs differ "
+                         f"from the oracle: {parity['mismatched_jobs']}")
+    if small and small.get("parity_mismatches"):
+        raise SystemExit(f"parity: small configuration, seeds {small['mismatched_seeds']} differ from the oracle")
 
 
 def main():

@@ -8,7 +8,7 @@ TransitionSystem, Equivalence) over the C ABI of ``libgeq.so``
 from ._lib import GeqError, library_path
 from .energy import (Energy, EnergyArray, EnergyConf, Upd, Update, UpdateArray, std_equivalences,
                      update)
-from .energygame import (Context, DeviceGames, EnergyGame, GameGraph, c_views, default_context, run_batch,
+from .energygame import (Context, DeviceGames, EnergyGame, GameGraph, b_min, c_views, default_context, run_batch,
                          run_batch_raw, run_static)
 from .lts import (Equivalence, EquivalenceRelation, GameBatch, GameBuild, Position, StartInfo,
                   TransitionSystem, compare_batch, signature_refinement_batch)
@@ -16,6 +16,6 @@ from .lts import (Equivalence, EquivalenceRelation, GameBatch, GameBuild, Positi
 __all__ = [
     "GeqError", "library_path", "Energy", "EnergyArray", "EnergyConf", "Upd", "Update", "UpdateArray",
     "std_equivalences", "update", "Context", "DeviceGames", "EnergyGame", "GameGraph", "default_context",
-    "run_batch", "run_batch_raw", "run_static", "c_views", "Equivalence", "EquivalenceRelation", "GameBatch", "GameBuild", "Position", "StartInfo",
+    "run_batch", "run_batch_raw", "run_static", "c_views", "b_min", "Equivalence", "EquivalenceRelation", "GameBatch", "GameBuild", "Position", "StartInfo",
     "TransitionSystem", "compare_batch", "signature_refinement_batch",
 ]

@@ -41,12 +41,12 @@ class geq_solve_stats(C.Structure):
 
 class geq_tuning(C.Structure):
     _fields_ = [("blocks_per_sm", C.c_uint32), ("rounds_per_graph", C.c_uint32),
-                ("small_limit", C.c_uint32), ("flags", C.c_uint32)]
+                ("small_limit", C.c_uint32), ("flags", C.c_uint32), ("lane_limits", C.c_uint32)]
 
 
 class geq_server_config(C.Structure):
     _fields_ = [("n_pipelines", C.c_uint32), ("max_batch_games", C.c_uint32), ("max_wait_us", C.c_uint32),
-                ("reserved", C.c_uint32), ("hbm_budget_bytes", C.c_uint64), ("max_queued", C.c_uint64)]
+                ("max_game_positions", C.c_uint32), ("hbm_budget_bytes", C.c_uint64), ("max_queued", C.c_uint64)]
 
 
 class geq_server_stats(C.Structure):
@@ -79,6 +79,7 @@ TUNE_PROFILE = 8
 TUNE_NO_THREAD_PATH = 16
 TUNE_NO_SPLIT = 32
 TUNE_BUILD_WARP_ALL = 64
+TUNE_FORCE_WIDE = 128
 
 STATUS = {0: "OK", 1: "NO_DEVICE", 2: "OUT_OF_MEMORY", 3: "INVALID_INPUT", 4: "TIMEOUT",
           5: "UNSUPPORTED", 6: "CUDA", 7: "IO", 8: "PARSE", 9: "BUSY", 10: "INTERNAL"}
@@ -110,6 +111,7 @@ _SIGS = {
     "geq_conf_update_size": ([geq_energy_conf], C.c_uint32),
     "geq_conf_update_mask": ([geq_energy_conf], C.c_uint32),
     "geq_conf_supported": ([geq_energy_conf], C.c_int),
+    "geq_conf_solvable": ([geq_energy_conf], C.c_int),
     "geq_energy_pack": ([geq_energy_conf, u32p, C.c_uint32, u32p], C.c_int),
     "geq_energy_unpack": ([geq_energy_conf, u32p, u32p], None),
     "geq_update_pack": ([geq_energy_conf, i32p, C.c_uint32, u32p], C.c_int),

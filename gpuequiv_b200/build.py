@@ -20,7 +20,7 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
-SOURCES = ["engine.cu", "gbuild.cu", "api.cpp", "lts.cpp", "gamebuild.cpp", "pipeline.cpp", "server.cpp"]
+SOURCES = ["engine.cu", "gbuild.cu", "wide.cu", "api.cpp", "lts.cpp", "gamebuild.cpp", "pipeline.cpp", "server.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -132,9 +132,15 @@ static geq_status make_inputs(uint32_t n_games, const geq_game_graph *graphs, co
         return sts[g];
       }
   }
-  if (!Conf(graphs[0].conf).supported())
-    return fail(GEQ_ERR_UNSUPPORTED, "EnergyConf {%u, %u} is outside the device codecs", graphs[0].conf.elements,
-                graphs[0].conf.max);
+  return GEQ_OK;
+}
+
+// The solver path of a batch's conf: true for the multi-word solver.
+static geq_status wide_path(const Engine &e, const geq_energy_conf &c, bool &wide) {
+  const Conf conf(c);
+  wide = !conf.supported() || (e.tuning.flags & GEQ_TUNE_FORCE_WIDE);
+  std::string why;
+  if (wide && !wide_supported(conf, &why)) return fail(GEQ_ERR_UNSUPPORTED, "%s", why.c_str());
   return GEQ_OK;
 }
 
@@ -170,6 +176,7 @@ uint32_t geq_conf_update_bits(geq_energy_conf c) { return Conf(c).update_bits();
 uint32_t geq_conf_update_size(geq_energy_conf c) { return Conf(c).update_size(); }
 uint32_t geq_conf_update_mask(geq_energy_conf c) { return Conf(c).update_mask(); }
 int geq_conf_supported(geq_energy_conf c) { return Conf(c).supported() ? 1 : 0; }
+int geq_conf_solvable(geq_energy_conf c) { return Conf(c).supported() || wide_supported(Conf(c)) ? 1 : 0; }
 
 // pack_energy (energy.rs:143-162)
 geq_status geq_energy_pack(geq_energy_conf cc, const uint32_t *values, uint32_t n, uint32_t *out) {
@@ -292,6 +299,7 @@ geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t) {
   if (t->blocks_per_sm) e->tuning.blocks_per_sm = std::min<uint32_t>(std::max<uint32_t>(t->blocks_per_sm, 2), 5);
   if (t->rounds_per_graph) e->tuning.rounds_per_graph = std::min<uint32_t>(t->rounds_per_graph, 256);
   if (t->small_limit) e->tuning.small_limit = std::min<uint32_t>(t->small_limit, 32);
+  if (t->lane_limits) e->tuning.lane_limits = t->lane_limits;
   e->tuning.flags = t->flags;
   return GEQ_OK;
 }
@@ -344,6 +352,10 @@ geq_status geq_device_games_create(geq_context *ctx, uint32_t n_games, const geq
   if (st) return st;
   std::vector<GameInput> in;
   if ((st = make_inputs(n_games, graphs, initial, to_reach, n_to_reach, in))) return st;
+  if (!Conf(graphs[0].conf).supported())
+    return fail(GEQ_ERR_UNSUPPORTED,
+                "device-resident games need a conf of the thermometer codecs (EnergyConf {%u, %u} is solved by "
+                "geq_energy_game_run / geq_energy_game_run_batch)", graphs[0].conf.elements, graphs[0].conf.max);
   std::unique_ptr<geq_device_games> dg(new geq_device_games());
   if ((st = e->upload(in, dg->impl))) return st;
   *out = dg.release();
@@ -386,6 +398,14 @@ geq_status geq_energy_game_run_batch(geq_context *ctx, uint32_t n_games, const g
   if (st) return st;
   std::vector<GameInput> in;
   if ((st = make_inputs(n_games, graphs, initial, to_reach, n_to_reach, in))) return st;
+  bool wide = false;
+  if ((st = wide_path(*e, graphs[0].conf, wide))) return st;
+  if (wide) {
+    std::unique_ptr<geq_solution> sol(new geq_solution());
+    if ((st = solve_wide(*e, ctx->device, in, *sol))) return st;
+    *out = sol.release();
+    return GEQ_OK;
+  }
   if (n_games == 1) {
     // a small single game: one launch of the one-block solver
     std::unique_ptr<geq_solution> sol(new geq_solution());

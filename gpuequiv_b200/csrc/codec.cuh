@@ -86,6 +86,20 @@ struct CodecStd {
     return t;
   }
   __host__ __device__ __forceinline__ uint32_t upd(uint32_t t, uint32_t u) const { return apply(t, prep(u)); }
+  // An edge's update as the round kernel reads it from its edge pairs: the
+  // decoded form when the update has at most two merges (bits 0-11 `lod`,
+  // 12-13 the merge count, 14-29 the merges), else the raw word with bit 31
+  // set (decoded when read).  Every update GameBuild emits has at most one
+  // merge.
+  __host__ __device__ static uint32_t pack_edge(uint32_t u) {
+    const Upd q = CodecStd{}.prep(u);
+    if (q.nm > 2u) return 0x80000000u | u;
+    return q.lod | (q.nm << 12) | ((uint32_t)q.mg << 14);
+  }
+  __host__ __device__ __forceinline__ Upd unpack_edge(uint32_t pw) const {
+    if (pw >> 31) return prep(pw & 0x7FFFFFFFu);
+    return Upd{pw & 0xFFFu, (pw >> 12) & 3u, (unsigned long long)((pw >> 14) & 0xFFFFu)};
+  }
 };
 
 struct CodecGen {
@@ -119,6 +133,8 @@ struct CodecGen {
   }
   using Upd = uint32_t;
   __host__ __device__ __forceinline__ Upd prep(uint32_t u) const { return u; }
+  __host__ __device__ static uint32_t pack_edge(uint32_t u) { return u; }
+  __host__ __device__ __forceinline__ Upd unpack_edge(uint32_t pw) const { return pw; }
   __host__ __device__ __forceinline__ uint32_t apply(uint32_t t, Upd u) const { return upd(t, u); }
   __host__ __device__ __forceinline__ uint32_t upd(uint32_t t, uint32_t u) const {
     if (u == 0) return t;

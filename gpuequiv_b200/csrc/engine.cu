@@ -2,8 +2,8 @@
 //
 // Reference path: EnergyGame::run -> GPURunner::execute_gpu
 // (src/energygame.rs:379-383, :1461-1523) with the attack shaders
-// (attack_update.wgsl:77-113, attack_minimize.wgsl:180-235) and the defend
-// shaders (defend_update.wgsl:73-101, defend_iterative.wgsl:283-368).
+// (attack_update.wgsl:77-113, attack_minimize.wgsl:69-122) and the defend
+// shaders (defend_update.wgsl:73-101, defend_iterative.wgsl:182-267).
 //
 // The reference runs a Jacobi worklist: every round it gathers the successor
 // energies of all queued positions on the host, uploads them, runs the four
@@ -151,6 +151,10 @@ struct KParams {
   uint32_t fblocks;      // blocks of k_commit, k_fcount, k_ffill
   const uint32_t *abits; // attacker positions as a bitmap (mwords words)
   uint32_t *bigq;        // frontier slots of the large positions of the round
+  // edge pairs for the lane path: successor id (low word) and the update in
+  // the codec's pack_edge form (high word); null: read col / wt
+  const unsigned long long *cw;
+  uint32_t td, tw, tk;   // lane-path limits: successors, candidates per step, list length
 };
 
 // Energy-list descriptors (one u64 per position):
@@ -452,7 +456,7 @@ __device__ Res scratch_store(const WarpCtx &x, unsigned long long src, uint32_t 
 }
 
 // ---- attacker (warp routines) ------------------------------------------------
-// attack_update.wgsl:77-113 + attack_minimize.wgsl:180-235: candidates are
+// attack_update.wgsl:77-113 + attack_minimize.wgsl:69-122: candidates are
 // the inverse-updated successor energies followed by the own energies; keep
 // the minimal ones (on ties the later copy, so own energies win); the
 // position changed iff a kept candidate came from a successor.
@@ -976,6 +980,30 @@ __device__ Res solve_position(const WarpCtx &x, const Cd &cd, uint32_t v) {
 }
 
 // ---- thread path: one lane per small position -----------------------------
+// Successor and update of edge k: one 8-byte load of the edge pair, or the
+// col / wt arrays where there are none (the one-block solver).
+__device__ __forceinline__ void load_edge(const KParams &p, Ctr *c, unsigned long long k, uint32_t &w, uint32_t &u) {
+  if (p.cw) {
+    const unsigned long long e = ld(p.cw, k, p.n_edges, c);
+    w = (uint32_t)e;
+    u = (uint32_t)(e >> 32);
+  } else {
+    w = ld(p.col, k, p.n_edges, c);
+    u = ld(p.wt, k, p.n_edges, c);
+  }
+}
+// up to four consecutive edges k0 .. k0+min(left,4)-1
+__device__ __forceinline__ void load_edges4(const KParams &p, Ctr *c, unsigned long long k0, uint32_t left,
+                                            uint32_t (&w)[4], uint32_t (&u)[4]) {
+#pragma unroll
+  for (int t = 0; t < 4; t++)
+    if ((uint32_t)t < left) load_edge(p, c, k0 + t, w[t], u[t]);
+}
+template <class Cd>
+__device__ __forceinline__ typename Cd::Upd edge_upd(const KParams &p, const Cd &cd, uint32_t u) {
+  return p.cw ? cd.unpack_edge(u) : cd.prep(u);
+}
+
 // Most positions have a handful of successors with one or two energies each.
 // Every lane of a warp solves its own such position.  Candidates stream into
 // an antichain held in a lane-private column of shared memory (bank = lane):
@@ -991,24 +1019,19 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
   const uint32_t e0 = ld(p.row, v, p.n_nodes + 1, c), e1 = ld(p.row, (unsigned long long)v + 1, p.n_nodes + 1, c);
   const uint32_t d = e1 - e0;
   if (d == 0) return T_SKIPPED;
-  if (d > TD) return T_BIG;
+  if (d > p.td) return T_BIG;
   const unsigned long long dv = ld(p.desc, v, p.n_nodes, c);
   const uint32_t cv = dcnt(dv);
   const bool attacker = ld(p.flags, v, p.n_nodes, c) & 1u;
   if (attacker) {
     // attack_update.wgsl + attack_minimize.wgsl: successor candidates, then
     // the own energies; changed iff a minimal value has no own copy
-    if (cv > TK) return T_BIG;
+    if (cv > p.tk) return T_BIG;
     uint32_t n = 0, om = 0, tot = 0;
     for (uint32_t j0 = 0; j0 < d; j0 += 4) {
       uint32_t w[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
       unsigned long long dw[4] = {0, 0, 0, 0};
-#pragma unroll
-      for (int t = 0; t < 4; t++)
-        if (j0 + t < d) {
-          w[t] = ld(p.col, (unsigned long long)e0 + j0 + t, p.n_edges, c);
-          u[t] = ld(p.wt, (unsigned long long)e0 + j0 + t, p.n_edges, c);
-        }
+      load_edges4(p, c, e0 + j0, d - j0, w, u);
 #pragma unroll
       for (int t = 0; t < 4; t++)
         if (j0 + t < d) dw[t] = ld(p.desc, w[t], p.n_nodes, c);
@@ -1017,8 +1040,8 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
         if (j0 + t < d) {
           const uint32_t cw = dcnt(dw[t]);
           tot += cw;
-          if (tot > TW) return T_BIG;
-          const auto pu = cd.prep(u[t]);
+          if (tot > p.tw) return T_BIG;
+          const auto pu = edge_upd(p, cd, u[t]);
           for (uint32_t q = 0; q < cw; q++)
             if (!ac_insert(scr, 0, n, om, cd.apply(cd.to_t(lelem(dw[t], q, arena, cap, c, p.ib, p.ibm)), pu), false))
               return T_BIG;
@@ -1045,34 +1068,35 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
   }
   uint32_t n;
   {
-    const uint32_t w0 = ld(p.col, e0, p.n_edges, c), u0 = ld(p.wt, e0, p.n_edges, c);
+    uint32_t w0, u0;
+    load_edge(p, c, e0, w0, u0);
     const unsigned long long d0 = ld(p.desc, w0, p.n_nodes, c);
     const uint32_t s = dcnt(d0);
-    const auto pu0 = cd.prep(u0);
+    const auto pu0 = edge_upd(p, cd, u0);
     unsigned long long tot = s;
     if (d == 1) {
-      // single successor: its updated list as is (defend_iterative.wgsl:301-313)
-      if (s > TK) return T_BIG;
+      // single successor: its updated list as is (defend_iterative.wgsl:200-211)
+      if (s > p.tk) return T_BIG;
       for (uint32_t q = 0; q < s; q++)
         SCR(TK + q) = cd.to_p(cd.apply(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), pu0));
       n = s;
     } else {
       // fold of pairwise suprema, minimised after every step
-      // (defend_iterative.wgsl:243-258, 283-368); the first list minimised
+      // (defend_iterative.wgsl:215-262); the first list minimised
       // too, which leaves the minimal suprema unchanged
-      if (s > TW) return T_BIG;
+      if (s > p.tw) return T_BIG;
       uint32_t sb = 0, nb = TK, ns = 0, om = 0;
       for (uint32_t q = 0; q < s; q++)
         if (!ac_insert(scr, sb, ns, om, cd.apply(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), pu0), false))
           return T_BIG;
       for (uint32_t j = 1; j < d; j++) {
-        const uint32_t w = ld(p.col, (unsigned long long)e0 + j, p.n_edges, c);
-        const uint32_t u = ld(p.wt, (unsigned long long)e0 + j, p.n_edges, c);
+        uint32_t w, u;
+        load_edge(p, c, (unsigned long long)e0 + j, w, u);
         const unsigned long long db = ld(p.desc, w, p.n_nodes, c);
         const uint32_t cb = dcnt(db);
         tot += cb;
-        if (ns * cb > TW) return T_BIG;
-        const auto pu = cd.prep(u);
+        if (ns * cb > p.tw) return T_BIG;
+        const auto pu = edge_upd(p, cd, u);
         uint32_t nn = 0;
         for (uint32_t q = 0; q < cb; q++) {
           const uint32_t bq = cd.apply(cd.to_t(lelem(db, q, arena, cap, c, p.ib, p.ibm)), pu);
@@ -1709,6 +1733,15 @@ __global__ void k_check_weights(const uint32_t *wt, unsigned long long m, uint32
 }
 
 // EnergyGame::with_reach (energygame.rs:355-365): {0} at every target.
+// Edge pairs of the lane path: successor id and the update in the codec's
+// pack_edge form (after k_fix_cols / k_check_weights).
+template <class Cd>
+__global__ void k_pack_edges(const uint32_t *col, const uint32_t *wt, unsigned long long m, unsigned long long *cw) {
+  for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < m;
+       k += (unsigned long long)gridDim.x * blockDim.x)
+    cw[k] = (unsigned long long)col[k] | ((unsigned long long)Cd::pack_edge(wt[k]) << 32);
+}
+
 __global__ void k_init_reach(unsigned long long *desc, const uint32_t *reach, unsigned long long n_reach) {
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_reach;
        i += (unsigned long long)gridDim.x * blockDim.x)
@@ -1984,6 +2017,8 @@ struct Engine::State {
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   std::vector<cudaGraphNode_t> gnodes[2];
   uint32_t g_rounds[2] = {0, 0}, g_bps[2] = {0, 0};
+  KParams g_kp[2] = {};              // the parameters the graph's nodes hold
+  bool g_kp_valid[2] = {false, false};
   unsigned long long *part = nullptr;
   size_t part_cap = 0;
   uint32_t *cnt = nullptr;
@@ -2007,6 +2042,7 @@ struct DeviceGamesImpl {
   uint32_t *row = nullptr, *col = nullptr, *wt = nullptr, *rrow = nullptr, *rcol = nullptr;
   uint8_t *flags = nullptr;
   unsigned long long *desc = nullptr, *desc_init = nullptr, *slot_new = nullptr;
+  unsigned long long *cw = nullptr;  // edge pairs (successor, packed update)
   uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr, *fpart = nullptr, *abits = nullptr, *bigq = nullptr;
   uint32_t *init_data = nullptr;
   unsigned long long init_total = 0;
@@ -2022,6 +2058,12 @@ struct DeviceGamesImpl {
   Ctr *ctr = nullptr;
   uint32_t next_stamp = 1;
   KParams kp{};
+  // bookkeeping of the solve in progress (Engine::solve_begin / solve_step)
+  struct Progress {
+    unsigned long long launches = 0, compactions = 0, round_launches = 0;
+    double round_ms = 0.0;
+    std::chrono::steady_clock::time_point t_start{};
+  } prog;
 
   template <class T>
   bool alloc(T *&p, size_t n) {
@@ -2185,6 +2227,8 @@ static geq_status staged_upload(std::vector<CopyJob> &jobs, const char *stage, c
 void *Engine::stream_handle() const { return (void *)st->stream; }
 std::shared_ptr<HostPool> Engine::host_pool() const { return st->hpool; }
 
+static geq_status static_scratch(int device, unsigned char *&out);
+
 geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
   int n = 0;
   cudaError_t e = cudaGetDeviceCount(&n);
@@ -2194,6 +2238,12 @@ geq_status Engine::create(int device, std::unique_ptr<Engine> &out) {
   CU(cudaSetDevice(device));
   cudaDeviceProp prop;
   CU(cudaGetDeviceProperties(&prop, device));
+  {
+    // reserve the scratch of geq_energy_game_run_static now (module load)
+    unsigned char *scratch = nullptr;
+    const geq_status rs = static_scratch(device, scratch);
+    if (rs) return rs;
+  }
   std::unique_ptr<Engine> eng(new Engine());
   eng->st.reset(new State());
   eng->n_sms = prop.multiProcessorCount;
@@ -2462,7 +2512,7 @@ geq_status Engine::alloc_work(DeviceGamesImpl &D, bool any_init) {
       (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, 2 * ((N + 31) / 32)) ||
       !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1) ||
       !D.alloc(D.fpart, 2 * (size_t)std::max(1, n_sms * 2)) || !D.alloc(D.abits, (N + 31) / 32) ||
-      !D.alloc(D.bigq, N))
+      !D.alloc(D.bigq, N) || !D.alloc(D.cw, M))
     return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
@@ -2511,6 +2561,10 @@ geq_status Engine::finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out) {
   CU(cudaMemcpyAsync(s.cnt, D.rrow, N * 4, cudaMemcpyDeviceToDevice, S));
   k_fill_reverse<<<grid, 256, 0, S>>>(D.row, D.col, N, M, s.cnt, D.rcol);
   if (N) k_abits<<<grid, 256, 0, S>>>(D.flags, N, (uint32_t)((N + 31) / 32), D.abits);
+  if (M) {
+    if (D.generic) k_pack_edges<CodecGen><<<grid, 256, 0, S>>>(D.col, D.wt, M, D.cw);
+    else k_pack_edges<CodecStd><<<grid, 256, 0, S>>>(D.col, D.wt, M, D.cw);
+  }
   CU(cudaMemcpyAsync(&s.h_ctr->pad, s.d_err, 4, cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   s.pool.put(roff, (N + 1) * 8);
@@ -2528,6 +2582,7 @@ geq_status Engine::finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out) {
   kp.fblocks = (uint32_t)std::max(1, n_sms * 2);
   kp.abits = D.abits;
   kp.bigq = D.bigq;
+  kp.cw = D.cw;
   kp.el = D.conf.elements; kp.mx = D.conf.max; kp.eb = D.conf.energy_bits(); kp.em = D.conf.energy_mask();
   kp.ub = D.conf.update_bits(); kp.um = D.conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
@@ -2573,6 +2628,14 @@ static geq_status compact(Engine &E, DeviceGamesImpl &dg, unsigned long long &la
   return GEQ_OK;
 }
 
+// Lane-path limits from geq_tuning.lane_limits (a zero field: the largest).
+static void set_lane_limits(KParams &kp, const geq_tuning &t) {
+  const uint32_t d = t.lane_limits & 0xFFu, w = (t.lane_limits >> 8) & 0xFFu, k = (t.lane_limits >> 16) & 0xFFu;
+  kp.td = d ? std::min(d, TD) : TD;
+  kp.tw = w ? std::min(w, TW) : TW;
+  kp.tk = k ? std::min(k, TK) : TK;
+}
+
 template <class Cd>
 static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent_t ea = nullptr,
                          cudaEvent_t eb = nullptr) {
@@ -2616,7 +2679,10 @@ static geq_status round_graph(Engine &E, const KParams &kp, bool generic, uint32
     if (ce != cudaSuccess) return fail(GEQ_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
     s.g_rounds[k] = R;
     s.g_bps[k] = E.tuning.blocks_per_sm;
-  } else {
+    s.g_kp[k] = kp;
+    s.g_kp_valid[k] = true;
+  } else if (!(s.g_kp_valid[k] && std::memcmp(&s.g_kp[k], &kp, sizeof(KParams)) == 0)) {
+    s.g_kp_valid[k] = false;
     for (cudaGraphNode_t node : s.gnodes[k]) {
       cudaGraphNodeType t;
       CU(cudaGraphNodeGetType(node, &t));
@@ -2628,15 +2694,25 @@ static geq_status round_graph(Engine &E, const KParams &kp, bool generic, uint32
       np.extra = nullptr;
       CU(cudaGraphExecKernelNodeSetParams(s.gexec[k], node, &np));
     }
+    s.g_kp[k] = kp;
+    s.g_kp_valid[k] = true;
   }
   out = s.gexec[k];
   return GEQ_OK;
 }
 
-geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
+// A solve in steps: solve_begin restarts from the uploaded initial state and
+// builds the first frontier; every solve_step runs one CUDA graph of R
+// worklist rounds (or one round as plain launches), compacts the arena when
+// needed and reports whether the frontier is empty.  solve() is begin + steps
+// until done; the serving loop interleaves the steps of several uploads on one
+// stream and retires games as their part of the frontier empties.
+geq_status Engine::solve_begin(DeviceGamesImpl &dg) {
   State &s = *st;
   cudaStream_t S = s.stream;
-  unsigned long long launches = 0, compactions = 0;
+  DeviceGamesImpl::Progress &pr = dg.prog;
+  pr = DeviceGamesImpl::Progress{};
+  pr.t_start = std::chrono::steady_clock::now();
   // restart from the uploaded initial state
   const int a0 = dg.arena_cur;
   CU(cudaEventRecord(s.ev0, S));
@@ -2655,48 +2731,53 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
     k_init_frontier_std<<<(unsigned)std::max(1, n_sms * 16), 256, 0, S>>>(dg.kp);
     k_fcount<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
     k_ffill<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
-    launches += 3;
+    pr.launches += 3;
   } else if (dg.n_reach) {
     const unsigned grid = (unsigned)std::max<unsigned long long>(
         1, std::min<unsigned long long>((dg.n_reach + 7) / 8, (unsigned long long)n_sms * 16));
     k_init_frontier<<<grid, 256, 0, S>>>(dg.kp, dg.reach, dg.n_reach);
     k_fcount<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
     k_ffill<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
-    launches += 3;
+    pr.launches += 3;
   }
   CU(cudaGetLastError());
+  return GEQ_OK;
+}
+
+geq_status Engine::solve_step(DeviceGamesImpl &dg, bool &done) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  DeviceGamesImpl::Progress &pr = dg.prog;
+  done = false;
+  set_lane_limits(dg.kp, tuning);
   const bool profile = (tuning.flags & GEQ_TUNE_PROFILE) != 0;
-  double round_ms = 0.0;
-  unsigned long long round_launches = 0;
   const bool use_graph = !(tuning.flags & (GEQ_TUNE_NO_GRAPH | GEQ_TUNE_PROFILE));
   const uint32_t R = use_graph ? std::max<uint32_t>(1, tuning.rounds_per_graph) : 1;
-  cudaGraphExec_t gexec = nullptr;
-  if (use_graph) {
-    geq_status g = round_graph(*this, dg.kp, dg.generic, R, gexec);
-    if (g) return g;
-  }
   // The device work of every launch is bounded; this bounds the host loop in
   // case the frontier never empties (GEQ_SOLVE_TIMEOUT_S seconds, default 600).
   const char *lim_env = std::getenv("GEQ_SOLVE_TIMEOUT_S");
   const double limit_s = lim_env ? std::atof(lim_env) : 600.0;
-  const auto t_start = std::chrono::steady_clock::now();
-  for (unsigned long long iter = 0;; iter++) {
+  for (;;) {
     if (use_graph) {
+      // the shared graph is pointed at this upload's parameters every step
+      cudaGraphExec_t gexec = nullptr;
+      geq_status g = round_graph(*this, dg.kp, dg.generic, R, gexec);
+      if (g) return g;
       CU(cudaGraphLaunch(gexec, S));
     } else {
       cudaEvent_t ea = profile ? s.eva : nullptr, eb = profile ? s.evb : nullptr;
       if (dg.generic) launch_round<CodecGen>(*this, dg.kp, S, ea, eb);
       else launch_round<CodecStd>(*this, dg.kp, S, ea, eb);
     }
-    launches += 4ull * R;
+    pr.launches += 4ull * R;
     CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
     CU(cudaStreamSynchronize(S));
     const Ctr c = *s.h_ctr;
     if (profile) {
       float ms = 0.f;
       CU(cudaEventElapsedTime(&ms, s.eva, s.evb));
-      round_ms += ms;
-      round_launches++;
+      pr.round_ms += ms;
+      pr.round_launches++;
     }
     if (c.error) {
       const char *what = (c.error & DERR_BOUNDS) ? "index out of range" :
@@ -2705,40 +2786,101 @@ geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
                   "device error %u (%s, line %u)", c.error, what, c.err_line);
     }
     if (c.overflow || c.arena_top > c.arena_cap - c.arena_cap / 4) {
-      geq_status a = compact(*this, dg, launches);
+      geq_status a = compact(*this, dg, pr.launches);
       if (a) return a;
-      compactions++;
-      if (c.overflow) continue;
+      pr.compactions++;
+      if (c.overflow) continue;  // the halted rounds run again
     }
-    if (c.fsize[c.cur] == 0) break;
-    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    if (c.fsize[c.cur] == 0) {
+      done = true;
+      dg.next_stamp = c.stamp + 2u;
+      return GEQ_OK;
+    }
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - pr.t_start).count();
     if (el > limit_s) return fail(GEQ_ERR_TIMEOUT, "no fixpoint after %llu rounds (%.0f s)", c.rounds, el);
+    return GEQ_OK;
   }
-  CU(cudaEventRecord(s.ev1, S));
+}
+
+geq_status Engine::solve_stats(DeviceGamesImpl &dg, geq_solve_stats *stats) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
   CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
   CU(cudaStreamSynchronize(S));
   const Ctr c = *s.h_ctr;
-  dg.next_stamp = c.stamp + 2u;
-#if GEQ_PATH_PROFILE
-  std::fprintf(stderr, "GEQ_PROF");
-  for (int i = 0; i < 32; i++) std::fprintf(stderr, " %llu", c.prof[i]);
-  std::fprintf(stderr, "\n");
-#endif
   if (stats) {
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, s.ev0, s.ev1);
+    *stats = geq_solve_stats{};
     stats->rounds = c.rounds;
     stats->positions_computed = c.positions;
     stats->edges_relaxed = c.edges;
     stats->algorithmic_bytes = c.bytes;
-    stats->arena_compactions = compactions;
-    stats->kernel_launches = launches;
-    stats->device_ms = ms;
-    stats->round_kernel_ms = round_ms;
-    stats->round_kernel_launches = round_launches;
+    stats->arena_compactions = dg.prog.compactions;
+    stats->kernel_launches = dg.prog.launches;
+    stats->round_kernel_ms = dg.prog.round_ms;
+    stats->round_kernel_launches = dg.prog.round_launches;
   }
   return GEQ_OK;
 }
+
+geq_status Engine::solve(DeviceGamesImpl &dg, geq_solve_stats *stats) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  geq_status st_ = solve_begin(dg);
+  if (st_) return st_;
+  for (bool done = false; !done;)
+    if ((st_ = solve_step(dg, done))) return st_;
+  CU(cudaEventRecord(s.ev1, S));
+  if ((st_ = solve_stats(dg, stats))) return st_;
+#if GEQ_PATH_PROFILE
+  {
+    const Ctr c = *s.h_ctr;
+    std::fprintf(stderr, "GEQ_PROF");
+    for (int i = 0; i < 32; i++) std::fprintf(stderr, " %llu", c.prof[i]);
+    std::fprintf(stderr, "\n");
+  }
+#endif
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, s.ev0, s.ev1);
+    stats->device_ms = ms;
+  }
+  return GEQ_OK;
+}
+
+// Games with at least one position in the current frontier; the others
+// have reached their fixpoint (games share no edges, so a game without a
+// frontier position never changes again).
+__global__ void k_active_games(const KParams p, const unsigned long long *node_base, uint32_t n_games,
+                               uint8_t *active) {
+  const Ctr *c = p.ctr;
+  const uint32_t cur = c->cur, fs = c->fsize[cur];
+  const uint32_t *F = cur ? p.front1 : p.front0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < fs; i += gridDim.x * blockDim.x) {
+    const uint32_t v = F[i];
+    if (v < p.n_nodes) active[game_of(node_base, n_games, v)] = 1;
+  }
+}
+
+geq_status Engine::active_games(DeviceGamesImpl &dg, std::vector<uint8_t> &active) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  const uint32_t G = dg.n_games;
+  uint8_t *d_act = (uint8_t *)s.pool.get(std::max<uint32_t>(G, 1));
+  if (!d_act) return fail(GEQ_ERR_OUT_OF_MEMORY, "active flags");
+  CU(cudaMemsetAsync(d_act, 0, G, S));
+  k_active_games<<<(unsigned)std::max(1, n_sms * 4), 256, 0, S>>>(dg.kp, dg.d_node_base, G, d_act);
+  active.assign(G, 0);
+  CU(cudaMemcpyAsync(active.data(), d_act, G, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  s.pool.put(d_act, std::max<uint32_t>(G, 1));
+  CU(cudaGetLastError());
+  return GEQ_OK;
+}
+
+uint32_t Engine::game_positions(const DeviceGamesImpl &dg, uint32_t g) {
+  return (uint32_t)(dg.node_base[g + 1] - dg.node_base[g]);
+}
+uint32_t Engine::n_games_of(const DeviceGamesImpl &dg) { return dg.n_games; }
 
 // Result lists of all positions: gathered on the device (counts, scan,
 // gather into one buffer, per-game relative offsets), then read back.  The
@@ -3213,23 +3355,19 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
   }
 }
 
-namespace {
-std::mutex g_static_mu;
-void *g_static_ptr[64] = {};
-}  // namespace
-
-// Address of the scratch on `device` (current), looked up once per device.
+// Device address of the scratch on the current device.  Looked up on every
+// call (cheap once the module is loaded), so that no address outlives the
+// context it belongs to (a cudaDeviceReset makes a new one).  The first
+// lookup on a device loads the module and with it reserves the array:
+// Engine::create does that lookup, so the scratch is reserved when a
+// context is created and not inside a later geq_energy_game_run_static.
 static geq_status static_scratch(int device, unsigned char *&out) {
-  if (device < 0 || device >= 64) return fail(GEQ_ERR_NO_DEVICE, "device %d out of range", device);
-  std::lock_guard<std::mutex> g(g_static_mu);
-  if (!g_static_ptr[device]) {
-    void *ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
-    if (e != cudaSuccess || !ptr)
-      return fail(GEQ_ERR_CUDA, "cudaGetSymbolAddress of the static scratch: %s", cudaGetErrorString(e));
-    g_static_ptr[device] = ptr;
-  }
-  out = (unsigned char *)g_static_ptr[device];
+  (void)device;
+  void *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+  if (e != cudaSuccess || !ptr)
+    return fail(GEQ_ERR_CUDA, "cudaGetSymbolAddress of the static scratch: %s", cudaGetErrorString(e));
+  out = (unsigned char *)ptr;
   return GEQ_OK;
 }
 
@@ -3290,6 +3428,8 @@ static void block_params(const BlockLayout &L, unsigned char *base, size_t bytes
   kp.ib = conf.elements * conf.energy_bits();
   kp.ibm = kp.ib >= 32 ? 0xFFFFFFFFu : ((1u << kp.ib) - 1u);
   kp.inl = std::min<uint32_t>(7u, 60u / kp.ib);
+  kp.cw = nullptr;
+  set_lane_limits(kp, geq_tuning{});
   sa = StaticArgs{};
   sa.reach = explicit_reach ? (const uint32_t *)(base + L.reach) : nullptr;
   sa.n_reach = explicit_reach ? n_reach : 0u;

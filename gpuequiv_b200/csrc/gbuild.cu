@@ -112,77 +112,131 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_down(const uint32_t *in, uint32
     }
 }
 
-// Three arrays scanned in one pass (the bounds of CountF).
-struct Scan3 {
+// Single-pass scans of up to three arrays, each with its item count read on
+// the device (chained scan with decoupled look-back): block b scans tiles b,
+// b + G, b + 2G, ... of SCAN_TILE values.  A tile publishes its sum at once,
+// then looks back over the tiles before it -- adding published sums until it
+// meets a published inclusive prefix -- and publishes its own inclusive
+// prefix.  The status words carry the scan's sequence number (bumped by the
+// last block of every launch), so no clearing is needed between launches.
+// The look-back waits are bounded: a tile that gives up sums its
+// predecessors' inputs itself, so the result never depends on how the blocks
+// were scheduled.
+struct ScanR {
   const uint32_t *in[3];
   uint32_t *out[3];
+  const unsigned long long *np[3];
+  unsigned long long *tot[3];
 };
-// Scans of R arrays whose length is read on the device: a fixed grid of nb
-// blocks, block b scanning the contiguous chunk b of ceil(n / nb) values tile
-// by tile (reduce, scan of the nb block sums, rescan with the block's carry).
-template <int R>
-__global__ void __launch_bounds__(SCAN_T) k_cscan_up(Scan3 a, const unsigned long long *np, const unsigned long long *go,
-                                                     unsigned long long *part, uint32_t nb) {
-  if (!*go) return;
-  const uint32_t n = (uint32_t)*np, chunk = (n + nb - 1) / nb;
-  const uint32_t lo = min(n, blockIdx.x * chunk), hi = min(n, lo + chunk);
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    unsigned long long s = 0;
-    for (uint32_t base = lo + threadIdx.x * SCAN_ITEMS; base < hi; base += SCAN_TILE)
-#pragma unroll
-      for (int k = 0; k < SCAN_ITEMS; k++)
-        if (base + k < hi) s += a.in[r][base + k];
-    unsigned long long total;
-    block_scan(s, total);
-    if (threadIdx.x == 0) part[r * nb + blockIdx.x] = total;
-  }
+struct LbCtl {
+  uint32_t seq, done;
+};
+constexpr uint32_t LB_AGG = 1u, LB_INC = 2u;
+constexpr uint32_t LB_SPIN_LIMIT = 1u << 16;
+
+__device__ __forceinline__ uint32_t ld_vol(const uint32_t *p) { return *(const volatile uint32_t *)p; }
+__device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p) {
+  return *(const volatile unsigned long long *)p;
 }
+
 template <int R>
-__global__ void __launch_bounds__(SCAN_T) k_cscan_mid(unsigned long long *part, uint32_t nb, unsigned long long *tot,
-                                                      const unsigned long long *go) {
-  if (!*go) return;
-  for (int r = 0; r < R; r++) {
-    unsigned long long carry = 0;
-    for (uint32_t b0 = 0; b0 < nb; b0 += SCAN_T) {
-      const uint32_t i = b0 + threadIdx.x;
-      const unsigned long long x = i < nb ? part[r * nb + i] : 0ull;
-      unsigned long long total;
-      const unsigned long long e = block_scan(x, total);
-      if (i < nb) part[r * nb + i] = carry + e;
-      carry += total;
-    }
-    if (threadIdx.x == 0) tot[r] = carry;
-  }
-}
-template <int R>
-__global__ void __launch_bounds__(SCAN_T) k_cscan_down(Scan3 a, const unsigned long long *np,
-                                                       const unsigned long long *go, const unsigned long long *part,
-                                                       uint32_t nb) {
-  if (!*go) return;
-  const uint32_t n = (uint32_t)*np, chunk = (n + nb - 1) / nb;
-  const uint32_t lo = min(n, blockIdx.x * chunk), hi = min(n, lo + chunk);
+__global__ void __launch_bounds__(SCAN_T) k_lbscan(ScanR a, const unsigned long long *go, LbCtl *ctl, uint32_t *flag,
+                                                   unsigned long long *agg, unsigned long long *inc, uint32_t tcap) {
+  __shared__ uint32_t s_seq, s_gaveup;
+  __shared__ unsigned long long s_prefix;
+  const bool run = !go || *go;
+  if (threadIdx.x == 0) s_seq = ld_vol(&ctl->seq) & 0x3FFFFFFFu;
+  __syncthreads();
+  const uint32_t tag = s_seq << 2;
 #pragma unroll
-  for (int r = 0; r < R; r++) {
-    unsigned long long carry = part[r * nb + blockIdx.x];
-    for (uint32_t t0 = lo; t0 < hi; t0 += SCAN_TILE) {
-      const uint32_t base = t0 + threadIdx.x * SCAN_ITEMS;
+  for (int r = 0; r < R && run; r++) {
+    const uint32_t n = (uint32_t)*a.np[r];
+    const uint32_t ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+    uint32_t *fl = flag + (size_t)r * tcap;
+    unsigned long long *ag = agg + (size_t)r * tcap, *ic = inc + (size_t)r * tcap;
+    if (ntiles == 0 && blockIdx.x == 0 && threadIdx.x == 0) *a.tot[r] = 0ull;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      const bool status = t < tcap;  // tiles beyond the status space take the direct path
+      const uint32_t base = t * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
       uint32_t v[SCAN_ITEMS];
       unsigned long long s = 0;
 #pragma unroll
       for (int k = 0; k < SCAN_ITEMS; k++) {
-        v[k] = base + k < hi ? a.in[r][base + k] : 0u;
+        v[k] = base + k < n ? a.in[r][base + k] : 0u;
         s += v[k];
       }
       unsigned long long total;
-      unsigned long long e = block_scan(s, total) + carry;
+      unsigned long long e = block_scan(s, total);
+      if (threadIdx.x == 0) {
+        unsigned long long prefix = 0;
+        uint32_t gaveup = 0;
+        if (!status) {
+          gaveup = 1;
+        } else if (t == 0) {
+          ic[0] = total;
+          __threadfence();
+          *(volatile uint32_t *)&fl[0] = tag | LB_INC;
+        } else {
+          ag[t] = total;
+          __threadfence();
+          *(volatile uint32_t *)&fl[t] = tag | LB_AGG;
+          uint32_t j = t - 1, spins = 0;
+          for (;;) {
+            const uint32_t f = ld_vol(&fl[j]);
+            if ((f & ~3u) != tag || (f & 3u) == 0u) {
+              if (++spins > LB_SPIN_LIMIT) {
+                gaveup = 1;
+                break;
+              }
+              __nanosleep(64);
+              continue;
+            }
+            __threadfence();
+            if ((f & 3u) == LB_INC) {
+              prefix += ld_vol(&ic[j]);
+              break;
+            }
+            prefix += ld_vol(&ag[j]);
+            j--;  // tile 0 always publishes an inclusive prefix
+          }
+        }
+        s_prefix = prefix;
+        s_gaveup = gaveup;
+      }
+      __syncthreads();
+      if (s_gaveup) {
+        // the block sums the inputs of every tile before this one itself
+        unsigned long long part = 0;
+        for (uint32_t i = threadIdx.x; i < t * SCAN_TILE; i += SCAN_T) part += a.in[r][i];
+        unsigned long long all;
+        block_scan(part, all);
+        if (threadIdx.x == 0) s_prefix = all;
+        __syncthreads();
+      }
+      const unsigned long long prefix = s_prefix;
+      if (threadIdx.x == 0 && t > 0 && status) {
+        ic[t] = prefix + total;
+        __threadfence();
+        *(volatile uint32_t *)&fl[t] = tag | LB_INC;
+      }
+      if (threadIdx.x == 0 && t + 1 == ntiles) *a.tot[r] = prefix + total;
+      e += prefix;
 #pragma unroll
       for (int k = 0; k < SCAN_ITEMS; k++)
-        if (base + k < hi) {
+        if (base + k < n) {
           a.out[r][base + k] = (uint32_t)e;
           e += v[k];
         }
-      carry += total;
+      __syncthreads();
+    }
+  }
+  // the last block of the launch moves the sequence on
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&ctl->done, 1u) == gridDim.x - 1) {
+      ctl->done = 0;
+      ctl->seq = ctl->seq + 1u;
+      __threadfence();
     }
   }
 }
@@ -375,6 +429,12 @@ struct DevBackend {
   unsigned long long *part = nullptr;
   uint32_t part_cap = 0;
   uint32_t launches = 0;
+  // single-pass scans: sequence/arrival counters and per-tile status of up to
+  // three arrays (lb_cap tiles each)
+  LbCtl *lb_ctl = nullptr;
+  uint32_t *lb_flag = nullptr;
+  unsigned long long *lb_agg = nullptr, *lb_inc = nullptr;
+  uint32_t lb_cap = 0;
 
   void note(cudaError_t e) {
     if (e != cudaSuccess && err == cudaSuccess) err = e;
@@ -442,33 +502,49 @@ struct DevBackend {
     launches++;
   }
   uint32_t cnb() const { return (uint32_t)n_sms * 2; }
-  bool reserve_part() {
-    if (part_cap >= 3 * cnb()) return true;
-    release(part);
-    part_cap = std::max<uint32_t>(3 * cnb(), 1024);
-    part = (unsigned long long *)alloc((size_t)part_cap * 8);
-    if (!part) {
-      part_cap = 0;
-      note(cudaErrorMemoryAllocation);
-      return false;
+  // status space for scans of up to max_items values (called whenever the
+  // level buffers are sized, before a level is recorded)
+  void scan_capacity(uint64_t max_items) {
+    const uint64_t tiles = (max_items + SCAN_TILE - 1) / SCAN_TILE + 1;
+    if (lb_ctl && tiles <= lb_cap) return;
+    const uint32_t cap = (uint32_t)std::max<uint64_t>(tiles * 2, 1024);
+    release(lb_flag);
+    release(lb_agg);
+    release(lb_inc);
+    lb_flag = (uint32_t *)alloc((size_t)3 * cap * 4);
+    lb_agg = (unsigned long long *)alloc((size_t)3 * cap * 8);
+    lb_inc = (unsigned long long *)alloc((size_t)3 * cap * 8);
+    if (!lb_ctl) {
+      lb_ctl = (LbCtl *)alloc(sizeof(LbCtl));
+      if (lb_ctl) fill(lb_ctl, 0, sizeof(LbCtl));
     }
-    return true;
+    if (!lb_flag || !lb_agg || !lb_inc || !lb_ctl) {
+      lb_cap = 0;
+      note(cudaErrorMemoryAllocation);
+      return;
+    }
+    fill(lb_flag, 0, (size_t)3 * cap * 4);  // tag 0 with state 0: never ready
+    lb_cap = cap;
+  }
+  template <int R>
+  void lbscan(const ScanR &a, const unsigned long long *go) {
+    if (!lb_cap) scan_capacity(0);
+    k_lbscan<R><<<cnb(), SCAN_T, 0, s>>>(a, go, lb_ctl, lb_flag, lb_agg, lb_inc, lb_cap);
+    launches++;
   }
   void scan_d(const uint32_t *in, uint32_t *out, const unsigned long long *np, unsigned long long *tot,
               const unsigned long long *go) {
-    const Scan3 a{{in, in, in}, {out, out, out}};
-    k_cscan_up<1><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
-    k_cscan_mid<1><<<1, SCAN_T, 0, s>>>(part, cnb(), tot, go);
-    k_cscan_down<1><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
-    launches += 3;
+    lbscan<1>(ScanR{{in, in, in}, {out, out, out}, {np, np, np}, {tot, tot, tot}}, go);
+  }
+  // two scans with their own counts in one launch
+  void scan2_d(const uint32_t *i0, uint32_t *o0, const unsigned long long *np0, unsigned long long *t0,
+               const uint32_t *i1, uint32_t *o1, const unsigned long long *np1, unsigned long long *t1,
+               const unsigned long long *go) {
+    lbscan<2>(ScanR{{i0, i1, i1}, {o0, o1, o1}, {np0, np1, np1}, {t0, t1, t1}}, go);
   }
   void scan3_d(const uint32_t *i0, const uint32_t *i1, const uint32_t *i2, uint32_t *o0, uint32_t *o1, uint32_t *o2,
                const unsigned long long *np, unsigned long long *tot, const unsigned long long *go) {
-    const Scan3 a{{i0, i1, i2}, {o0, o1, o2}};
-    k_cscan_up<3><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
-    k_cscan_mid<3><<<1, SCAN_T, 0, s>>>(part, cnb(), tot, go);
-    k_cscan_down<3><<<cnb(), SCAN_T, 0, s>>>(a, np, go, part, cnb());
-    launches += 3;
+    lbscan<3>(ScanR{{i0, i1, i2}, {o0, o1, o2}, {np, np, np}, {tot, tot + 1, tot + 2}}, go);
   }
   // ---- the level loop as a CUDA graph: a WHILE node whose body is one
   // recorded level followed by k_level_cond, so that one launch runs levels
@@ -482,7 +558,6 @@ struct DevBackend {
   bool plain = false;  // levels as plain launches, one per host sync (profilers see every kernel)
   bool has_graph() const { return gexec != nullptr; }
   void begin_capture() {
-    reserve_part();
     if (plain) return;  // the level that "capture" enqueues runs as it is
     if (!d_loop) d_loop = (uint32_t *)alloc(2 * sizeof(uint32_t));
     if (!d_loop) note(cudaErrorMemoryAllocation);
@@ -528,6 +603,8 @@ struct DevBackend {
     drop_graph();
     if (d_loop) cudaFreeAsync(d_loop, s);
     if (part) cudaFreeAsync(part, s);
+    for (void *q : {(void *)lb_ctl, (void *)lb_flag, (void *)lb_agg, (void *)lb_inc})
+      if (q) cudaFreeAsync(q, s);
   }
 };
 
@@ -731,11 +808,15 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
 }
 
 // GameBuild::compare of every job on the device, handed to the solver as an
-// upload (the graphs never leave the device).  jobs whose game exceeds
-// max_positions (0 = no bound) fail with GEQ_ERR_OUT_OF_MEMORY.
+// upload (the graphs never leave the device).  Jobs whose game exceeds
+// max_positions (0 = no bound) fail the call with GEQ_ERR_OUT_OF_MEMORY --
+// unless `over` is given: then over[j] marks them and they are uploaded as
+// the part the builder numbered before it stopped expanding them (a well
+// formed game whose unexpanded positions have no successors), whose lists
+// the caller must discard.
 geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *start_off,
                             const uint32_t *p, const uint32_t *q, uint64_t max_positions, GamesPtr &out,
-                            double *build_ms, std::vector<uint8_t> *trivial) {
+                            double *build_ms, std::vector<uint8_t> *trivial, std::vector<uint8_t> *over) {
   DeviceBuild db;
   geq_status st = device_build(eng, device, n_jobs, L, start_off, p, q, max_positions, db, trivial);
   if (st) return st;
@@ -744,9 +825,13 @@ geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts 
   db.be.copy(jover.data(), db.r.jover, (size_t)n_jobs * 4);
   db.be.fetch(jm.data(), db.r.jm, (size_t)n_jobs * 4);
   if (!db.be.ok()) return fail(GEQ_ERR_CUDA, "device game build: %s", cudaGetErrorString(db.be.err));
-  for (uint32_t j = 0; j < n_jobs; j++)
-    if (jover[j]) return fail(GEQ_ERR_OUT_OF_MEMORY, "job %u: game exceeds %llu positions", j,
-                              (unsigned long long)max_positions);
+  if (over) over->assign(n_jobs, 0);
+  for (uint32_t j = 0; j < n_jobs; j++) {
+    if (!jover[j]) continue;
+    if (!over)
+      return fail(GEQ_ERR_OUT_OF_MEMORY, "job %u: game exceeds %llu positions", j, (unsigned long long)max_positions);
+    (*over)[j] = 1;
+  }
   if (build_ms) *build_ms = db.upload_ms + db.minimize_ms + db.build_ms;
   // jobs without positions (no start pairs, or the bisimilar short cut) add
   // nothing to the arrays: the games are the other jobs, in order

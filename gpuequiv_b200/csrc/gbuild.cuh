@@ -760,8 +760,10 @@ struct LevelEndF {
 //   template <class F> void each(uint32_t n, const F &);
 //   void scan(const uint32_t *in, uint32_t *out, uint32_t n, unsigned long long *dev_total);
 //   void gen_heavy(const View &, const unsigned long long *go);  (the positions CountF queued in v.hq)
-//   each_d / scan_d / scan3_d: the same with the item count read on the device
-//     (*n), doing nothing while *go == 0 (a stalled or finished loop);
+//   each_d / scan_d / scan2_d / scan3_d: the same with the item count read on
+//     the device (*n), doing nothing while *go == 0 (a stalled or finished
+//     loop); scan2_d scans two arrays with their own counts;
+//   void scan_capacity(uint64_t max_items): room for scans of that many items;
 //   begin_capture / end_capture(go) / run_graph(limit) / note_levels /
 //     has_graph / drop_graph: one level recorded once and run repeatedly
 //     (on the device a CUDA graph WHILE node: up to `limit` levels per launch,
@@ -1021,6 +1023,7 @@ class Builder {
     v_.scap = scap_;
     v_.ncap = ncap_;
     v_.t = d_tot_ ? d_tot_->t : nullptr;
+    be_.scan_capacity(std::max<uint64_t>(capF_, capS_));
   }
   const unsigned long long *tp(int k) const { return &d_tot_->t[k]; }
   // One breadth-first level, every count read on the device (no host sync):
@@ -1038,8 +1041,7 @@ class Builder {
     be_.each_d(tp(T_C), capC_, go, SetFillF{v_});
     be_.each_d(tp(T_S), capS_, go, SuccProbeF{v_});
     be_.each_d(tp(T_S), capS_, go, SuccFlagF{v_});
-    be_.scan_d(v_.snew, v_.srank, tp(T_S), &d_tot_->t[T_NEW], go);
-    be_.scan_d(v_.fcnt, v_.feoff, tp(T_F), &d_tot_->t[T_EDGE], go);
+    be_.scan2_d(v_.snew, v_.srank, tp(T_S), &d_tot_->t[T_NEW], v_.fcnt, v_.feoff, tp(T_F), &d_tot_->t[T_EDGE], go);
     be_.each_d(tp(T_S), capS_, go, SuccNewF{v_});
     be_.each_d(tp(T_S), capS_, go, SuccFillF{v_});
     be_.each_d(tp(T_F), capF_, go, EdgeF{v_});

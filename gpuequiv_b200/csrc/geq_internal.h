@@ -184,6 +184,15 @@ class Engine {
   // games already on the device (BuiltGames), standard reach
   geq_status upload_built(const BuiltGames &b, GamesPtr &out);
   geq_status solve(DeviceGamesImpl &dg, geq_solve_stats *stats);
+  // the same in steps: restart from the uploaded state, then one graph of
+  // rounds per step (done: the frontier is empty); counters of the solve so far
+  geq_status solve_begin(DeviceGamesImpl &dg);
+  geq_status solve_step(DeviceGamesImpl &dg, bool &done);
+  geq_status solve_stats(DeviceGamesImpl &dg, geq_solve_stats *stats);
+  // active[g] = 1 while game g has a position in the frontier
+  geq_status active_games(DeviceGamesImpl &dg, std::vector<uint8_t> &active);
+  static uint32_t game_positions(const DeviceGamesImpl &dg, uint32_t g);
+  static uint32_t n_games_of(const DeviceGamesImpl &dg);
   // All positions of all games.
   geq_status download(DeviceGamesImpl &dg, geq_solution &sol);
   // download in two steps: prepare gathers every list on the device and
@@ -239,7 +248,14 @@ struct Lts;
 // there are none).
 geq_status build_and_upload(Engine &eng, int device, uint32_t n_jobs, const Lts *const *L, const uint32_t *start_off,
                             const uint32_t *p, const uint32_t *q, uint64_t max_positions, GamesPtr &out,
-                            double *build_ms, std::vector<uint8_t> *trivial = nullptr);
+                            double *build_ms, std::vector<uint8_t> *trivial = nullptr,
+                            std::vector<uint8_t> *over = nullptr);
+
+// Games whose EnergyConf is outside the thermometer codecs (Conf::supported
+// false), or every game under GEQ_TUNE_FORCE_WIDE: the multi-word solver of
+// wide.cu, one game after the other on the engine's stream.
+bool wide_supported(const Conf &c, std::string *why = nullptr);
+geq_status solve_wide(Engine &e, int device, std::vector<GameInput> &in, geq_solution &sol);
 
 // A large batch split in two halves by positions on engines ea and eb: the
 // upload of the second half overlaps the solve of the first.

@@ -1,8 +1,12 @@
 // server.cpp - the serving loop: queued single-game requests solved in
 // batches by pipeline threads, each owning an Engine (stream, staging,
-// device pool, CUDA graphs).  While one pipeline solves its batch on the
-// device, another stages and uploads the next, so the device always has a
-// batch in flight (continuous batching over alternating pipelines).
+// device pool, CUDA graphs).  A pipeline keeps up to MAX_SESSIONS admitted
+// batches resident and runs one step (a CUDA graph of worklist rounds) of
+// each in turn: requests that arrive while batches are on the device are
+// admitted at the next step boundary, as device memory (the admission budget)
+// allows, and every game is answered as soon as its own part of the frontier
+// is empty, not when its batch ends.  Several pipelines do this on their own
+// streams, so one stages and uploads while another's rounds run.
 //
 // A request is one game with standard initialisation, as EnergyGame::run
 // after EnergyGame::standard_reach (energygame.rs:347-352, :379-383), or one
@@ -32,6 +36,8 @@ namespace {
 // per edge successor, update and reverse entry; doubled for the pool's
 // power-of-two blocks, plus the fixed minimum arena.
 constexpr uint64_t BATCH_BASE_BYTES = 32ull << 20;
+// resident batches per pipeline (more arrivals wait and are batched together)
+constexpr size_t MAX_SESSIONS = 4;
 uint64_t game_footprint(uint64_t n, uint64_t m) { return 2 * (70 * n + 12 * m) + 4096; }
 // A compare query's game is not known before it is built: estimated at 16
 // positions and 64 edges per state and transition of its LTS, plus the
@@ -95,67 +101,104 @@ std::unique_ptr<geq_solution> split_one(const geq_solution &all, uint32_t g) {
   return s;
 }
 
-// Compare queries of a batch: minimised, built and solved together on the
-// device (the path of geq_compare_batch); each request gets the energies of
-// its start position.  On failure of several, each is retried alone.
-void run_compares(Engine &e, int device, std::vector<Request *> &batch) {
-  const uint32_t n = (uint32_t)batch.size();
-  std::vector<const Lts *> L(n);
-  std::vector<uint32_t> p(n), q(n), start_off(n + 1);
-  for (uint32_t i = 0; i < n; i++) {
-    L[i] = &batch[i]->lts;
-    p[i] = batch[i]->p;
-    q[i] = batch[i]->q;
-  }
-  for (uint32_t i = 0; i <= n; i++) start_off[i] = i;
-  std::vector<uint8_t> trivial;
-  GamesPtr dg;
-  geq_solution part;
-  geq_status st = build_and_upload(e, device, n, L.data(), start_off.data(), p.data(), q.data(), 0, dg, nullptr,
-                                   &trivial);
-  if (!st && dg) st = e.solve(*dg, &part.stats);
-  if (!st && dg) {
-    const uint32_t games = (uint32_t)std::count(trivial.begin(), trivial.end(), 0);
-    std::vector<uint32_t> first(games, 0), count(games, 1);
-    st = e.download_selected(*dg, first, count, part);
-  }
-  dg.reset();
-  if (st) {
-    if (n > 1) {
-      for (Request *r : batch) {
-        std::vector<Request *> one{r};
-        run_compares(e, device, one);
-      }
-      return;
-    }
-    batch[0]->st = st;
-    batch[0]->err = geq_last_error();
-    return;
-  }
-  uint32_t k = 0;
-  for (uint32_t i = 0; i < n; i++) {
+// Games of confs without a thermometer codec: the multi-word solver, one
+// request at a time.
+void run_wide(Engine &e, int device, std::vector<Request *> &batch) {
+  for (Request *r : batch) {
+    std::vector<GameInput> in(1);
+    GameInput &gi = in[0];
+    gi.g.conf = r->conf;
+    gi.g.n_vertices = r->n;
+    gi.g.row_offsets = r->row.data();
+    gi.g.column_indices = r->col.data();
+    gi.g.weights = r->wt.data();
+    gi.g.attacker_pos = r->att.data();
+    gi.to_reach = r->reach.data();
+    gi.n_reach = (uint32_t)r->reach.size();
     std::unique_ptr<geq_solution> sol(new geq_solution());
-    sol->energy_size = 1;
-    sol->n_vertices.assign(1, 1);
-    sol->offsets_base.assign(1, 0);
-    sol->data_base.assign(1, 0);
-    sol->stats = part.stats;
-    if (trivial[i]) {
-      sol->offsets = {0, 0};  // bisimilar: lib.rs:279-281
+    const geq_status st = solve_wide(e, device, in, *sol);
+    if (st) {
+      r->st = st;
+      r->err = geq_last_error();
     } else {
-      const uint64_t cnt = part.offsets[part.offsets_base[k] + 1];
-      sol->offsets = {0, cnt};
-      sol->data.assign(part.data.begin() + part.data_base[k], part.data.begin() + part.data_base[k] + cnt);
-      k++;
+      r->sol = std::move(sol);
     }
-    batch[i]->sol = std::move(sol);
   }
 }
 
-// Upload, solve and download one batch on engine `e`; on failure of a batch
-// of several games each game is retried alone so that only the faulty one
-// fails.
-void run_batch(Engine &e, std::vector<Request *> &batch) {
+// ---- sessions: uploaded batches that are solved a step at a time ------------
+// A pipeline keeps every batch it has admitted resident as a session and runs
+// one step (one CUDA graph of worklist rounds) of each session in turn, so a
+// batch admitted while others are on the device starts at the next step
+// boundary instead of after them.  After every step the games whose part of
+// the frontier is empty have reached their fixpoint (games share no edges):
+// their lists are read back and their requests answered at once.
+struct Session {
+  GamesPtr dg;
+  std::vector<Request *> req;    // game g -> its request (null: nobody waits for it)
+  std::vector<uint8_t> retired;  // per game
+  bool first_only = false;       // compare queries: only the start position's energies
+  uint64_t footprint = 0;
+  uint32_t live = 0;             // games not retired
+};
+
+void finish(geq_server *s, const std::vector<Request *> &done) {
+  if (done.empty()) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (Request *r : done) {
+      r->state = 2;
+      if (r->st) s->stats.failed++;
+      else s->stats.completed++;
+    }
+    s->stats.running -= done.size();
+  }
+  s->cv_done.notify_all();
+}
+
+void fail_req(Request *r, geq_status st, const std::string &msg, std::vector<Request *> &done) {
+  r->st = st;
+  r->err = msg;
+  done.push_back(r);
+}
+
+// Read back and answer the listed games of a session.
+geq_status retire(Engine &e, Session &ss, const std::vector<uint32_t> &games, std::vector<Request *> &done) {
+  const uint32_t G = Engine::n_games_of(*ss.dg);
+  std::vector<uint32_t> first(G, 0), count(G, 0), want;
+  for (uint32_t g : games)
+    if (ss.req[g]) {
+      count[g] = ss.first_only ? 1u : Engine::game_positions(*ss.dg, g);
+      want.push_back(g);
+    }
+  geq_solve_stats stt{};
+  geq_status st = e.solve_stats(*ss.dg, &stt);
+  geq_solution part;
+  if (!st && !want.empty()) st = e.download_selected(*ss.dg, first, count, part);
+  for (uint32_t g : games) {
+    ss.retired[g] = 1;
+    ss.live--;
+  }
+  if (st) {
+    const std::string msg = geq_last_error();
+    for (uint32_t g : want) fail_req(ss.req[g], st, msg, done);
+    return st;
+  }
+  part.stats = stt;
+  for (uint32_t g : want) {
+    Request *r = ss.req[g];
+    r->sol = split_one(part, g);
+    done.push_back(r);
+  }
+  return GEQ_OK;
+}
+
+// Games of one conf with a thermometer codec: a lone small game in one
+// launch of the one-block solver, else an upload that becomes a session.  An
+// upload of several games that fails is retried game by game, so that a
+// malformed game fails alone.
+void start_games(Engine &e, std::vector<Request *> &batch, uint64_t footprint,
+                 std::vector<std::unique_ptr<Session>> &out, std::vector<Request *> &done) {
   std::vector<GameInput> in(batch.size());
   for (size_t i = 0; i < batch.size(); i++) {
     Request &r = *batch[i];
@@ -170,87 +213,197 @@ void run_batch(Engine &e, std::vector<Request *> &batch) {
     gi.n_reach = (uint32_t)r.reach.size();
   }
   if (batch.size() == 1) {
-    // a lone small game: one launch of the one-block solver
     std::unique_ptr<geq_solution> one(new geq_solution());
     bool handled = false;
     const geq_status st = e.solve_small(in[0], *one, handled);
-    if (st) {
-      batch[0]->st = st;
-      batch[0]->err = geq_last_error();
-      return;
-    }
+    if (st) return fail_req(batch[0], st, geq_last_error(), done);
     if (handled) {
       batch[0]->sol = std::move(one);
+      done.push_back(batch[0]);
       return;
     }
   }
-  GamesPtr dg;
-  geq_solution sol;
-  geq_status st = e.upload(in, dg);
-  if (!st) st = e.solve(*dg, &sol.stats);
-  if (!st) st = e.download(*dg, sol);
-  dg.reset();
+  std::unique_ptr<Session> ss(new Session());
+  geq_status st = e.upload(in, ss->dg);
+  if (!st) st = e.solve_begin(*ss->dg);
   if (st) {
     if (batch.size() > 1) {
       for (Request *r : batch) {
         std::vector<Request *> one{r};
-        run_batch(e, one);
+        start_games(e, one, r->footprint, out, done);
       }
       return;
     }
-    batch[0]->st = st;
-    batch[0]->err = geq_last_error();
-    return;
+    return fail_req(batch[0], st, geq_last_error(), done);
   }
-  parallel_for((uint32_t)batch.size(), [&](uint32_t i) { batch[i]->sol = split_one(sol, i); },
-               batch.size() >= 256 ? 0u : 1u);
+  ss->req.assign(batch.begin(), batch.end());
+  ss->retired.assign(batch.size(), 0);
+  ss->live = (uint32_t)batch.size();
+  ss->footprint = footprint;
+  out.push_back(std::move(ss));
+}
+
+// Compare queries: minimised and built together on the device (the path of
+// geq_compare_batch), then a session whose games answer with their start
+// position.  Bisimilar pairs are answered at once with no energies
+// (lib.rs:279-281); a query whose game exceeds the position bound fails
+// alone.  If the build of several fails, each query is tried alone.
+void start_compares(Engine &e, int device, uint64_t max_positions, std::vector<Request *> &batch, uint64_t footprint,
+                    std::vector<std::unique_ptr<Session>> &out, std::vector<Request *> &done) {
+  const uint32_t n = (uint32_t)batch.size();
+  std::vector<const Lts *> L(n);
+  std::vector<uint32_t> p(n), q(n), start_off(n + 1);
+  for (uint32_t i = 0; i < n; i++) {
+    L[i] = &batch[i]->lts;
+    p[i] = batch[i]->p;
+    q[i] = batch[i]->q;
+  }
+  for (uint32_t i = 0; i <= n; i++) start_off[i] = i;
+  std::vector<uint8_t> trivial, over;
+  std::unique_ptr<Session> ss(new Session());
+  geq_status st = build_and_upload(e, device, n, L.data(), start_off.data(), p.data(), q.data(), max_positions, ss->dg,
+                                   nullptr, &trivial, &over);
+  if (!st && ss->dg) st = e.solve_begin(*ss->dg);
+  if (st) {
+    if (n > 1) {
+      for (Request *r : batch) {
+        std::vector<Request *> one{r};
+        start_compares(e, device, max_positions, one, r->footprint, out, done);
+      }
+      return;
+    }
+    return fail_req(batch[0], st, geq_last_error(), done);
+  }
+  for (uint32_t i = 0; i < n; i++) {
+    Request *r = batch[i];
+    if (trivial[i]) {
+      std::unique_ptr<geq_solution> sol(new geq_solution());
+      sol->energy_size = 1;
+      sol->n_vertices.assign(1, 1);
+      sol->offsets_base.assign(1, 0);
+      sol->data_base.assign(1, 0);
+      sol->offsets = {0, 0};  // bisimilar: no game, no energies
+      r->sol = std::move(sol);
+      done.push_back(r);
+    } else {
+      // its game is in the upload (cut at the bound when over[i]): game k
+      if (over[i]) fail_req(r, GEQ_ERR_OUT_OF_MEMORY, "game exceeds " + std::to_string(max_positions) + " positions",
+                            done);
+      ss->req.push_back(over[i] ? nullptr : r);
+    }
+  }
+  if (!ss->dg) return;
+  ss->retired.assign(ss->req.size(), 0);
+  ss->live = (uint32_t)ss->req.size();
+  ss->first_only = true;
+  ss->footprint = footprint;
+  out.push_back(std::move(ss));
+}
+
+// One step of a session, then the games that reached their fixpoint retire.
+// false: the session is finished (or failed) and can be dropped.
+bool step_session(Engine &e, Session &ss, std::vector<Request *> &done) {
+  bool fin = false;
+  geq_status st = e.solve_step(*ss.dg, fin);
+  std::vector<uint32_t> ret;
+  if (!st) {
+    std::vector<uint8_t> active;
+    if (!fin) st = e.active_games(*ss.dg, active);
+    if (!st)
+      for (uint32_t g = 0; g < ss.retired.size(); g++)
+        if (!ss.retired[g] && (fin || !active[g])) ret.push_back(g);
+  }
+  if (st) {
+    const std::string msg = geq_last_error();
+    for (uint32_t g = 0; g < ss.retired.size(); g++)
+      if (!ss.retired[g]) {
+        ss.retired[g] = 1;
+        if (ss.req[g]) fail_req(ss.req[g], st, msg, done);
+      }
+    ss.live = 0;
+    return false;
+  }
+  if (!ret.empty()) retire(e, ss, ret, done);
+  return ss.live > 0;
 }
 
 void pipeline(geq_server *s, Engine *e) {
   cudaSetDevice(s->device);
+  std::vector<std::unique_ptr<Session>> active;
+  uint64_t used = 0;  // footprint of the resident sessions
   for (;;) {
     std::vector<Request *> batch;
+    uint64_t fp = BATCH_BASE_BYTES;
     {
       std::unique_lock<std::mutex> lk(s->mu);
-      s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
-      if (s->stop) break;
-      // batching window: a few hundred microseconds for more requests
-      if (s->queue.size() < s->cfg.max_batch_games)
-        s->cv_work.wait_for(lk, std::chrono::microseconds(s->cfg.max_wait_us),
-                            [&] { return s->stop || s->queue.size() >= s->cfg.max_batch_games; });
-      if (s->stop) break;
-      uint64_t fp = BATCH_BASE_BYTES;
-      while (!s->queue.empty() && batch.size() < s->cfg.max_batch_games) {
+      if (active.empty()) {
+        s->cv_work.wait(lk, [&] { return s->stop || !s->queue.empty(); });
+        if (s->stop) break;
+        // batching window: a few hundred microseconds for more requests
+        if (s->queue.size() < s->cfg.max_batch_games)
+          s->cv_work.wait_for(lk, std::chrono::microseconds(s->cfg.max_wait_us),
+                              [&] { return s->stop || s->queue.size() >= s->cfg.max_batch_games; });
+        if (s->stop) break;
+      }
+      // admit what has arrived, while it fits beside the resident sessions
+      // (a pipeline without sessions always takes the first request)
+      while (!s->queue.empty() && batch.size() < s->cfg.max_batch_games && active.size() < MAX_SESSIONS) {
         Request *r = s->queue.front();
-        if (!batch.empty() && fp + r->footprint > s->budget) break;
+        if ((!batch.empty() || !active.empty()) && used + fp + r->footprint > s->budget) break;
         fp += r->footprint;
         s->queue.pop_front();
         r->state = 1;
         batch.push_back(r);
       }
-      if (batch.empty()) continue;
-      s->stats.batches++;
-      s->stats.games_in_batches += batch.size();
-      s->stats.running += batch.size();
-      s->stats.queued = s->queue.size();
-      if (fp > s->stats.max_batch_footprint) s->stats.max_batch_footprint = fp;
-    }
-    {
-      std::vector<Request *> games, compares;
-      for (Request *r : batch) (r->kind ? compares : games).push_back(r);
-      if (!games.empty()) run_batch(*e, games);
-      if (!compares.empty()) run_compares(*e, s->device, compares);
-    }
-    {
-      std::lock_guard<std::mutex> lk(s->mu);
-      for (Request *r : batch) {
-        r->state = 2;
-        if (r->st) s->stats.failed++;
-        else s->stats.completed++;
+      if (!batch.empty()) {
+        s->stats.batches++;
+        s->stats.games_in_batches += batch.size();
+        s->stats.running += batch.size();
+        s->stats.queued = s->queue.size();
+        if (used + fp > s->stats.max_batch_footprint) s->stats.max_batch_footprint = used + fp;
       }
-      s->stats.running -= batch.size();
     }
-    s->cv_done.notify_all();
+    std::vector<Request *> done;
+    if (!batch.empty()) {
+      std::vector<Request *> games, compares, wide;
+      uint64_t fg = 0, fc = 0;
+      for (Request *r : batch) {
+        if (r->kind) {
+          compares.push_back(r);
+          fc += r->footprint;
+        } else if (Conf(r->conf).supported()) {
+          games.push_back(r);
+          fg += r->footprint;
+        } else {
+          wide.push_back(r);
+        }
+      }
+      const size_t before = active.size();
+      if (!games.empty()) start_games(*e, games, fg, active, done);
+      if (!compares.empty()) start_compares(*e, s->device, s->cfg.max_game_positions, compares, fc, active, done);
+      for (size_t k = before; k < active.size(); k++) used += active[k]->footprint;
+      if (!wide.empty()) {
+        run_wide(*e, s->device, wide);
+        done.insert(done.end(), wide.begin(), wide.end());
+      }
+    }
+    // one step of every resident session
+    for (size_t k = 0; k < active.size();) {
+      if (step_session(*e, *active[k], done)) {
+        k++;
+      } else {
+        used -= std::min(used, active[k]->footprint);
+        active.erase(active.begin() + k);
+      }
+    }
+    finish(s, done);
+  }
+  // stopped: the sessions in flight finish
+  for (auto &ss : active) {
+    std::vector<Request *> done;
+    while (step_session(*e, *ss, done)) {
+    }
+    finish(s, done);
   }
 }
 
@@ -288,16 +441,17 @@ geq_status geq_server_submit(geq_server *s, const geq_game_graph *graph, uint64_
   if (!s || !graph || !ticket) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
   geq_status st = validate_graph(*graph);
   if (st) return st;
-  if (!Conf(graph->conf).supported())
-    return fail(GEQ_ERR_UNSUPPORTED, "EnergyConf {%u, %u} is outside the device codecs", graph->conf.elements,
-                graph->conf.max);
+  std::string why;
+  if (!Conf(graph->conf).supported() && !wide_supported(Conf(graph->conf), &why))
+    return fail(GEQ_ERR_UNSUPPORTED, "%s", why.c_str());
   const uint64_t n = graph->n_vertices, m = graph->row_offsets[n];
+  const uint64_t us = Conf(graph->conf).update_size();
   std::unique_ptr<Request> r(new Request());
   r->conf = graph->conf;
   r->n = graph->n_vertices;
   r->row.assign(graph->row_offsets, graph->row_offsets + n + 1);
   r->col.assign(graph->column_indices, graph->column_indices + m);
-  r->wt.assign(graph->weights, graph->weights + m);
+  r->wt.assign(graph->weights, graph->weights + m * us);
   r->att.assign(graph->attacker_pos, graph->attacker_pos + n);
   for (auto &a : r->att) a = a ? 1 : 0;
   r->reach = standard_reach_of(*graph);

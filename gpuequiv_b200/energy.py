@@ -47,7 +47,14 @@ class EnergyConf:
         return lib.geq_conf_update_mask(self._c())
 
     def supported(self) -> bool:
+        """A thermometer codec exists for this conf (the batched round
+        kernels, device-resident games, the allocation-free entry point)."""
         return bool(lib.geq_conf_supported(self._c()))
+
+    def solvable(self) -> bool:
+        """EnergyGame.run, run_batch and the serving loop solve games of this
+        conf (the multi-word solver takes the confs without a codec)."""
+        return bool(lib.geq_conf_solvable(self._c()))
 
     def __eq__(self, o):
         return isinstance(o, EnergyConf) and (self.elements, self.max) == (o.elements, o.max)

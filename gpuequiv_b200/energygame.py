@@ -61,8 +61,14 @@ class Context:
         lib.geq_context_get_tuning(self.h, C.byref(t))
         return {f: getattr(t, f) for f, _ in t._fields_}
 
-    def set_tuning(self, blocks_per_sm=0, rounds_per_graph=0, small_limit=0, flags=0):
-        t = geq_tuning(blocks_per_sm, rounds_per_graph, small_limit, flags)
+    def set_tuning(self, blocks_per_sm=0, rounds_per_graph=0, small_limit=0, flags=0, lane_limits=0):
+        """Zero fields keep their value (flags are always set).  lane_limits:
+        (successors, candidates, list length) of the lane path, or its packed
+        u32 form."""
+        if isinstance(lane_limits, (tuple, list)):
+            d, w, k = lane_limits
+            lane_limits = (d & 0xFF) | ((w & 0xFF) << 8) | ((k & 0xFF) << 16)
+        t = geq_tuning(blocks_per_sm, rounds_per_graph, small_limit, flags, lane_limits)
         check(lib.geq_context_set_tuning(self.h, C.byref(t)))
 
 
@@ -305,8 +311,15 @@ def run_batch_raw(graphs: Sequence[GameGraph], context: Context | None = None, v
         views = (geq_game_graph * n)(*[g.c_view() for g in graphs])
     sol = C.c_void_p()
     check(lib.geq_energy_game_run_batch(ctx.h, n, views, None, None, None, C.byref(sol)))
+    offs, data = _flat_lists(sol, graphs)
+    return offs, data, _stats_of(sol)
+
+
+def _flat_lists(sol, graphs):
+    """Per-game (offsets, data) views of a solution's flat memory; the
+    solution is freed once the last view is gone."""
+    n = len(graphs)
     owner = _SolutionOwner(sol)
-    stats = _stats_of(sol)
     po, pd = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
     no, nw = C.c_uint64(), C.c_uint64()
     check(lib.geq_solution_flat(sol, C.byref(po), C.byref(no), C.byref(pd), C.byref(nw)))
@@ -321,7 +334,19 @@ def run_batch_raw(graphs: Sequence[GameGraph], context: Context | None = None, v
     obl, dbl = ob.tolist(), db.tolist()
     offs = [flat_o[obl[i]:obl[i + 1]] for i in range(n)]
     data = [flat_d[dbl[i]:dbl[i + 1]] for i in range(n)]
-    return offs, data, stats
+    return offs, data
+
+
+def b_min(graph: GameGraph, offsets) -> int:
+    """Schedule-independent byte floor of a solve, from its final lists A*
+    (offsets[n+1], STANDARD: one word per energy): every row pair and edge
+    read once, the attacker flags once, every final list written once and
+    read once per predecessor -- 4(n+1) + 8m + n + sum_v 4|A*_v|(1 + indeg(v))."""
+    n = graph.n_vertices()
+    m = graph.n_edges()
+    indeg = np.bincount(graph.column_indices, minlength=n).astype(np.int64) if m else np.zeros(n, np.int64)
+    cnt = np.diff(np.asarray(offsets, dtype=np.int64))
+    return int(4 * (n + 1) + 8 * m + n + 4 * int(np.dot(cnt, 1 + indeg)))
 
 
 def run_static(graph: GameGraph, context: Context | None = None, to_reach=None, data_cap: int | None = None):
@@ -376,6 +401,13 @@ class DeviceGames:
         check(lib.geq_device_games_solve(self.ctx.h, self.h, C.byref(st)))
         return st.as_dict()
 
+    def download_raw(self):
+        """All games' lists as (offsets, data) per game, views of one flat
+        page-locked block (no per-position objects)."""
+        sol = C.c_void_p()
+        check(lib.geq_device_games_download(self.ctx.h, self.h, C.byref(sol)))
+        return _flat_lists(sol, self.graphs)
+
     def download(self):
         sol = C.c_void_p()
         check(lib.geq_device_games_download(self.ctx.h, self.h, C.byref(sol)))
@@ -397,4 +429,4 @@ class DeviceGames:
 
 
 __all__ = ["Context", "default_context", "GameGraph", "EnergyGame", "run_batch", "run_batch_raw", "c_views",
-           "DeviceGames", "GeqError"]
+           "DeviceGames", "GeqError", "b_min"]

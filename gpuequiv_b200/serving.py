@@ -22,9 +22,12 @@ class Server:
     ``poll(ticket, timeout_ms)``."""
 
     def __init__(self, context: Context | None = None, n_pipelines: int = 0, max_batch_games: int = 0,
-                 max_wait_us: int = 0, hbm_budget_bytes: int = 0, max_queued: int = 0):
+                 max_wait_us: int = 0, hbm_budget_bytes: int = 0, max_queued: int = 0, max_game_positions: int = 0):
+        """max_game_positions: a compare query whose game would have more
+        positions fails alone with OUT_OF_MEMORY (0: no bound)."""
         ctx = context or default_context()
-        cfg = geq_server_config(n_pipelines, max_batch_games, max_wait_us, 0, hbm_budget_bytes, max_queued)
+        cfg = geq_server_config(n_pipelines, max_batch_games, max_wait_us, max_game_positions, hbm_budget_bytes,
+                                max_queued)
         h = C.c_void_p()
         check(lib.geq_server_create(ctx.h, C.byref(cfg), C.byref(h)))
         self.h = h

@@ -38,7 +38,9 @@ extern "C" {
 #pragma GCC visibility push(default)
 #endif
 
-#define GEQ_ABI_VERSION 1
+/* 2: geq_tuning.lane_limits, geq_server_config.max_game_positions,
+ *    geq_conf_solvable, GEQ_TUNE_FORCE_WIDE */
+#define GEQ_ABI_VERSION 2
 
 /* Error codes.  Replaces gpuequiv::Error (src/error.rs:3-40) and the
  * TryFrom<SerdeGameGraph> checks (src/energygame.rs:65-83). */
@@ -73,9 +75,18 @@ uint32_t geq_conf_energy_mask(geq_energy_conf c);  /* energy.rs:61-63 */
 uint32_t geq_conf_update_bits(geq_energy_conf c);  /* energy.rs:70-73 */
 uint32_t geq_conf_update_size(geq_energy_conf c);  /* energy.rs:65-68 */
 uint32_t geq_conf_update_mask(geq_energy_conf c);  /* energy.rs:75-77 */
-/* 1 if the solver kernels accept this conf (energy and update fit one word
- * and elements*max <= 32), else 0. */
+/* 1 if the conf has a thermometer codec (energy and update fit one word and
+ * elements*max <= 32): the batched round kernels, device-resident games and
+ * geq_energy_game_run_static take it.  Else 0. */
 int geq_conf_supported(geq_energy_conf c);
+/* 1 if geq_energy_game_run / _batch and the serving loop solve games of this
+ * conf: every conf with elements >= 1, an energy of at most 64 words and an
+ * update of at most 128 words (e.g. ONE_DIMENSION {1, u32::MAX}: one 32-bit
+ * field; {30, 3}: 2 energy words, 8 update words); the confs without a
+ * thermometer codec take the multi-word solver.  EnergyConf itself has no
+ * limit (energy.rs:36-78); the reference generates its shaders per conf
+ * (shadergen.rs:159-189). */
+int geq_conf_solvable(geq_energy_conf c);
 
 /* ---- Energy / Update packing ------------------------------------------- */
 /* Energy::new (energy.rs:88-93, pack_energy :143-162).  n_values <= elements;
@@ -187,12 +198,16 @@ geq_status geq_energy_game_run(geq_context *ctx, const geq_game_graph *graph,
  *   lists in the layout of geq_energy_lists; *n_words = result words, set
  *   also when data_cap is too small (then GEQ_ERR_INVALID_INPUT and data is
  *   not written).  After any other error offsets and data are unspecified.
- * Limit: 45 bytes per position + 12 per edge of the scratch hold the game;
- *   the rest (at least 16 KiB) holds the energy lists.  A larger game gives
- *   GEQ_ERR_UNSUPPORTED, lists that outgrow the rest GEQ_ERR_OUT_OF_MEMORY.
- * The scratch address is looked up (cudaGetSymbolAddress) by the first call
- * per device, with the context's device current: make that first call
- * before any stream capture.  All contexts of a device share the scratch:
+ * Limit: the game takes 45 bytes per position + 12 per edge + 4 per
+ *   explicit to_reach entry of the scratch, plus up to 4 KiB of alignment
+ *   (each of its 15 arrays starts on a 256-byte boundary); the rest (at least
+ *   16 KiB) holds the energy lists.  A larger game gives GEQ_ERR_UNSUPPORTED,
+ *   lists that outgrow the rest GEQ_ERR_OUT_OF_MEMORY.
+ * The scratch is reserved on a device when a context is created there
+ * (geq_context_create loads the module that holds it): create the context
+ * before the caller's own allocator reserves the device's memory.  Every call
+ * looks the scratch's device address up (cudaGetSymbolAddress) with the
+ * context's device current.  All contexts of a device share the scratch:
  * calls that overlap in time on one device race on it, so the caller must
  * serialise them.
  * No counterpart in the reference, whose runs create their buffers per run
@@ -233,11 +248,13 @@ void geq_device_games_free(geq_device_games *dg);
  * Requests (one game each, standard initialisation) are queued by
  * geq_server_submit and solved by pipeline threads, each with its own CUDA
  * stream, staging and device memory: a pipeline takes every queued request
- * that fits its batch limits, uploads the batch as one id space, solves it
- * with the batched round loop and splits the lists per request, while the
- * other pipelines upload or solve the batches before and after it (continuous
- * batching over alternating pipelines).  A batch is admitted only while its
- * estimated device footprint stays within hbm_budget_bytes / n_pipelines.
+ * that fits, uploads them as one batch (one id space) and keeps up to four
+ * such batches resident, running one CUDA graph of worklist rounds of each in
+ * turn -- requests that arrive while others are on the device are admitted at
+ * the next step boundary, and each game's lists are returned as soon as its
+ * own part of the frontier is empty (its fixpoint), not when its batch ends
+ * (continuous batching).  The resident batches of a pipeline stay within an
+ * estimated device footprint of hbm_budget_bytes / n_pipelines.
  * Results are identical to geq_energy_game_run of the same game: every game
  * keeps its own positions and frontier inside a batch.  The crate has no
  * server; its callers run EnergyGame::run per request (energygame.rs:379-383),
@@ -248,7 +265,10 @@ typedef struct geq_server_config {
   uint32_t max_batch_games;   /* requests per batch at most (0: 4096) */
   uint32_t max_wait_us;       /* a pipeline waits this long for more requests
                                  once it holds fewer than max_batch_games (0: 200) */
-  uint32_t reserved;
+  uint32_t max_game_positions; /* compare queries: a query whose game would have more
+                                 positions fails alone with GEQ_ERR_OUT_OF_MEMORY
+                                 (0: no bound; the game is exponential in the
+                                 nondeterminism of the LTS) */
   uint64_t hbm_budget_bytes;  /* device footprint of all in-flight batches (0: 150 GB) */
   uint64_t max_queued;        /* queued requests before submit answers BUSY (0: 1,000,000) */
 } geq_server_config;
@@ -289,6 +309,12 @@ typedef struct geq_tuning {
   uint32_t rounds_per_graph;  /* worklist rounds captured per CUDA graph launch */
   uint32_t small_limit;       /* candidates handled in registers per position (1..32) */
   uint32_t flags;             /* GEQ_TUNE_* bits */
+  uint32_t lane_limits;       /* positions the round kernel solves one per lane (the
+                                 others go to one warp each): at most bits 0-7
+                                 successors (1..16), bits 8-15 candidates per step
+                                 (1..64), bits 16-23 energies in the own / first list
+                                 (1..16); 0 keeps the current value, a zero field
+                                 means the largest */
 } geq_tuning;
 #define GEQ_TUNE_FORCE_GENERIC 1u /* generic codec even for STANDARD (cross-check) */
 #define GEQ_TUNE_FORCE_LARGE 2u   /* bypass the register paths (cross-check) */
@@ -297,6 +323,7 @@ typedef struct geq_tuning {
 #define GEQ_TUNE_NO_THREAD_PATH 16u /* no lane-per-position path (cross-check) */
 #define GEQ_TUNE_NO_SPLIT 32u     /* a large batch on one engine, not as two pipelined halves */
 #define GEQ_TUNE_BUILD_WARP_ALL 64u /* device GameBuild: every attack position by the warp path (cross-check) */
+#define GEQ_TUNE_FORCE_WIDE 128u  /* geq_energy_game_run(_batch): the multi-word solver for every conf (cross-check) */
 geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t);
 void geq_context_get_tuning(const geq_context *ctx, geq_tuning *t);
 

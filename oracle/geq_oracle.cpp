@@ -219,7 +219,7 @@ bool earray_eq(const Arith &ar, const EList &self, const EList &other) {
   return true;
 }
 
-// defend_iterative.wgsl:224-281 `minimize`, executed for one workgroup of 64
+// defend_iterative.wgsl:123-180 `minimize`, executed for one workgroup of 64
 // invocations.  All reads of a chunk happen before its writes, as the
 // workgroup/storage barriers in the shader guarantee.
 uint32_t wg_minimize(const Arith &ar, std::vector<uint32_t> &sup, uint32_t sbase,
@@ -254,7 +254,7 @@ uint32_t wg_minimize(const Arith &ar, std::vector<uint32_t> &sup, uint32_t sbase
       }
       flag[l] = is_minimal;
     }
-    // prefix_sum (defend_iterative.wgsl:182-214): exclusive scan + total.
+    // prefix_sum (defend_iterative.wgsl:81-113): exclusive scan + total.
     uint32_t prefix = 0;
     for (uint32_t l = 0; l < 64; l++) {
       if (flag[l]) {
@@ -267,7 +267,7 @@ uint32_t wg_minimize(const Arith &ar, std::vector<uint32_t> &sup, uint32_t sbase
   return n_minimized;
 }
 
-// defend_iterative.wgsl:283-368 `intersection` for one defender node.
+// defend_iterative.wgsl:182-267 `intersection` for one defender node.
 // `en` holds the already inv-updated energies of the successors back to back,
 // `so` the n_succ+1 region offsets (relative to en).  Returns the status.
 int32_t wg_intersection(const Arith &ar, const uint32_t *en, const uint32_t *so,
@@ -360,7 +360,7 @@ void run_game(const Graph &g, std::vector<EList> &E, const std::vector<uint32_t>
     def_list.clear();
 
     // ---- attack: update + minimize (attack_update.wgsl:77-113,
-    //      attack_minimize.wgsl:180-235) ----
+    //      attack_minimize.wgsl:69-122) ----
     std::vector<std::pair<uint32_t, EList>> atk_res;
     for (uint32_t v : atk_nodes) {
       st.atk_visits++;
@@ -750,7 +750,7 @@ void parallel_for(uint32_t n, uint32_t threads, F f) {
 
 // One worklist step of position v against the lists E, as a round of
 // run_game applies it (energygame.rs:774-944, attack_update.wgsl:77-113,
-// attack_minimize.wgsl:180-235, defend_iterative.wgsl:283-368): true when
+// attack_minimize.wgsl:69-122, defend_iterative.wgsl:182-267): true when
 // the reference would change v's list.  Defenders whose suprema outgrow the
 // preallocated memory are retried with more, as run_game does in a later
 // round.
@@ -1115,7 +1115,18 @@ void ora_run_games_parallel(uint32_t n_games, uint32_t elements, uint32_t max, c
                             const uint32_t *const *row_offsets, const uint32_t *const *col,
                             const uint32_t *const *weights, const uint8_t *const *attacker,
                             uint32_t n_threads, uint64_t *out_total) {
-  parallel_for(n_games, n_threads, [&](uint32_t i) {
+  ora_solve_games(n_games, elements, max, n_pos, row_offsets, col, weights, attacker, n_threads, nullptr,
+                  out_total, nullptr);
+}
+
+void ora_solve_games(uint32_t n_games, uint32_t elements, uint32_t max, const uint32_t *n_pos,
+                     const uint32_t *const *row_offsets, const uint32_t *const *col,
+                     const uint32_t *const *weights, const uint8_t *const *attacker, uint32_t n_threads,
+                     const uint32_t *order, uint64_t *out_total, OraSolution **out_sol) {
+  // one shared work counter over the whole set: a thread takes the next game
+  // (in `order` when given) as soon as it is free
+  parallel_for(n_games, n_threads, [&](uint32_t k) {
+    const uint32_t i = order ? order[k] : k;
     Graph g;
     g.conf = Conf{elements, max};
     g.n = n_pos[i];
@@ -1132,8 +1143,24 @@ void ora_run_games_parallel(uint32_t n_games, uint32_t elements, uint32_t max, c
     run_game(g, E, reach, st);
     uint64_t t = 0;
     for (auto &e : E) t += e.size() / g.conf.energy_size();
-    out_total[i] = t;
+    if (out_total) out_total[i] = t;
+    if (out_sol) {
+      auto *s = new OraSolution;
+      s->esize = g.conf.energy_size();
+      s->E = std::move(E);
+      s->st = st;
+      out_sol[i] = s;
+    }
   });
+}
+
+uint64_t ora_b_min(uint32_t n, const uint32_t *row_offsets, const uint32_t *col, const uint64_t *offsets) {
+  const uint64_t m = row_offsets[n];
+  std::vector<uint64_t> indeg(n, 0);
+  for (uint64_t k = 0; k < m; k++) indeg[col[k]]++;
+  uint64_t b = 4ull * (n + 1) + 8ull * m + n;
+  for (uint32_t v = 0; v < n; v++) b += 4ull * (offsets[v + 1] - offsets[v]) * (1ull + indeg[v]);
+  return b;
 }
 
 }  // extern "C"

@@ -69,7 +69,7 @@ void ora_solution_free(OraSolution *s);
 uint32_t ora_standard_reach(uint32_t n, const uint32_t *row_offsets,
                             const uint8_t *attacker, uint32_t *out);
 
-/* One workgroup of defend_iterative.wgsl:283-368 on already-updated
+/* One workgroup of defend_iterative.wgsl:182-267 on already-updated
  * energies.  succ_offsets has n_succ+1 entries (relative to energies).
  * Returns the shader's status (>=0: size of the result written to sup_out,
  * <0: -required memory).  sup_out needs room for `mem` energies. */
@@ -132,6 +132,18 @@ void ora_run_games_parallel(uint32_t n_games, uint32_t elements, uint32_t max,
                             const uint32_t *const *weights,
                             const uint8_t *const *attacker, uint32_t n_threads,
                             uint64_t *out_total);
+/* The same with the lists kept: games are taken from one shared counter in
+ * `order` (NULL: index order) by n_threads threads; out_total and out_sol
+ * (one OraSolution per game, freed by ora_solution_free) may each be NULL. */
+void ora_solve_games(uint32_t n_games, uint32_t elements, uint32_t max, const uint32_t *n_pos,
+                     const uint32_t *const *row_offsets, const uint32_t *const *col,
+                     const uint32_t *const *weights, const uint8_t *const *attacker, uint32_t n_threads,
+                     const uint32_t *order, uint64_t *out_total, OraSolution **out_sol);
+/* Schedule-independent byte floor of a solve from its final lists A*:
+ * 4(n+1) + 8m + n + sum_v 4|A*_v|(1 + indeg(v)) -- every row pair and edge
+ * read once, the attacker flags once, every final list written once and read
+ * once per predecessor (STANDARD: one word per energy). */
+uint64_t ora_b_min(uint32_t n, const uint32_t *row_offsets, const uint32_t *col, const uint64_t *offsets);
 
 #ifdef __cplusplus
 }

@@ -95,6 +95,11 @@ def lib():
         L.ora_run_games_parallel.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u32p,
                                              C.POINTER(u32p), C.POINTER(u32p), C.POINTER(u32p),
                                              C.POINTER(u8p), C.c_uint32, u64p]
+        L.ora_solve_games.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u32p,
+                                      C.POINTER(u32p), C.POINTER(u32p), C.POINTER(u32p),
+                                      C.POINTER(u8p), C.c_uint32, u32p, u64p, C.POINTER(C.c_void_p)]
+        L.ora_b_min.argtypes = [C.c_uint32, u32p, u32p, u64p]
+        L.ora_b_min.restype = C.c_uint64
         L.ora_check_fixpoint.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p, u32p, u8p, u64p, u32p,
                                          C.c_uint32, u32p]
         L.ora_check_fixpoint.restype = C.c_uint64
@@ -296,7 +301,7 @@ class Lts:
 class Build:
     """GameBuild of the oracle: positions and the CSR game graph."""
 
-    def __init__(self, handle):
+    def __init__(self, handle, positions=True):
         L = lib()
         self.n = L.ora_build_n_nodes(handle)
         m = L.ora_build_n_edges(handle)
@@ -310,7 +315,7 @@ class Build:
         self.col, self.wt, self.attacker = self.col[:m], self.wt[:m], self.attacker[:self.n]
         self.positions = []
         k, p, nq, nqx = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
-        for i in range(self.n):
+        for i in range(self.n if positions else 0):
             L.ora_build_position(handle, i, C.byref(k), C.byref(p), C.byref(nq), C.byref(nqx))
             q = np.zeros(max(nq.value, 1), dtype=np.uint32)
             qx = np.zeros(max(nqx.value, 1), dtype=np.uint32)
@@ -320,8 +325,10 @@ class Build:
         L.ora_build_free(handle)
 
     @classmethod
-    def compare(cls, lts: Lts, p: int, q: int):
-        return cls(lib().ora_build_compare(lts.h, p, q))
+    def compare(cls, lts: Lts, p: int, q: int, positions=True):
+        """GameBuild::compare; positions=False skips reading the positions
+        back (only the graph)."""
+        return cls(lib().ora_build_compare(lts.h, p, q), positions)
 
     @classmethod
     def compare_all(cls, lts: Lts):
@@ -341,6 +348,52 @@ def compare_batch(lts_list, ps, qs, threads=1):
     lib().ora_compare_batch(n, hs, _p(p, C.c_uint32), _p(q, C.c_uint32), threads,
                             _p(cnt, C.c_uint64), _p(nodes, C.c_uint64))
     return cnt, nodes
+
+
+def _game_arrays(games):
+    n = len(games)
+    keep = []
+    npos = np.array([len(g[0]) - 1 for g in games], dtype=np.uint32)
+    rows = (u32p * n)()
+    cols = (u32p * n)()
+    wts = (u32p * n)()
+    atts = (u8p * n)()
+    for i, (r, c, w, a) in enumerate(games):
+        r = np.ascontiguousarray(r, dtype=np.uint32)
+        c = np.ascontiguousarray(c if len(c) else np.zeros(1), dtype=np.uint32)
+        w = np.ascontiguousarray(w if len(w) else np.zeros(1), dtype=np.uint32)
+        a = np.ascontiguousarray(a if len(a) else np.zeros(1), dtype=np.uint8)
+        keep += [r, c, w, a]
+        rows[i], cols[i], wts[i], atts[i] = _p(r, C.c_uint32), _p(c, C.c_uint32), _p(w, C.c_uint32), _p(a, C.c_uint8)
+    return npos, rows, cols, wts, atts, keep
+
+
+def solve_games(games, threads=1, largest_first=False, elements=6, max_=3):
+    """Oracle solve of many games (standard reach) on `threads` threads that
+    share one work counter (largest games first when asked, so that one big
+    game does not end up last).  Returns one Solution per game."""
+    n = len(games)
+    if n == 0:
+        return []
+    npos, rows, cols, wts, atts, keep = _game_arrays(games)
+    order = None
+    if largest_first:
+        size = np.array([len(g[1]) + len(g[0]) for g in games], dtype=np.int64)
+        order = np.ascontiguousarray(np.argsort(-size, kind="stable"), dtype=np.uint32)
+    handles = (C.c_void_p * n)()
+    lib().ora_solve_games(n, elements, max_, _p(npos, C.c_uint32), rows, cols, wts, atts, threads,
+                          None if order is None else _p(order, C.c_uint32), None, handles)
+    es = lib().ora_energy_size(elements, max_)
+    return [Solution(handles[i], int(npos[i]), es) for i in range(n)]
+
+
+def b_min(row_offsets, col, offsets):
+    """The schedule-independent byte floor 4(n+1) + 8m + n + sum_v 4|A*_v|(1 +
+    indeg(v)) of a game from its final list offsets (STANDARD conf)."""
+    r = np.ascontiguousarray(row_offsets, dtype=np.uint32)
+    c = np.ascontiguousarray(col if len(col) else np.zeros(1), dtype=np.uint32)
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    return int(lib().ora_b_min(len(r) - 1, _p(r, C.c_uint32), _p(c, C.c_uint32), _p(o, C.c_uint64)))
 
 
 def run_games_parallel(games, threads=1, elements=6, max_=3):

@@ -70,6 +70,14 @@ struct HostBackend {
               const unsigned long long *go) {
     if (*go) scan(in, out, (uint32_t)*np, tot);
   }
+  void scan2_d(const uint32_t *a, uint32_t *x, const unsigned long long *na, unsigned long long *ta,
+               const uint32_t *b, uint32_t *y, const unsigned long long *nb, unsigned long long *tb,
+               const unsigned long long *go) {
+    if (!*go) return;
+    scan(a, x, (uint32_t)*na, ta);
+    scan(b, y, (uint32_t)*nb, tb);
+  }
+  void scan_capacity(uint64_t) {}
   void scan3_d(const uint32_t *a, const uint32_t *b, const uint32_t *c, uint32_t *x, uint32_t *y, uint32_t *z,
                const unsigned long long *np, unsigned long long *t, const unsigned long long *go) {
     if (!*go) return;

@@ -3,9 +3,7 @@
 Every constant cites the file:line of Gobbel2000/gpuequiv (v1.0.0) it was
 copied from.  The reference is Rust + WGSL and cannot run in this image (no
 Rust toolchain, no graphics stack), so these known answers are the pin for the
-CPU oracle and, through it, for the CUDA path.  ``check_transcription.py`` in
-this folder re-reads the reference's test sources (when they are present) and
-confirms the numbers below match them.
+CPU oracle and, through it, for the CUDA path.
 
 Energies are given as value lists (shorter lists are zero-padded, as
 ``Energy::new`` does); updates in the crate's i32 form (0 Zero, -1 Decrement,

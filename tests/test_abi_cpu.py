@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol(geq):
     assert set(declared) <= exported, set(declared) - exported
     assert set(declared) <= set(_lib.EXPORTED), set(declared) - set(_lib.EXPORTED)
     assert exported <= set(declared), exported - set(declared)
-    assert _lib.lib.geq_abi_version() == 1
+    assert _lib.lib.geq_abi_version() == 2
 
 
 def test_conf_sizes(geq):
@@ -44,6 +44,13 @@ def test_conf_sizes(geq):
                 c.update_mask()) == expect
     assert geq.EnergyConf.STANDARD.supported()
     assert not geq.EnergyConf.ONE_DIMENSION.supported()
+    # every conf of the crate's own tests is solvable; those without a
+    # thermometer codec by the multi-word solver
+    for conf, _ in G.CONF_SIZES:
+        assert geq.EnergyConf(*conf).solvable(), conf
+    assert geq.EnergyConf.ONE_DIMENSION.solvable() and geq.EnergyConf(30, 3).solvable()
+    assert not geq.EnergyConf(300, 0xFFFFFFFF).solvable()  # 300 energy words
+    assert not geq.EnergyConf(0, 3).solvable()
 
 
 def test_packing_golden(geq):

@@ -26,6 +26,8 @@ MODES = {
     # every register budget of the round kernel
     "bps2": dict(blocks_per_sm=2, rounds_per_graph=3),
     "bps5": dict(blocks_per_sm=5, rounds_per_graph=16),
+    # tighter lane-path limits: more positions take the warp routines
+    "lanes_small": dict(lane_limits=(4, 8, 4)),
 }
 
 
@@ -296,8 +298,10 @@ def test_invalid_inputs(geq, ctx):
                                np.array([0xF], np.uint32), np.array([1], np.uint8), C)
     with pytest.raises(geq.GeqError):
         geq.EnergyGame.standard_reach(g).run(ctx)
-    g1 = geq.GameGraph.from_csr(np.array([0, 0], np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.uint32),
-                                np.array([1], np.uint8), geq.EnergyConf.ONE_DIMENSION)
+    # a conf beyond the multi-word solver (300 words per energy)
+    big = geq.EnergyConf(300, 0xFFFFFFFF)
+    g1 = geq.GameGraph.from_csr(np.array([0, 0], np.uint32), np.zeros(0, np.uint32),
+                                np.zeros((0, big.update_size()), np.uint32), np.array([1], np.uint8), big)
     with pytest.raises(geq.GeqError) as e:
         geq.EnergyGame.standard_reach(g1).run(ctx)
     assert e.value.name == "UNSUPPORTED"

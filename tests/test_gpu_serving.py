@@ -158,3 +158,91 @@ def test_compare_queries_alone_equal_in_the_mix(geq, ctx):
     for i, ref in oracle_of.items():
         assert got[i] == sorted(int(x) for x in np.asarray(ref).reshape(-1)), i
     assert st["failed"] == 0
+
+
+def test_compare_query_position_bound(geq, ctx):
+    """With max_game_positions, a query whose game would be larger fails alone
+    (OUT_OF_MEMORY) while the queries of its batch that fit are answered as
+    compare() alone answers them."""
+    from gpuequiv_b200 import GeqError, synth
+    from gpuequiv_b200.serving import Server
+    rows = synth.batched_manifest()["jobs"]
+    big = [r for r in rows if r[1] > 50_000][:2]
+    small = [r for r in rows if r[1] <= 5_000][:12]
+    bound = 20_000
+    jobs = []
+    for seed, npos, _ in small[:6] + big[:1] + small[6:] + big[1:]:
+        src, dst, lab, p, q = synth.batched_lts(seed)
+        jobs.append((geq.TransitionSystem.from_arrays(src, dst, lab), int(p), int(q), npos > bound))
+    alone = {i: sorted(int(x) for x in np.asarray(geq.compare_batch([j[:3]], context=ctx)[0].array).reshape(-1))
+             for i, j in enumerate(jobs) if not j[3]}
+    with Server(ctx, n_pipelines=1, max_wait_us=20_000, max_game_positions=bound) as srv:
+        tickets = [srv.submit_compare(*j[:3]) for j in jobs]
+        for i, (t, j) in enumerate(zip(tickets, jobs)):
+            if j[3]:
+                with pytest.raises(GeqError) as e:
+                    srv.poll(t, timeout_ms=120_000)
+                assert e.value.name == "OUT_OF_MEMORY"
+            else:
+                offs, data, _ = srv.poll(t, timeout_ms=120_000)
+                assert sorted(int(x) for x in data[int(offs[0]):int(offs[1])]) == alone[i], i
+        st = srv.stats()
+    assert st["failed"] == 2 and st["completed"] == len(jobs) - 2
+
+
+def test_games_retire_at_their_own_fixpoint(geq, ctx):
+    """Games of one resident batch are answered when their own part of the
+    frontier empties: a small game solved beside a deep one comes back after
+    fewer rounds than the deep one (the rounds its batch had run when it was
+    read back), and every list equals the game solved alone and the oracle."""
+    from gpuequiv_b200 import synth
+    from gpuequiv_b200.serving import Server
+    from oracle import ora
+    rows = synth.batched_manifest()["jobs"]
+
+    def game(seed):
+        src, dst, lab, p, q = synth.batched_lts(seed)
+        red, mp = geq.TransitionSystem.from_arrays(src, dst, lab).bisimilar_minimize()
+        return geq.GameBuild.compare(red, int(mp[p]), int(mp[q])).game
+
+    def alone_rounds(g):
+        return geq.run_batch_raw([g], ctx)[2]["rounds"]
+
+    R = ctx.tuning()["rounds_per_graph"]
+    deep = next(g for g in (game(r[0]) for r in sorted(rows[:800], key=lambda r: -r[1])[:40])
+                if alone_rounds(g) >= 3 * R)
+    small = [g for g in (game(r[0]) for r in rows[:400] if 30 <= r[1] <= 400) if alone_rounds(g) < R][:24]
+    assert len(small) >= 8
+    games = [deep] + small
+    expect = [_alone(geq, ctx, g) for g in games]
+    with Server(ctx, n_pipelines=1, max_wait_us=50_000) as srv:
+        tickets = [srv.submit(g) for g in games]
+        res = [srv.poll(t, timeout_ms=120_000) for t in tickets]
+        st = srv.stats()
+    assert st["batches"] == 1 and st["failed"] == 0
+    rounds = [r[2]["rounds"] for r in res]
+    assert max(rounds[1:]) < rounds[0], rounds
+    for i, (g, (offs, data, _)) in enumerate(zip(games, res)):
+        assert _canon(offs, data) == expect[i], i
+    for i in (1, 2, 3):
+        g = games[i]
+        sol = ora.run_game(6, 3, g.row_offsets, g.column_indices, g.weights.array.reshape(-1), g.attacker_pos,
+                           ora.standard_reach(g.row_offsets, g.attacker_pos))
+        assert _canon(sol.offsets, sol.data) == expect[i], i
+
+
+def test_requests_admitted_while_batches_run(geq, ctx):
+    """Requests submitted while earlier batches are resident join as new
+    batches between steps; all results equal the games solved alone."""
+    from gpuequiv_b200.serving import Server
+    games = _games(geq, 200)
+    expect = [_alone(geq, ctx, g) for g in games]
+    with Server(ctx, n_pipelines=1, max_wait_us=100) as srv:
+        tickets = []
+        for k in range(0, len(games), 25):
+            tickets += [srv.submit(g) for g in games[k:k + 25]]
+        got = [srv.poll(t, timeout_ms=120_000) for t in tickets]
+        st = srv.stats()
+    assert st["failed"] == 0 and st["completed"] == len(games)
+    for i, (offs, data, _) in enumerate(got):
+        assert _canon(offs, data) == expect[i], i
