@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--query-bound", type=int, default=200_000,
                     help="position bound of a served query's game (larger games are refused)")
     ap.add_argument("--query-pool", type=int, default=2048, help="distinct queries the arrivals draw from")
+    ap.add_argument("--large-states", type=int, default=0,
+                    help="states of the single-LTS equivalences() leg (the large generator; 0: none)")
     ap.add_argument("--no-stress", dest="stress", action="store_false", help="skip the stress-game leg")
     ap.add_argument("--solve-only", action="store_true",
                     help="build, upload and solve only (the command profiled with ncu)")
@@ -517,6 +519,48 @@ def run_small(ctx, seeds, check: bool) -> dict:
     return out
 
 
+def run_large(ctx, n_states: int, check: bool, pairs: int = 48) -> dict:
+    """The large configuration's generator (power-law out-degree, 12 labels,
+    tau p 0.15, a strongly connected core of 10 %, 4 transitions per state)
+    at n_states states: TransitionSystem::equivalences() of the whole system
+    (minimisation, the compare_all game built and solved on the device).  With
+    `check` the energies of a sample of start pairs are compared with the
+    oracle's TransitionSystem::compare of the same pairs (the energies of a
+    position depend only on the part of the game it reaches)."""
+    import gpuequiv_b200 as geq
+    synth = synth_mod()
+    src, dst, lab = synth.large_lts(1, n=n_states, m=4 * n_states)
+    lts = geq.TransitionSystem.from_arrays(src, dst, lab)
+    times = []
+    for _ in range(2):
+        t = time.perf_counter()
+        eq = lts.equivalences(ctx)
+        times.append(time.perf_counter() - t)
+    out = {"workload": f"large generator at {n_states} states, {4 * n_states} transitions, 12 labels, tau p 0.15, "
+                       f"10 % strongly connected core: equivalences() of the whole system",
+           "seconds": min(times), "start_positions": eq.n_starting_points()}
+    if not check:
+        return out
+    from oracle import ora
+    rng = np.random.default_rng(5)
+    olts = ora.Lts.from_arrays(src, dst, lab)
+    checked = bad = 0
+    for _ in range(pairs * 50):
+        if checked >= pairs:
+            break
+        p, q = (int(x) for x in rng.integers(0, n_states, 2))
+        mine = eq.energies(p, q)
+        if p == q or mine is None:
+            continue
+        ref = ora.compare(olts, p, q)
+        checked += 1
+        if sorted(int(x) for x in mine.array.reshape(-1)) != sorted(int(x) for x in np.asarray(ref).reshape(-1)):
+            bad += 1
+    out.update({"parity_checked": checked, "parity_mismatches": bad,
+                "what": "start-pair energies against the oracle's compare(p, q)"})
+    return out
+
+
 # ---- arms -----------------------------------------------------------------------
 def run_lts_pipeline(ctx, seeds, graphs, args, d: Dist) -> dict:
     """compare_batch over the batch's LTSs: the whole LTS -> energies path
@@ -778,6 +822,7 @@ def run_ours(args, d: Dist):
 
     # ---- small configuration: equivalences() of 100 seeded 40-state LTSs ----
     small = run_small(ctx, list(range(100)), check=d.rank == 0)
+    large = run_large(ctx, args.large_states, check=d.rank == 0) if args.large_states else None
 
     # ---- stress configuration: one 2M-position / 10M-edge game, resident ----
     stress = None
@@ -862,6 +907,7 @@ def run_ours(args, d: Dist):
             "batched_vs_plain": value / plain_rate if plain_rate else None,
             "lts_pipeline": lts_pipe,
             "small": small,
+            "large_single": large,
             "stress": stress,
             "serving": {"workload": "game requests (geq_server_submit) drawn from this batch's games: Poisson "
                                     "arrivals, then a closed loop of 8192 requests in flight (saturation); "
@@ -887,6 +933,8 @@ def run_ours(args, d: Dist):
     if parity and parity["parity_mismatches"]:
         raise SystemExit(f"parity: {parity['parity_mismatches']} of {parity['parity_checked']} checked jobs differ "
                          f"from the oracle: {parity['mismatched_jobs']}")
+    if large and large.get("parity_mismatches"):
+        raise SystemExit(f"parity: large single LTS, {large['parity_mismatches']} start pairs differ from the oracle")
     if small and small.get("parity_mismatches"):
         raise SystemExit(f"parity: small configuration, seeds {small['mismatched_seeds']} differ from the oracle")
 

@@ -80,6 +80,7 @@ TUNE_NO_THREAD_PATH = 16
 TUNE_NO_SPLIT = 32
 TUNE_BUILD_WARP_ALL = 64
 TUNE_FORCE_WIDE = 128
+TUNE_NO_READY = 256
 
 STATUS = {0: "OK", 1: "NO_DEVICE", 2: "OUT_OF_MEMORY", 3: "INVALID_INPUT", 4: "TIMEOUT",
           5: "UNSUPPORTED", 6: "CUDA", 7: "IO", 8: "PARSE", 9: "BUSY", 10: "INTERNAL"}

@@ -155,6 +155,9 @@ struct KParams {
   // the codec's pack_edge form (high word); null: read col / wt
   const unsigned long long *cw;
   uint32_t td, tw, tk;   // lane-path limits: successors, candidates per step, list length
+  // per defender: successors whose list is still empty (null: not counted,
+  // every predecessor of a changed position is pushed)
+  uint32_t *missing;
 };
 
 // Energy-list descriptors (one u64 per position):
@@ -1015,13 +1018,15 @@ __device__ __forceinline__ typename Cd::Upd edge_upd(const KParams &p, const Cd 
 // routines.
 template <class Cd>
 __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32_t *arena, unsigned long long cap,
-                            uint32_t v, uint32_t *scr, uint32_t &out_cnt, uint32_t &edges, uint32_t &bytes) {
+                            uint32_t v, uint32_t *scr, uint32_t &out_cnt, uint32_t &edges, uint32_t &bytes,
+                            uint32_t &old_cnt) {
   const uint32_t e0 = ld(p.row, v, p.n_nodes + 1, c), e1 = ld(p.row, (unsigned long long)v + 1, p.n_nodes + 1, c);
   const uint32_t d = e1 - e0;
   if (d == 0) return T_SKIPPED;
   if (d > p.td) return T_BIG;
   const unsigned long long dv = ld(p.desc, v, p.n_nodes, c);
   const uint32_t cv = dcnt(dv);
+  old_cnt = cv;
   const bool attacker = ld(p.flags, v, p.n_nodes, c) & 1u;
   if (attacker) {
     // attack_update.wgsl + attack_minimize.wgsl: successor candidates, then
@@ -1136,12 +1141,30 @@ __device__ __forceinline__ void mark_push(const KParams &p, uint32_t u, uint32_t
   atomicOr(p.mark + (stamp & 1u) * p.mwords + (u >> 5), 1u << (u & 31u));
 }
 
+// Push predecessor u of a changed position.  A defender is computed only once
+// every successor has energies (energygame.rs:789-792), so with `missing`
+// counted it is pushed only then: the change that fills its last empty
+// successor (`first`: the changed list was empty before) pushes it, and later
+// changes push it as any predecessor.  The reference visits it and skips it
+// meanwhile; the lists are the same.
+__device__ __forceinline__ void push_one(const KParams &p, uint32_t u, uint32_t stamp, uint32_t first) {
+  if (p.missing && !((p.abits[u >> 5] >> (u & 31u)) & 1u)) {
+    if (first) {
+      if (atomicSub(&p.missing[u], 1u) != 1u) return;
+    } else if (*(volatile const uint32_t *)&p.missing[u] != 0u) {
+      return;
+    }
+  }
+  mark_push(p, u, stamp);
+}
+
 // Put the predecessors of the flagged lanes' positions into the next
 // frontier.  The reverse-CSR ranges of all flagged lanes are concatenated and
 // walked 32 entries at a time, so a position with many predecessors is spread
 // over the whole warp.
 __device__ void push_preds_warp(const KParams &p, Ctr *c, uint32_t *sm, uint32_t v, bool flagged, uint32_t stamp,
-                                uint32_t lane) {
+                                uint32_t lane, bool first = false) {
+  const uint32_t firsts = __ballot_sync(FULL, flagged && first);
   uint32_t b = 0, n = 0;
   if (flagged) {
     b = ld(p.rrow, v, p.n_nodes + 1, c);
@@ -1165,7 +1188,7 @@ __device__ void push_preds_warp(const KParams &p, Ctr *c, uint32_t *sm, uint32_t
       const uint32_t start = lo ? sm[SM_PINC + lo - 1] : 0u;
       const unsigned long long k = (unsigned long long)sm[SM_PBEG + lo] + (t - start);
       const uint32_t u = ld(p.rcol, k, p.n_edges, c);
-      if (CHECK_IDX(c, u, p.n_nodes)) mark_push(p, u, stamp);
+      if (CHECK_IDX(c, u, p.n_nodes)) push_one(p, u, stamp, (firsts >> lo) & 1u);
     }
   }
   __syncwarp();
@@ -1208,8 +1231,9 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
     const bool active = slot < fs;
     const uint32_t v = active ? ld(F, slot, p.n_nodes, c) : 0u;
     int ts = T_NONE;
-    uint32_t cnt = 0;
-    if (active) ts = p.thread_path ? thread_solve(p, c, cd, arena, cap, v, scr, cnt, t_edges, t_bytes) : T_BIG;
+    uint32_t cnt = 0, old_cnt = 0;
+    if (active)
+      ts = p.thread_path ? thread_solve(p, c, cd, arena, cap, v, scr, cnt, t_edges, t_bytes, old_cnt) : T_BIG;
     if (ts != T_NONE && ts != T_BIG && ts != T_SKIPPED) t_pos++;
     // inline results need no arena; one reservation for the others
     unsigned long long nd = NONE_DESC;
@@ -1258,7 +1282,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
       }
     }
 #endif
-    push_preds_warp(p, c, sm, v, ts == T_CHANGED, stamp, lane);
+    push_preds_warp(p, c, sm, v, ts == T_CHANGED, stamp, lane, old_cnt == 0u);
     if (ts == T_OVERFLOW) mark_push(p, v, stamp);
 #if GEQ_PATH_PROFILE
     if (lane == 0) PROF_ADD(PF_CYC_PUSH, clock64() - tq1);
@@ -1327,10 +1351,11 @@ __global__ void __launch_bounds__(BLOCK, 3) k_round_big(const KParams p) {
       atomicAdd(&c->prof[PF_B_DEG], (unsigned long long)(p.row[v + 1] - p.row[v]));
     }
 #endif
+    const bool was_empty = dcnt(ld(p.desc, v, p.n_nodes, c)) == 0u;  // committed list, before this round
     const Res r = solve_position(x, cd, v);
     if (r.st != R_SKIPPED) w_pos++;
     if (lane == 0 && CHECK_IDX(c, slot, p.n_nodes)) p.slot_new[slot] = (r.st == R_CHANGED) ? r.d : NONE_DESC;
-    push_preds_warp(p, c, sm, v, lane == 0 && r.st == R_CHANGED, stamp, lane);
+    push_preds_warp(p, c, sm, v, lane == 0 && r.st == R_CHANGED, stamp, lane, was_empty);
     if (r.st == R_OVERFLOW && lane == 0) mark_push(p, v, stamp);  // retried after compaction
   }
 #if GEQ_PATH_PROFILE
@@ -1733,6 +1758,17 @@ __global__ void k_check_weights(const uint32_t *wt, unsigned long long m, uint32
 }
 
 // EnergyGame::with_reach (energygame.rs:355-365): {0} at every target.
+// Successors with an empty initial list, per defender (attackers: 0).
+__global__ void k_missing_init(const KParams p, const unsigned long long *desc0, uint32_t *miss) {
+  for (unsigned long long v = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; v < p.n_nodes;
+       v += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t m = 0;
+    if (!(p.flags[v] & 1u))
+      for (uint32_t k = p.row[v]; k < p.row[v + 1]; k++) m += dcnt(desc0[p.col[k]]) == 0u ? 1u : 0u;
+    miss[v] = m;
+  }
+}
+
 // Edge pairs of the lane path: successor id and the update in the codec's
 // pack_edge form (after k_fix_cols / k_check_weights).
 template <class Cd>
@@ -2043,6 +2079,7 @@ struct DeviceGamesImpl {
   uint8_t *flags = nullptr;
   unsigned long long *desc = nullptr, *desc_init = nullptr, *slot_new = nullptr;
   unsigned long long *cw = nullptr;  // edge pairs (successor, packed update)
+  uint32_t *missing = nullptr, *missing_init = nullptr;  // defenders: successors with no energies yet
   uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr, *fpart = nullptr, *abits = nullptr, *bigq = nullptr;
   uint32_t *init_data = nullptr;
   unsigned long long init_total = 0;
@@ -2512,7 +2549,7 @@ geq_status Engine::alloc_work(DeviceGamesImpl &D, bool any_init) {
       (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, 2 * ((N + 31) / 32)) ||
       !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1) ||
       !D.alloc(D.fpart, 2 * (size_t)std::max(1, n_sms * 2)) || !D.alloc(D.abits, (N + 31) / 32) ||
-      !D.alloc(D.bigq, N) || !D.alloc(D.cw, M))
+      !D.alloc(D.bigq, N) || !D.alloc(D.cw, M) || !D.alloc(D.missing, N) || !D.alloc(D.missing_init, N))
     return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
@@ -2583,6 +2620,8 @@ geq_status Engine::finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out) {
   kp.abits = D.abits;
   kp.bigq = D.bigq;
   kp.cw = D.cw;
+  kp.missing = nullptr;
+  if (N) k_missing_init<<<grid, 256, 0, S>>>(kp, D.desc_init, D.missing_init);
   kp.el = D.conf.elements; kp.mx = D.conf.max; kp.eb = D.conf.energy_bits(); kp.em = D.conf.energy_mask();
   kp.ub = D.conf.update_bits(); kp.um = D.conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
@@ -2720,6 +2759,10 @@ geq_status Engine::solve_begin(DeviceGamesImpl &dg) {
   CU(cudaMemcpyAsync(dg.arena[a0], dg.init_data, dg.init_total * 4, cudaMemcpyDeviceToDevice, S));
   if (dg.next_stamp > 0xF0000000u) dg.next_stamp = 1;
   CU(cudaMemsetAsync(dg.mark, 0, 2ull * dg.kp.mwords * 4, S));
+  // defenders wait for their successors' lists (GEQ_TUNE_NO_READY: push
+  // every predecessor, as the reference's visit lists do)
+  dg.kp.missing = (tuning.flags & GEQ_TUNE_NO_READY) ? nullptr : dg.missing;
+  if (dg.kp.missing && dg.N) CU(cudaMemcpyAsync(dg.missing, dg.missing_init, dg.N * 4, cudaMemcpyDeviceToDevice, S));
   Ctr h{};
   h.arena = dg.arena[a0];
   h.arena_cap = dg.arena_cap[a0];
@@ -3257,8 +3300,9 @@ __global__ void __launch_bounds__(BLOCK, 1) k_solve_static(const KParams p, cons
       const bool active = slot < fs;
       const uint32_t v = active ? ld(F, slot, p.n_nodes, c) : 0u;
       int ts = T_NONE;
-      uint32_t cnt = 0;
-      if (active) ts = p.thread_path ? thread_solve(p, c, cd, arena, cap, v, scr, cnt, t_edges, t_bytes) : T_BIG;
+      uint32_t cnt = 0, old_cnt = 0;
+      if (active)
+        ts = p.thread_path ? thread_solve(p, c, cd, arena, cap, v, scr, cnt, t_edges, t_bytes, old_cnt) : T_BIG;
       if (ts != T_NONE && ts != T_BIG && ts != T_SKIPPED) t_pos++;
       unsigned long long nd = NONE_DESC;
       if (ts == T_CHANGED && cnt <= p.inl) {

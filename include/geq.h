@@ -324,6 +324,8 @@ typedef struct geq_tuning {
 #define GEQ_TUNE_NO_SPLIT 32u     /* a large batch on one engine, not as two pipelined halves */
 #define GEQ_TUNE_BUILD_WARP_ALL 64u /* device GameBuild: every attack position by the warp path (cross-check) */
 #define GEQ_TUNE_FORCE_WIDE 128u  /* geq_energy_game_run(_batch): the multi-word solver for every conf (cross-check) */
+#define GEQ_TUNE_NO_READY 256u    /* push every predecessor of a changed position, also defenders that still
+                                     wait for an empty successor (cross-check) */
 geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t);
 void geq_context_get_tuning(const geq_context *ctx, geq_tuning *t);
 
