@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--plain-sample", type=int, default=256)
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch shape)")
-    ap.add_argument("--serve-rates", default="5000,20000",
+    ap.add_argument("--serve-rates", default="5000,10000",
                     help="Poisson arrival rates (req/s) of the game-request serving leg; empty: none")
     ap.add_argument("--query-rates", default="200,1000,5000",
                     help="Poisson arrival rates (req/s) of the serving configuration (equivalence queries on LTSs "
@@ -227,7 +227,7 @@ def build_games_oracle(seeds):
         src, dst, lab, p, q = synth.batched_lts(seed)
         lts = ora.Lts.from_arrays(src, dst, lab)
         red, mp = lts.bisimilar_minimize()
-        b = ora.Build.compare(red, int(mp[p]), int(mp[q]))
+        b = ora.Build.compare(red, int(mp[p]), int(mp[q]), positions=False)
         games.append((b.row, b.col, b.wt, b.attacker))
     return games
 
@@ -429,7 +429,8 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
             r = _lat_summary((t_done - t_sub) * 1e3, status, t_done.max() - t0)
             batches = st["batches"] - st0["batches"]
             r.update({"lambda_req_s": lam, "batches": int(batches),
-                      "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches)})
+                      "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches),
+                      "pipeline_thread_ms": {k: round(st[k] - st0[k], 1) for k in ("admit_ms", "step_ms", "retire_ms")}})
             out["runs"].append(r)
         if saturation_s > 0:
             pick = np.arange(len(items))
@@ -439,7 +440,8 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
             r = _lat_summary(lat, status, done_at.max() - t0)
             batches = st["batches"] - st0["batches"]
             r.update({"outstanding": outstanding, "batches": int(batches),
-                      "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches)})
+                      "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches),
+                      "pipeline_thread_ms": {k: round(st[k] - st0[k], 1) for k in ("admit_ms", "step_ms", "retire_ms")}})
             out["saturation"] = r
     return out
 

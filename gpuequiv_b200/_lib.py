@@ -52,7 +52,8 @@ class geq_server_config(C.Structure):
 class geq_server_stats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
                 ("batches", C.c_uint64), ("queued", C.c_uint64), ("running", C.c_uint64),
-                ("games_in_batches", C.c_uint64), ("max_batch_footprint", C.c_uint64)]
+                ("games_in_batches", C.c_uint64), ("max_batch_footprint", C.c_uint64), ("admit_ms", C.c_double), ("step_ms", C.c_double),
+                ("retire_ms", C.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -80,7 +81,8 @@ TUNE_NO_THREAD_PATH = 16
 TUNE_NO_SPLIT = 32
 TUNE_BUILD_WARP_ALL = 64
 TUNE_FORCE_WIDE = 128
-TUNE_NO_READY = 256
+TUNE_READY = 256
+TUNE_NO_EDGE_PAIRS = 512
 
 STATUS = {0: "OK", 1: "NO_DEVICE", 2: "OUT_OF_MEMORY", 3: "INVALID_INPUT", 4: "TIMEOUT",
           5: "UNSUPPORTED", 6: "CUDA", 7: "IO", 8: "PARSE", 9: "BUSY", 10: "INTERNAL"}

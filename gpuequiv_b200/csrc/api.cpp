@@ -333,7 +333,7 @@ geq_status geq_solution_flat(const geq_solution *s, const uint64_t **offsets, ui
   *offsets = s->off_ptr();
   *n_offsets = s->offsets_len();
   *data = s->data_ptr();
-  *n_words = s->data_len() / (s->energy_size ? s->energy_size : 1);
+  *n_words = s->data_len();
   return GEQ_OK;
 }
 

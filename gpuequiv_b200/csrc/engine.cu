@@ -1868,6 +1868,33 @@ __global__ void k_rel_offsets(const unsigned long long *goff, unsigned long long
   }
 }
 
+// Selection of whole games: position i of the selection is position
+// i - pre[g] of selected game g (first id base[g]).
+__global__ void k_sel_expand(const unsigned long long *base, const unsigned long long *pre, uint32_t g_count,
+                             unsigned long long k, uint32_t *sel) {
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < k;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t g = game_of(pre, g_count, i);
+    sel[i] = (uint32_t)(base[g] + (i - pre[g]));
+  }
+}
+
+// Clear the frontier-bitmap bits of position ranges [b, e) (games that must
+// not be solved): words at a range's ends are shared with its neighbours.
+__global__ void k_clear_ranges(uint32_t *mh, const unsigned long long *ranges, uint32_t n_ranges) {
+  for (uint32_t r = blockIdx.x; r < n_ranges; r += gridDim.x) {
+    const unsigned long long b = ranges[2 * r], e = ranges[2 * r + 1];
+    if (b >= e) continue;
+    const unsigned long long w0 = b >> 5, w1 = (e - 1) >> 5;
+    for (unsigned long long w = w0 + threadIdx.x; w <= w1; w += blockDim.x) {
+      uint32_t m = ~0u;
+      if (w == w0) m &= ~0u << (uint32_t)(b & 31u);
+      if (w == w1) m &= ~0u >> (31u - (uint32_t)((e - 1) & 31u));
+      atomicAnd(&mh[w], ~m);
+    }
+  }
+}
+
 // Counts of selected positions (sel = global ids).
 __global__ void k_sel_counts(const unsigned long long *desc, const uint32_t *sel, unsigned long long k,
                              uint32_t *cnt) {
@@ -2080,6 +2107,7 @@ struct DeviceGamesImpl {
   unsigned long long *desc = nullptr, *desc_init = nullptr, *slot_new = nullptr;
   unsigned long long *cw = nullptr;  // edge pairs (successor, packed update)
   uint32_t *missing = nullptr, *missing_init = nullptr;  // defenders: successors with no energies yet
+  std::vector<unsigned long long> off_ranges;  // position ranges of games that are not solved (pairs)
   uint32_t *mark = nullptr, *front0 = nullptr, *front1 = nullptr, *fpart = nullptr, *abits = nullptr, *bigq = nullptr;
   uint32_t *init_data = nullptr;
   unsigned long long init_total = 0;
@@ -2549,7 +2577,7 @@ geq_status Engine::alloc_work(DeviceGamesImpl &D, bool any_init) {
       (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, 2 * ((N + 31) / 32)) ||
       !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1) ||
       !D.alloc(D.fpart, 2 * (size_t)std::max(1, n_sms * 2)) || !D.alloc(D.abits, (N + 31) / 32) ||
-      !D.alloc(D.bigq, N) || !D.alloc(D.cw, M) || !D.alloc(D.missing, N) || !D.alloc(D.missing_init, N))
+      !D.alloc(D.bigq, N) || !D.alloc(D.cw, M))
     return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
   if (!D.alloc(D.arena[0], cap)) return fail(GEQ_ERR_OUT_OF_MEMORY, "energy arena of %llu words", cap);
@@ -2621,7 +2649,6 @@ geq_status Engine::finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out) {
   kp.bigq = D.bigq;
   kp.cw = D.cw;
   kp.missing = nullptr;
-  if (N) k_missing_init<<<grid, 256, 0, S>>>(kp, D.desc_init, D.missing_init);
   kp.el = D.conf.elements; kp.mx = D.conf.max; kp.eb = D.conf.energy_bits(); kp.em = D.conf.energy_mask();
   kp.ub = D.conf.update_bits(); kp.um = D.conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
@@ -2759,10 +2786,20 @@ geq_status Engine::solve_begin(DeviceGamesImpl &dg) {
   CU(cudaMemcpyAsync(dg.arena[a0], dg.init_data, dg.init_total * 4, cudaMemcpyDeviceToDevice, S));
   if (dg.next_stamp > 0xF0000000u) dg.next_stamp = 1;
   CU(cudaMemsetAsync(dg.mark, 0, 2ull * dg.kp.mwords * 4, S));
-  // defenders wait for their successors' lists (GEQ_TUNE_NO_READY: push
-  // every predecessor, as the reference's visit lists do)
-  dg.kp.missing = (tuning.flags & GEQ_TUNE_NO_READY) ? nullptr : dg.missing;
-  if (dg.kp.missing && dg.N) CU(cudaMemcpyAsync(dg.missing, dg.missing_init, dg.N * 4, cudaMemcpyDeviceToDevice, S));
+  dg.kp.cw = (tuning.flags & GEQ_TUNE_NO_EDGE_PAIRS) ? nullptr : dg.cw;
+  // GEQ_TUNE_READY: defenders wait for their successors' lists (counted per
+  // defender, set up at the first such solve); else every predecessor of a
+  // changed position is pushed, as the reference's visit lists do
+  dg.kp.missing = nullptr;
+  if ((tuning.flags & GEQ_TUNE_READY) && dg.N) {
+    if (!dg.missing) {
+      if (!dg.alloc(dg.missing, dg.N) || !dg.alloc(dg.missing_init, dg.N))
+        return fail(GEQ_ERR_OUT_OF_MEMORY, "defender counts for %llu positions", dg.N);
+      k_missing_init<<<(unsigned)std::max(1, n_sms * 8), 256, 0, S>>>(dg.kp, dg.desc_init, dg.missing_init);
+    }
+    CU(cudaMemcpyAsync(dg.missing, dg.missing_init, dg.N * 4, cudaMemcpyDeviceToDevice, S));
+    dg.kp.missing = dg.missing;
+  }
   Ctr h{};
   h.arena = dg.arena[a0];
   h.arena_cap = dg.arena_cap[a0];
@@ -2772,6 +2809,11 @@ geq_status Engine::solve_begin(DeviceGamesImpl &dg) {
   CU(cudaMemcpyAsync(dg.ctr, s.h_ctr, sizeof(Ctr), cudaMemcpyHostToDevice, S));
   if (dg.std_reach && dg.N) {
     k_init_frontier_std<<<(unsigned)std::max(1, n_sms * 16), 256, 0, S>>>(dg.kp);
+    if (!dg.off_ranges.empty()) {
+      geq_status cr = clear_off_ranges(dg, h.stamp);
+      if (cr) return cr;
+      pr.launches++;
+    }
     k_fcount<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
     k_ffill<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
     pr.launches += 3;
@@ -2779,11 +2821,115 @@ geq_status Engine::solve_begin(DeviceGamesImpl &dg) {
     const unsigned grid = (unsigned)std::max<unsigned long long>(
         1, std::min<unsigned long long>((dg.n_reach + 7) / 8, (unsigned long long)n_sms * 16));
     k_init_frontier<<<grid, 256, 0, S>>>(dg.kp, dg.reach, dg.n_reach);
+    if (!dg.off_ranges.empty()) {
+      geq_status cr = clear_off_ranges(dg, h.stamp);
+      if (cr) return cr;
+      pr.launches++;
+    }
     k_fcount<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
     k_ffill<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
     pr.launches += 3;
   }
   CU(cudaGetLastError());
+  return GEQ_OK;
+}
+
+// Games that are not to be solved: their initial frontier is cleared, so no
+// position of theirs is ever computed (games share no edges).
+void Engine::skip_games(DeviceGamesImpl &dg, const std::vector<uint32_t> &games) {
+  for (uint32_t g : games) {
+    dg.off_ranges.push_back(dg.node_base[g]);
+    dg.off_ranges.push_back(dg.node_base[g + 1]);
+  }
+}
+geq_status Engine::clear_off_ranges(DeviceGamesImpl &dg, uint32_t stamp) {
+  State &s = *st;
+  const size_t bytes = dg.off_ranges.size() * 8;
+  unsigned long long *d = (unsigned long long *)s.pool.get(bytes);
+  if (!d) return fail(GEQ_ERR_OUT_OF_MEMORY, "skipped games");
+  CU(cudaMemcpyAsync(d, dg.off_ranges.data(), bytes, cudaMemcpyHostToDevice, s.stream));
+  const uint32_t n = (uint32_t)(dg.off_ranges.size() / 2);
+  k_clear_ranges<<<std::min<uint32_t>(n, 1024), 256, 0, s.stream>>>(dg.mark + (stamp & 1u) * dg.kp.mwords, d, n);
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(s.stream));  // the ranges are pageable host memory
+  s.pool.put(d, bytes);
+  return GEQ_OK;
+}
+
+// Lists of whole games (or only their first position): the selection is
+// expanded, counted, scanned and gathered on the device and read back into
+// page-locked blocks; solution game i is games[i].
+geq_status Engine::download_games(DeviceGamesImpl &dg, const std::vector<uint32_t> &games, bool first_only,
+                                  geq_solution &sol) {
+  State &s = *st;
+  cudaStream_t S = s.stream;
+  const uint32_t G = (uint32_t)games.size();
+  std::vector<unsigned long long> hb(2 * (size_t)G + 1);  // bases, then prefix of counts
+  unsigned long long K = 0;
+  for (uint32_t i = 0; i < G; i++) {
+    const uint32_t g = games[i];
+    hb[i] = dg.node_base[g];
+    hb[G + i] = K;
+    K += first_only ? 1ull : dg.node_base[g + 1] - dg.node_base[g];
+  }
+  hb[2 * (size_t)G] = K;
+  unsigned long long launches = 0;
+  geq_status a = ensure_cnt(s, K + 1);
+  if (a) return a;
+  const size_t hb_bytes = hb.size() * 8;
+  unsigned long long *d_hb = (unsigned long long *)s.pool.get(hb_bytes);
+  uint32_t *d_sel = (uint32_t *)s.pool.get(std::max<unsigned long long>(K, 1) * 4);
+  unsigned long long *goff = (unsigned long long *)s.pool.get((K + 1) * 8);
+  unsigned long long *rel = (unsigned long long *)s.pool.get((K + G) * 8);
+  struct Give {
+    State &s;
+    std::vector<std::pair<void *, size_t>> v;
+    ~Give() {
+      for (auto &x : v)
+        if (x.first) s.pool.put(x.first, x.second);
+    }
+  } give{s, {{d_hb, hb_bytes}, {d_sel, std::max<unsigned long long>(K, 1) * 4}, {goff, (K + 1) * 8},
+             {rel, (K + G) * 8}}};
+  if (!d_hb || !d_sel || !goff || !rel) return fail(GEQ_ERR_OUT_OF_MEMORY, "selection of %u games", G);
+  CU(cudaMemcpyAsync(d_hb, hb.data(), hb_bytes, cudaMemcpyHostToDevice, S));
+  const unsigned grid = (unsigned)std::max(1, n_sms * 8);
+  if (K) {
+    k_sel_expand<<<grid, 256, 0, S>>>(d_hb, d_hb + G, G, K, d_sel);
+    k_sel_counts<<<grid, 256, 0, S>>>(dg.desc, d_sel, K, s.cnt);
+  }
+  if ((a = scan_u32(s, s.cnt, K, goff, launches))) return a;
+  k_rel_offsets<<<grid, 256, 0, S>>>(goff, K, d_hb + G, G, rel);
+  unsigned long long total = 0;
+  CU(cudaMemcpyAsync(&s.h_ctr->positions, goff + K, 8, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  total = s.h_ctr->positions;
+  uint32_t *out = (uint32_t *)s.pool.get(std::max<unsigned long long>(total, 1) * 4);
+  if (!out) return fail(GEQ_ERR_OUT_OF_MEMORY, "selection data");
+  give.v.push_back({out, std::max<unsigned long long>(total, 1) * 4});
+  if (K) k_sel_gather<<<grid, 256, 0, S>>>(dg.desc, d_sel, K, goff, dg.arena[dg.arena_cur], dg.kp.ib, dg.kp.ibm, out);
+  CU(cudaGetLastError());
+  sol.energy_size = 1;
+  sol.offsets.clear();
+  sol.data.clear();
+  const bool pinned = sol.off_buf.alloc(s.hpool, (K + G) * 8) && sol.data_buf.alloc(s.hpool, std::max<unsigned long long>(total, 1) * 4);
+  if (!pinned) return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu offsets", K + G);
+  CU(cudaMemcpyAsync(sol.off_buf.p, rel, (K + G) * 8, cudaMemcpyDeviceToHost, S));
+  if (total) CU(cudaMemcpyAsync(sol.data_buf.p, out, total * 4, cudaMemcpyDeviceToHost, S));
+  CU(cudaStreamSynchronize(S));
+  sol.n_offsets = K + G;
+  sol.n_words = total;
+  sol.n_vertices.resize(G);
+  sol.offsets_base.resize(G);
+  sol.data_base.resize(G);
+  const unsigned long long *ro = (const unsigned long long *)sol.off_buf.p;
+  unsigned long long db = 0;
+  for (uint32_t i = 0; i < G; i++) {
+    const unsigned long long n = hb[G + i + 1] - hb[G + i];
+    sol.n_vertices[i] = (uint32_t)n;
+    sol.offsets_base[i] = hb[G + i] + i;
+    sol.data_base[i] = db;
+    db += ro[hb[G + i] + i + n];
+  }
   return GEQ_OK;
 }
 

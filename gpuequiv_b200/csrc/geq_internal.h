@@ -191,6 +191,12 @@ class Engine {
   geq_status solve_stats(DeviceGamesImpl &dg, geq_solve_stats *stats);
   // active[g] = 1 while game g has a position in the frontier
   geq_status active_games(DeviceGamesImpl &dg, std::vector<uint8_t> &active);
+  // games never to be solved from the next solve_begin on (their lists stay initial)
+  void skip_games(DeviceGamesImpl &dg, const std::vector<uint32_t> &games);
+  // the lists of the listed games (all positions, or the first only), one
+  // solution game per listed game, in page-locked memory
+  geq_status download_games(DeviceGamesImpl &dg, const std::vector<uint32_t> &games, bool first_only,
+                            geq_solution &sol);
   static uint32_t game_positions(const DeviceGamesImpl &dg, uint32_t g);
   static uint32_t n_games_of(const DeviceGamesImpl &dg);
   // All positions of all games.
@@ -232,6 +238,7 @@ class Engine {
   std::unique_ptr<State> st;
 
  private:
+  geq_status clear_off_ranges(DeviceGamesImpl &dg, uint32_t stamp);
   geq_status alloc_work(DeviceGamesImpl &D, bool any_init);
   geq_status finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out);
 };

@@ -164,17 +164,13 @@ void fail_req(Request *r, geq_status st, const std::string &msg, std::vector<Req
 
 // Read back and answer the listed games of a session.
 geq_status retire(Engine &e, Session &ss, const std::vector<uint32_t> &games, std::vector<Request *> &done) {
-  const uint32_t G = Engine::n_games_of(*ss.dg);
-  std::vector<uint32_t> first(G, 0), count(G, 0), want;
+  std::vector<uint32_t> want;
   for (uint32_t g : games)
-    if (ss.req[g]) {
-      count[g] = ss.first_only ? 1u : Engine::game_positions(*ss.dg, g);
-      want.push_back(g);
-    }
+    if (ss.req[g]) want.push_back(g);
   geq_solve_stats stt{};
   geq_status st = e.solve_stats(*ss.dg, &stt);
   geq_solution part;
-  if (!st && !want.empty()) st = e.download_selected(*ss.dg, first, count, part);
+  if (!st && !want.empty()) st = e.download_games(*ss.dg, want, ss.first_only, part);
   for (uint32_t g : games) {
     ss.retired[g] = 1;
     ss.live--;
@@ -185,9 +181,9 @@ geq_status retire(Engine &e, Session &ss, const std::vector<uint32_t> &games, st
     return st;
   }
   part.stats = stt;
-  for (uint32_t g : want) {
-    Request *r = ss.req[g];
-    r->sol = split_one(part, g);
+  for (uint32_t i = 0; i < want.size(); i++) {
+    Request *r = ss.req[want[i]];
+    r->sol = split_one(part, i);
     done.push_back(r);
   }
   return GEQ_OK;
@@ -263,7 +259,17 @@ void start_compares(Engine &e, int device, uint64_t max_positions, std::vector<R
   std::unique_ptr<Session> ss(new Session());
   geq_status st = build_and_upload(e, device, n, L.data(), start_off.data(), p.data(), q.data(), max_positions, ss->dg,
                                    nullptr, &trivial, &over);
-  if (!st && ss->dg) st = e.solve_begin(*ss->dg);
+  if (!st && ss->dg) {
+    // the games cut at the position bound are never solved
+    std::vector<uint32_t> skip;
+    for (uint32_t i = 0, k = 0; i < n; i++)
+      if (!trivial[i]) {
+        if (over[i]) skip.push_back(k);
+        k++;
+      }
+    if (!skip.empty()) e.skip_games(*ss->dg, skip);
+    st = e.solve_begin(*ss->dg);
+  }
   if (st) {
     if (n > 1) {
       for (Request *r : batch) {
@@ -302,7 +308,11 @@ void start_compares(Engine &e, int device, uint64_t max_positions, std::vector<R
 
 // One step of a session, then the games that reached their fixpoint retire.
 // false: the session is finished (or failed) and can be dropped.
-bool step_session(Engine &e, Session &ss, std::vector<Request *> &done) {
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+bool step_session(Engine &e, Session &ss, std::vector<Request *> &done, double &retire_ms) {
   bool fin = false;
   geq_status st = e.solve_step(*ss.dg, fin);
   std::vector<uint32_t> ret;
@@ -323,7 +333,11 @@ bool step_session(Engine &e, Session &ss, std::vector<Request *> &done) {
     ss.live = 0;
     return false;
   }
-  if (!ret.empty()) retire(e, ss, ret, done);
+  if (!ret.empty()) {
+    const auto t0 = std::chrono::steady_clock::now();
+    retire(e, ss, ret, done);
+    retire_ms += ms_since(t0);
+  }
   return ss.live > 0;
 }
 
@@ -364,7 +378,9 @@ void pipeline(geq_server *s, Engine *e) {
       }
     }
     std::vector<Request *> done;
+    double admit_ms = 0, step_ms = 0, retire_ms = 0;
     if (!batch.empty()) {
+      const auto t0 = std::chrono::steady_clock::now();
       std::vector<Request *> games, compares, wide;
       uint64_t fg = 0, fc = 0;
       for (Request *r : batch) {
@@ -386,22 +402,32 @@ void pipeline(geq_server *s, Engine *e) {
         run_wide(*e, s->device, wide);
         done.insert(done.end(), wide.begin(), wide.end());
       }
+      admit_ms = ms_since(t0);
     }
     // one step of every resident session
+    const auto t1 = std::chrono::steady_clock::now();
     for (size_t k = 0; k < active.size();) {
-      if (step_session(*e, *active[k], done)) {
+      if (step_session(*e, *active[k], done, retire_ms)) {
         k++;
       } else {
         used -= std::min(used, active[k]->footprint);
         active.erase(active.begin() + k);
       }
     }
+    step_ms = ms_since(t1) - retire_ms;
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->stats.admit_ms += admit_ms;
+      s->stats.step_ms += step_ms;
+      s->stats.retire_ms += retire_ms;
+    }
     finish(s, done);
   }
   // stopped: the sessions in flight finish
   for (auto &ss : active) {
     std::vector<Request *> done;
-    while (step_session(*e, *ss, done)) {
+    double retire_ms = 0;
+    while (step_session(*e, *ss, done, retire_ms)) {
     }
     finish(s, done);
   }

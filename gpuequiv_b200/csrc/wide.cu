@@ -548,7 +548,13 @@ static geq_status solve_one_game(cudaStream_t S, int n_sms, const GameInput &gi,
     WCU(cudaMemcpyAsync(d_arena, init_words.data(), init_words.size() * 4, cudaMemcpyHostToDevice, S));
   if (gi.n_reach) WCU(cudaMemcpyAsync(d_reach, gi.to_reach, gi.n_reach * 4ull, cudaMemcpyHostToDevice, S));
   WCU(cudaMemsetAsync(d_mark, 0, mwords * 4ull, S));
-  WCU(cudaMemsetAsync(d_ctr, 0, sizeof(Ctr), S));
+  {
+    // new lists go after the initial ones
+    Ctr h0{};
+    h0.arena_top = init_e;
+    WCU(cudaMemcpyAsync(d_ctr, &h0, sizeof(Ctr), cudaMemcpyHostToDevice, S));
+    WCU(cudaStreamSynchronize(S));  // h0 is on the stack
+  }
 
   p.row = d_row; p.col = d_col; p.wt = d_wt; p.rrow = d_rrow; p.rcol = d_rcol; p.att = d_att;
   p.desc = d_desc; p.arena = d_arena; p.arena_cap = arena_cap;

@@ -326,9 +326,10 @@ def _flat_lists(sol, graphs):
     flat_o = _borrow(po, no.value, C.c_uint64, np.uint64, owner)
     flat_d = _borrow(pd, nw.value, C.c_uint32, np.uint32, owner)
     nv = np.fromiter((g.n_vertices() for g in graphs), dtype=np.int64, count=n)
+    es = graphs[0].get_conf().energy_size() if n else 1
     ob = np.zeros(n + 1, np.int64)
     np.cumsum(nv + 1, out=ob[1:])
-    tot = flat_o[ob[1:] - 1].astype(np.int64) if n else np.zeros(0, np.int64)
+    tot = flat_o[ob[1:] - 1].astype(np.int64) * es if n else np.zeros(0, np.int64)
     db = np.zeros(n + 1, np.int64)
     np.cumsum(tot, out=db[1:])
     obl, dbl = ob.tolist(), db.tolist()

@@ -164,10 +164,11 @@ uint32_t geq_solution_n_games(const geq_solution *s);
 geq_status geq_solution_lists(const geq_solution *s, uint32_t game, geq_energy_lists *out);
 /* All games' lists at once (borrowed): game g's n_vertices(g)+1 offsets start
  * at offsets[first_offset(g)] where first_offset(g) = sum over h < g of
- * (n_vertices(h) + 1); they are relative to game g's first word, and game g's
- * words follow game g-1's in `data`.  Lets a binding hand the whole batch to
- * its caller without per-game calls.  No counterpart in the crate, whose
- * results are per EnergyGame. */
+ * (n_vertices(h) + 1); they count energies from game g's first energy, and
+ * game g's energies follow game g-1's in `data`; *n_words is the number of
+ * words in `data` (energies x energy_size).  Lets a binding hand the whole
+ * batch to its caller without per-game calls.  No counterpart in the crate,
+ * whose results are per EnergyGame. */
 geq_status geq_solution_flat(const geq_solution *s, const uint64_t **offsets, uint64_t *n_offsets,
                              const uint32_t **data, uint64_t *n_words);
 void geq_solution_stats(const geq_solution *s, geq_solve_stats *out);
@@ -275,7 +276,11 @@ typedef struct geq_server_config {
 typedef struct geq_server_stats {
   uint64_t submitted, completed, failed, batches, queued, running;
   uint64_t games_in_batches;     /* sum of batch sizes */
-  uint64_t max_batch_footprint;  /* bytes, largest admitted batch estimate */
+  uint64_t max_batch_footprint;  /* bytes, largest resident footprint estimate */
+  double admit_ms;               /* pipeline threads' wall time: staging, upload (and
+                                    minimisation + GameBuild of queries) of batches */
+  double step_ms;                /* ... rounds of resident batches */
+  double retire_ms;              /* ... reading back and answering finished games */
 } geq_server_stats;
 /* The server solves on the device of `ctx` and copies its tuning; ctx may be
  * destroyed afterwards.  cfg may be NULL (defaults). */
@@ -324,8 +329,10 @@ typedef struct geq_tuning {
 #define GEQ_TUNE_NO_SPLIT 32u     /* a large batch on one engine, not as two pipelined halves */
 #define GEQ_TUNE_BUILD_WARP_ALL 64u /* device GameBuild: every attack position by the warp path (cross-check) */
 #define GEQ_TUNE_FORCE_WIDE 128u  /* geq_energy_game_run(_batch): the multi-word solver for every conf (cross-check) */
-#define GEQ_TUNE_NO_READY 256u    /* push every predecessor of a changed position, also defenders that still
-                                     wait for an empty successor (cross-check) */
+#define GEQ_TUNE_READY 256u       /* count per defender the successors without energies and push a defender
+                                     only once it has none (the reference visits and skips it); measured
+                                     slower on the spectroscopy batch, off by default */
+#define GEQ_TUNE_NO_EDGE_PAIRS 512u /* the lane path reads col / wt and decodes updates (cross-check) */
 geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t);
 void geq_context_get_tuning(const geq_context *ctx, geq_tuning *t);
 

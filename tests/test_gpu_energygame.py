@@ -28,8 +28,8 @@ MODES = {
     "bps5": dict(blocks_per_sm=5, rounds_per_graph=16),
     # tighter lane-path limits: more positions take the warp routines
     "lanes_small": dict(lane_limits=(4, 8, 4)),
-    # every predecessor pushed, as the reference's visit lists
-    "noready": dict(flags=256),
+    # defenders pushed only once every successor has energies
+    "ready": dict(flags=256),
 }
 
 
