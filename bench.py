@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--query-bound", type=int, default=200_000,
                     help="position bound of a served query's game (larger games are refused)")
     ap.add_argument("--query-pool", type=int, default=2048, help="distinct queries the arrivals draw from")
-    ap.add_argument("--large-states", type=int, default=0,
+    ap.add_argument("--large-states", type=int, default=12800,
                     help="states of the single-LTS equivalences() leg (the large generator; 0: none)")
     ap.add_argument("--no-stress", dest="stress", action="store_false", help="skip the stress-game leg")
     ap.add_argument("--solve-only", action="store_true",
@@ -545,16 +545,17 @@ def run_large(ctx, n_states: int, check: bool, pairs: int = 48) -> dict:
         return out
     from oracle import ora
     rng = np.random.default_rng(5)
-    olts = ora.Lts.from_arrays(src, dst, lab)
+    red, mp = ora.Lts.from_arrays(src, dst, lab).bisimilar_minimize()  # as compare() does, once
     checked = bad = 0
     for _ in range(pairs * 50):
         if checked >= pairs:
             break
         p, q = (int(x) for x in rng.integers(0, n_states, 2))
         mine = eq.energies(p, q)
-        if p == q or mine is None:
+        if p == q or mine is None or mp[p] == mp[q]:
             continue
-        ref = ora.compare(olts, p, q)
+        b = ora.Build.compare(red, int(mp[p]), int(mp[q]), positions=False)
+        ref = ora.run_game(6, 3, b.row, b.col, b.wt, b.attacker, ora.standard_reach(b.row, b.attacker)).lists()[0]
         checked += 1
         if sorted(int(x) for x in mine.array.reshape(-1)) != sorted(int(x) for x in np.asarray(ref).reshape(-1)):
             bad += 1

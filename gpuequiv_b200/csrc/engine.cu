@@ -1032,7 +1032,14 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
     // attack_update.wgsl + attack_minimize.wgsl: successor candidates, then
     // the own energies; changed iff a minimal value has no own copy
     if (cv > p.tk) return T_BIG;
+    // the own energies first (the old minimal set, all flagged own): in the
+    // common case that nothing changes, every successor candidate then meets
+    // a member below it at once.  The minimal set is the same in any order;
+    // a candidate equal to an own member is dropped, so the own copy stays
+    // (the later copy wins, attack_minimize.wgsl:84-92).
     uint32_t n = 0, om = 0, tot = 0;
+    for (uint32_t q = 0; q < cv; q++)
+      if (!ac_insert(scr, 0, n, om, cd.to_t(lelem(dv, q, arena, cap, c, p.ib, p.ibm)), true)) return T_BIG;
     for (uint32_t j0 = 0; j0 < d; j0 += 4) {
       uint32_t w[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
       unsigned long long dw[4] = {0, 0, 0, 0};
@@ -1052,8 +1059,6 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
               return T_BIG;
         }
     }
-    for (uint32_t q = 0; q < cv; q++)
-      if (!ac_insert(scr, 0, n, om, cd.to_t(lelem(dv, q, arena, cap, c, p.ib, p.ibm)), true)) return T_BIG;
     edges += d;
     bytes += 12u + 4u * cv + 16u * d + 4u * tot;
     if (om == (1u << n) - 1u) return T_UNCHANGED;
@@ -1061,58 +1066,62 @@ __device__ int thread_solve(const KParams &p, Ctr *c, const Cd &cd, const uint32
     out_cnt = n;
     return T_CHANGED;
   }
-  // defender: skipped while a successor has no energies (energygame.rs:789-792)
-  for (uint32_t j0 = 0; j0 < d; j0 += 4) {
-    uint32_t w[4] = {0, 0, 0, 0};
-#pragma unroll
-    for (int t = 0; t < 4; t++)
-      if (j0 + t < d) w[t] = ld(p.col, (unsigned long long)e0 + j0 + t, p.n_edges, c);
-#pragma unroll
-    for (int t = 0; t < 4; t++)
-      if (j0 + t < d && dcnt(ld(p.desc, w[t], p.n_nodes, c)) == 0u) return T_SKIPPED;
-  }
-  uint32_t n;
+  // defender: skipped while a successor has no energies
+  // (energygame.rs:789-792); successors read four at a time, each group
+  // checked for an empty list before it is folded in.  d == 1: the
+  // successor's updated list as is (defend_iterative.wgsl:200-211); else the
+  // fold of pairwise suprema, minimised after every step
+  // (defend_iterative.wgsl:215-262) -- the first list minimised too, which
+  // leaves the minimal suprema unchanged.
+  uint32_t n = 0;
   {
-    uint32_t w0, u0;
-    load_edge(p, c, e0, w0, u0);
-    const unsigned long long d0 = ld(p.desc, w0, p.n_nodes, c);
-    const uint32_t s = dcnt(d0);
-    const auto pu0 = edge_upd(p, cd, u0);
-    unsigned long long tot = s;
-    if (d == 1) {
-      // single successor: its updated list as is (defend_iterative.wgsl:200-211)
-      if (s > p.tk) return T_BIG;
-      for (uint32_t q = 0; q < s; q++)
-        SCR(TK + q) = cd.to_p(cd.apply(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), pu0));
-      n = s;
-    } else {
-      // fold of pairwise suprema, minimised after every step
-      // (defend_iterative.wgsl:215-262); the first list minimised
-      // too, which leaves the minimal suprema unchanged
-      if (s > p.tw) return T_BIG;
-      uint32_t sb = 0, nb = TK, ns = 0, om = 0;
-      for (uint32_t q = 0; q < s; q++)
-        if (!ac_insert(scr, sb, ns, om, cd.apply(cd.to_t(lelem(d0, q, arena, cap, c, p.ib, p.ibm)), pu0), false))
-          return T_BIG;
-      for (uint32_t j = 1; j < d; j++) {
-        uint32_t w, u;
-        load_edge(p, c, (unsigned long long)e0 + j, w, u);
-        const unsigned long long db = ld(p.desc, w, p.n_nodes, c);
-        const uint32_t cb = dcnt(db);
+    uint32_t sb = 0, nb = TK, ns = 0, om = 0;
+    unsigned long long tot = 0;
+    for (uint32_t j0 = 0; j0 < d; j0 += 4) {
+      uint32_t w[4] = {0, 0, 0, 0}, u[4] = {0, 0, 0, 0};
+      unsigned long long dw[4] = {0, 0, 0, 0};
+      load_edges4(p, c, e0 + j0, d - j0, w, u);
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+        if (j0 + t < d) dw[t] = ld(p.desc, w[t], p.n_nodes, c);
+#pragma unroll
+      for (int t = 0; t < 4; t++)
+        if (j0 + t < d && dcnt(dw[t]) == 0u) return T_SKIPPED;
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        if (j0 + t >= d) continue;
+        const uint32_t cb = dcnt(dw[t]);
         tot += cb;
+        const auto pu = edge_upd(p, cd, u[t]);
+        if (j0 + t == 0) {
+          if (d == 1) {
+            if (cb > p.tk) return T_BIG;
+            for (uint32_t q = 0; q < cb; q++)
+              SCR(TK + q) = cd.to_p(cd.apply(cd.to_t(lelem(dw[t], q, arena, cap, c, p.ib, p.ibm)), pu));
+            n = cb;
+          } else {
+            if (cb > p.tw) return T_BIG;
+            for (uint32_t q = 0; q < cb; q++)
+              if (!ac_insert(scr, sb, ns, om, cd.apply(cd.to_t(lelem(dw[t], q, arena, cap, c, p.ib, p.ibm)), pu),
+                             false))
+                return T_BIG;
+          }
+          continue;
+        }
         if (ns * cb > p.tw) return T_BIG;
-        const auto pu = edge_upd(p, cd, u);
         uint32_t nn = 0;
         for (uint32_t q = 0; q < cb; q++) {
-          const uint32_t bq = cd.apply(cd.to_t(lelem(db, q, arena, cap, c, p.ib, p.ibm)), pu);
+          const uint32_t bq = cd.apply(cd.to_t(lelem(dw[t], q, arena, cap, c, p.ib, p.ibm)), pu);
           for (uint32_t k = 0; k < ns; k++)
             if (!ac_insert(scr, nb, nn, om, SCR(sb + k) | bq, false)) return T_BIG;
         }
-        const uint32_t t = sb;
+        const uint32_t tmp = sb;
         sb = nb;
-        nb = t;
+        nb = tmp;
         ns = nn;
       }
+    }
+    if (d > 1) {
       for (uint32_t q = 0; q < ns; q++) SCR(TK + q) = cd.to_p(SCR(sb + q));
       n = ns;
     }

@@ -38,6 +38,9 @@ namespace {
 constexpr uint64_t BATCH_BASE_BYTES = 32ull << 20;
 // resident batches per pipeline (more arrivals wait and are batched together)
 constexpr size_t MAX_SESSIONS = 4;
+// equivalence queries per batch: a batch's device GameBuild runs as many
+// levels as its deepest game, which every query of the batch waits for
+constexpr size_t MAX_COMPARE_BATCH = 128;
 uint64_t game_footprint(uint64_t n, uint64_t m) { return 2 * (70 * n + 12 * m) + 4096; }
 // A compare query's game is not known before it is built: estimated at 16
 // positions and 64 edges per state and transition of its LTS, plus the
@@ -361,8 +364,11 @@ void pipeline(geq_server *s, Engine *e) {
       }
       // admit what has arrived, while it fits beside the resident sessions
       // (a pipeline without sessions always takes the first request)
+      size_t n_compares = 0;
       while (!s->queue.empty() && batch.size() < s->cfg.max_batch_games && active.size() < MAX_SESSIONS) {
         Request *r = s->queue.front();
+        if (r->kind && n_compares >= MAX_COMPARE_BATCH) break;
+        n_compares += r->kind ? 1 : 0;
         if ((!batch.empty() || !active.empty()) && used + fp + r->footprint > s->budget) break;
         fp += r->footprint;
         s->queue.pop_front();
