@@ -295,9 +295,11 @@ def peak_hbm():
 class Load:
     """Drives a geq_server from host threads through the C ABI: arrival i
     submits item pick[i] (a game view or an (lts, p, q) query) at its arrival
-    time (open loop) or as soon as a previous request of its thread finished
-    (closed loop, `outstanding` requests in flight).  Latency = submit ->
-    the request's solution in the caller's hands (geq_server_poll returned)."""
+    time (open loop) or whenever fewer than `outstanding` requests are in
+    flight (closed loop).  Finished requests are taken from the server's
+    completion queue (geq_server_poll_any) in the order they finish, so one
+    slow request does not hold back the recording of others.  Latency =
+    submit -> the request's solution in the caller's hands."""
 
     def __init__(self, srv, items, queries: bool, threads: int = 4):
         from gpuequiv_b200._lib import lib
@@ -315,83 +317,111 @@ class Load:
             raise RuntimeError(f"submit failed: status {st}")
         return t.value
 
-    def _poll(self, ticket):
+    def _poll_any(self, timeout_ms):
+        """(ticket, status) of a finished request, or None after timeout_ms."""
         import ctypes as C
         sol = C.c_void_p()
-        st = self.lib.geq_server_poll(self.h, ticket, -1, C.byref(sol))
+        t = C.c_uint64()
+        st = self.lib.geq_server_poll_any(self.h, timeout_ms, C.byref(t), C.byref(sol))
+        if t.value == 0:
+            return None
         if st == 0:
             self.lib.geq_solution_free(sol)
-        return st
+        return t.value, st
+
+    def _pollers(self, total_fn, done):
+        """Poller threads appending (ticket, time, status) to `done` until
+        total_fn() requests have finished (total_fn None: not known yet)."""
+        import threading
+
+        def poller():
+            while True:
+                n = total_fn()
+                if n is not None and len(done) >= n:
+                    return
+                r = self._poll_any(50)
+                if r is not None:
+                    done.append((r[0], time.perf_counter(), r[1]))
+
+        th = [threading.Thread(target=poller) for _ in range(max(1, self.threads // 2))]
+        for x in th:
+            x.start()
+        return th
 
     def open_loop(self, arrivals, pick):
-        import queue
         import threading
         n = len(arrivals)
-        t_sub, t_done, status = np.zeros(n), np.zeros(n), np.zeros(n, np.int32)
+        subs, done = [], []
         t0 = time.perf_counter() + 0.05
 
-        def submitter(k, q):
+        def submitter(k):
+            mine = []
             for i in range(k, n, self.threads):
                 wait = t0 + arrivals[i] - time.perf_counter()
                 if wait > 0:
                     time.sleep(wait)
-                t_sub[i] = time.perf_counter()
-                q.put((i, self._submit(self.items[pick[i]])))
-            q.put(None)
+                ts = time.perf_counter()
+                mine.append((self._submit(self.items[pick[i]]), ts))
+            subs.extend(mine)
 
-        def poller(q):
-            while True:
-                x = q.get()
-                if x is None:
-                    return
-                i, t = x
-                status[i] = self._poll(t)
-                t_done[i] = time.perf_counter()
-
-        qs = [queue.Queue() for _ in range(self.threads)]
-        th = [threading.Thread(target=submitter, args=(k, qs[k])) for k in range(self.threads)]
-        th += [threading.Thread(target=poller, args=(qs[k],)) for k in range(self.threads)]
+        th = [threading.Thread(target=submitter, args=(k,)) for k in range(self.threads)]
         for x in th:
             x.start()
-        for x in th:
+        pol = self._pollers(lambda: n, done)
+        for x in th + pol:
             x.join()
-        return t_sub, t_done, status, t0
+        sub = dict(subs)
+        lat = np.array([(td - sub[t]) * 1e3 for t, td, _ in done])
+        status = np.array([st for _, _, st in done], np.int32)
+        t_end = max(td for _, td, _ in done)
+        return lat, status, t_end - t0
 
     def closed_loop(self, pick, outstanding: int, seconds: float):
-        import collections
         import threading
-        per = max(1, outstanding // self.threads)
-        lat, stat, done_at = [], [], []
-        lock = threading.Lock()
+        subs, done = [], []
+        slots = threading.Semaphore(outstanding)
         t0 = time.perf_counter()
         t_end = t0 + seconds
+        n_sub = [0]
+        stop = [False]
 
-        def worker(k):
+        def submitter(k):
             rng = np.random.default_rng(k)
-            fifo = collections.deque()
-            my_lat, my_stat, my_done = [], [], []
-            while True:
-                while len(fifo) < per and time.perf_counter() < t_end:
-                    fifo.append((time.perf_counter(), self._submit(self.items[pick[int(rng.integers(len(pick)))]])))
-                if not fifo:
-                    break
-                ts, t = fifo.popleft()
-                st = self._poll(t)
-                now = time.perf_counter()
-                my_lat.append((now - ts) * 1e3)
-                my_stat.append(st)
-                my_done.append(now)
-            with lock:
-                lat.extend(my_lat)
-                stat.extend(my_stat)
-                done_at.extend(my_done)
+            mine = []
+            while time.perf_counter() < t_end:
+                if not slots.acquire(timeout=0.05):
+                    continue
+                ts = time.perf_counter()
+                mine.append((self._submit(self.items[pick[int(rng.integers(len(pick)))]]), ts))
+            subs.extend(mine)
 
-        th = [threading.Thread(target=worker, args=(k,)) for k in range(self.threads)]
+        def releaser():
+            seen = 0
+            while not stop[0]:
+                while seen < len(done):
+                    slots.release()
+                    seen += 1
+                time.sleep(0.0005)
+
+        th = [threading.Thread(target=submitter, args=(k,)) for k in range(2)]
+        rel = threading.Thread(target=releaser)
         for x in th:
             x.start()
+        rel.start()
+        total = [None]
+        pol = self._pollers(lambda: total[0], done)
         for x in th:
             x.join()
-        return np.array(lat), np.array(stat, np.int32), np.array(done_at), t0
+        total[0] = len(subs)
+        for x in pol:
+            x.join()
+        stop[0] = True
+        rel.join()
+        sub = dict(subs)
+        lat = np.array([(td - sub[t]) * 1e3 for t, td, _ in done])
+        status = np.array([st for _, _, st in done], np.int32)
+        span = max(td for _, td, _ in done) - t0
+        return lat, status, span
 
 
 def _lat_summary(lat_ms, status, span_s):
@@ -424,9 +454,9 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
             arrivals = np.sort(rng.uniform(0, seconds, n))
             pick = rng.integers(0, len(items), n)
             st0 = srv.stats()
-            t_sub, t_done, status, t0 = load.open_loop(arrivals, pick)
+            lat, status, span = load.open_loop(arrivals, pick)
             st = srv.stats()
-            r = _lat_summary((t_done - t_sub) * 1e3, status, t_done.max() - t0)
+            r = _lat_summary(lat, status, span)
             batches = st["batches"] - st0["batches"]
             r.update({"lambda_req_s": lam, "batches": int(batches),
                       "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches),
@@ -435,9 +465,9 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
         if saturation_s > 0:
             pick = np.arange(len(items))
             st0 = srv.stats()
-            lat, status, done_at, t0 = load.closed_loop(pick, outstanding, saturation_s)
+            lat, status, span = load.closed_loop(pick, outstanding, saturation_s)
             st = srv.stats()
-            r = _lat_summary(lat, status, done_at.max() - t0)
+            r = _lat_summary(lat, status, span)
             batches = st["batches"] - st0["batches"]
             r.update({"outstanding": outstanding, "batches": int(batches),
                       "mean_batch": (st["games_in_batches"] - st0["games_in_batches"]) / max(1, batches),

@@ -149,6 +149,7 @@ _SIGS = {
     "geq_server_submit": ([vp, C.POINTER(geq_game_graph), C.POINTER(C.c_uint64)], C.c_int),
     "geq_server_submit_compare": ([vp, vp, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint64)], C.c_int),
     "geq_server_poll": ([vp, C.c_uint64, C.c_int32, C.POINTER(vp)], C.c_int),
+    "geq_server_poll_any": ([vp, C.c_int32, C.POINTER(C.c_uint64), C.POINTER(vp)], C.c_int),
     "geq_server_get_stats": ([vp, C.POINTER(geq_server_stats)], None),
     "geq_server_destroy": ([vp], None),
     "geq_lts_from_edges": ([C.c_uint64, u32p, u32p, i32p, C.POINTER(vp)], C.c_int),

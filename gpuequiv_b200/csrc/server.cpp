@@ -79,6 +79,7 @@ struct geq_server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::deque<Request *> queue;
+  std::deque<uint64_t> done_q;  // tickets in the order their requests finished
   std::unordered_map<uint64_t, std::unique_ptr<Request>> reqs;
   uint64_t next_ticket = 1;
   bool stop = false;
@@ -151,6 +152,7 @@ void finish(geq_server *s, const std::vector<Request *> &done) {
     std::lock_guard<std::mutex> lk(s->mu);
     for (Request *r : done) {
       r->state = 2;
+      s->done_q.push_back(r->ticket);
       if (r->st) s->stats.failed++;
       else s->stats.completed++;
     }
@@ -547,6 +549,34 @@ geq_status geq_server_poll(geq_server *s, uint64_t ticket, int32_t timeout_ms, g
   if (timeout_ms < 0) s->cv_done.wait(lk, done);
   else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), done))
     return fail(GEQ_ERR_TIMEOUT, "request %llu not finished", (unsigned long long)ticket);
+  const geq_status st = r->st;
+  if (st) set_last_error(r->err);
+  else *out = r->sol.release();
+  s->reqs.erase(it);
+  return st;
+}
+
+geq_status geq_server_poll_any(geq_server *s, int32_t timeout_ms, uint64_t *ticket, geq_solution **out) {
+  if (!s || !out || !ticket) return fail(GEQ_ERR_INVALID_INPUT, "NULL argument");
+  *out = nullptr;
+  *ticket = 0;
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    // tickets already taken by geq_server_poll are passed over
+    while (!s->done_q.empty() && !s->reqs.count(s->done_q.front())) s->done_q.pop_front();
+    if (!s->done_q.empty()) break;
+    auto ready = [&] { return !s->done_q.empty(); };
+    if (timeout_ms < 0) {
+      s->cv_done.wait(lk, ready);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
+      return fail(GEQ_ERR_TIMEOUT, "no request finished");
+    }
+  }
+  const uint64_t t = s->done_q.front();
+  s->done_q.pop_front();
+  auto it = s->reqs.find(t);
+  Request *r = it->second.get();
+  *ticket = t;
   const geq_status st = r->st;
   if (st) set_last_error(r->err);
   else *out = r->sol.release();

@@ -62,6 +62,27 @@ class Server:
         return (_borrow(po, no.value, C.c_uint64, np.uint64, owner),
                 _borrow(pd, nw.value, C.c_uint32, np.uint32, owner), _stats_of(sol))
 
+    def poll_any(self, timeout_ms: int = -1):
+        """(ticket, (offsets, data, stats)) of whichever request finished
+        first, or None if none finishes within timeout_ms (< 0: wait).  A
+        failed request raises GeqError (its ticket in ``.ticket``)."""
+        sol = C.c_void_p()
+        t = C.c_uint64()
+        st = lib.geq_server_poll_any(self.h, timeout_ms, C.byref(t), C.byref(sol))
+        if st == TIMEOUT and t.value == 0:
+            return None
+        try:
+            check(st)
+        except GeqError as e:
+            e.ticket = t.value
+            raise
+        owner = _SolutionOwner(sol)
+        po, pd = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+        no, nw = C.c_uint64(), C.c_uint64()
+        check(lib.geq_solution_flat(sol, C.byref(po), C.byref(no), C.byref(pd), C.byref(nw)))
+        return t.value, (_borrow(po, no.value, C.c_uint64, np.uint64, owner),
+                         _borrow(pd, nw.value, C.c_uint32, np.uint32, owner), _stats_of(sol))
+
     def stats(self) -> dict:
         st = geq_server_stats()
         lib.geq_server_get_stats(self.h, C.byref(st))

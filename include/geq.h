@@ -303,6 +303,12 @@ geq_status geq_server_submit_compare(geq_server *srv, const struct geq_lts *lts,
  * status: the request failed with that status (message in geq_last_error)
  * and the ticket is retired.  GEQ_ERR_INVALID_INPUT for an unknown ticket. */
 geq_status geq_server_poll(geq_server *srv, uint64_t ticket, int32_t timeout_ms, geq_solution **out);
+/* The same for whichever request finished first (a completion queue):
+ * waits up to timeout_ms (< 0: forever) for a finished request not yet
+ * polled, writes its ticket to *ticket and retires it; the status and *out
+ * are those geq_server_poll would give for that ticket.  GEQ_ERR_TIMEOUT
+ * (and *ticket = 0) when none finished in time. */
+geq_status geq_server_poll_any(geq_server *srv, int32_t timeout_ms, uint64_t *ticket, geq_solution **out);
 void geq_server_get_stats(geq_server *srv, geq_server_stats *out);
 /* Finishes the batches in flight, fails the queued requests, frees all. */
 void geq_server_destroy(geq_server *srv);

@@ -246,3 +246,25 @@ def test_requests_admitted_while_batches_run(geq, ctx):
     assert st["failed"] == 0 and st["completed"] == len(games)
     for i, (offs, data, _) in enumerate(got):
         assert _canon(offs, data) == expect[i], i
+
+
+def test_poll_any_returns_each_request_once(geq, ctx):
+    """The completion queue (geq_server_poll_any) hands out every request
+    exactly once, in the order they finish, with the lists of the game solved
+    alone; a ticket taken by geq_server_poll is not handed out again."""
+    from gpuequiv_b200.serving import Server
+    games = _games(geq, 60)
+    expect = [_alone(geq, ctx, g) for g in games]
+    with Server(ctx, n_pipelines=2, max_wait_us=300) as srv:
+        tickets = [srv.submit(g) for g in games]
+        first = srv.poll(tickets[0], timeout_ms=60_000)
+        got = {tickets[0]: _canon(first[0], first[1])}
+        while len(got) < len(games):
+            r = srv.poll_any(timeout_ms=60_000)
+            assert r is not None
+            t, (offs, data, _) = r
+            assert t not in got
+            got[t] = _canon(offs, data)
+        assert srv.poll_any(timeout_ms=0) is None
+    for i, t in enumerate(tickets):
+        assert got[t] == expect[i], i
