@@ -133,11 +133,21 @@ struct geq_solution {
   std::vector<uint32_t> data;
   geq::HostBuf off_buf, data_buf;
   uint64_t n_offsets = 0, n_words = 0;  // sizes when the HostBufs are used
+  // a view of one game of another solution (the serving loop's answers):
+  // its lists stay where they are, kept alive by `shared`
+  std::shared_ptr<const geq_solution> shared;
+  const uint64_t *view_off = nullptr;
+  const uint32_t *view_data = nullptr;
+  uint64_t view_noff = 0, view_nwords = 0;
   geq_solve_stats stats{};
-  const uint64_t *off_ptr() const { return off_buf.p ? (const uint64_t *)off_buf.p : offsets.data(); }
-  const uint32_t *data_ptr() const { return data_buf.p ? (const uint32_t *)data_buf.p : data.data(); }
-  uint64_t offsets_len() const { return off_buf.p ? n_offsets : offsets.size(); }
-  uint64_t data_len() const { return data_buf.p ? n_words : data.size(); }
+  const uint64_t *off_ptr() const {
+    return view_off ? view_off : off_buf.p ? (const uint64_t *)off_buf.p : offsets.data();
+  }
+  const uint32_t *data_ptr() const {
+    return view_off ? view_data : data_buf.p ? (const uint32_t *)data_buf.p : data.data();
+  }
+  uint64_t offsets_len() const { return view_off ? view_noff : off_buf.p ? n_offsets : offsets.size(); }
+  uint64_t data_len() const { return view_off ? view_nwords : data_buf.p ? n_words : data.size(); }
 };
 
 namespace geq {

@@ -88,22 +88,24 @@ struct geq_server {
 
 namespace {
 
-// One game of a batch solution as a solution of its own.
-std::unique_ptr<geq_solution> split_one(const geq_solution &all, uint32_t g) {
+// One game of a batch solution as a solution of its own that views the
+// batch's lists (no copy; the batch lives until its last view is freed).
+std::unique_ptr<geq_solution> view_one(const std::shared_ptr<const geq_solution> &all, uint32_t g) {
   std::unique_ptr<geq_solution> s(new geq_solution());
-  const uint32_t n = all.n_vertices[g];
-  const uint64_t *o = all.off_ptr() + all.offsets_base[g];
-  const uint64_t words = o[n];
-  s->energy_size = all.energy_size;
+  const uint32_t n = all->n_vertices[g], es = all->energy_size;
+  s->energy_size = es;
   s->n_vertices.assign(1, n);
   s->offsets_base.assign(1, 0);
   s->data_base.assign(1, 0);
-  s->offsets.assign(o, o + n + 1);
-  const uint32_t *d = all.data_ptr() + all.data_base[g] * all.energy_size;
-  s->data.assign(d, d + words * all.energy_size);
-  s->stats = all.stats;
+  s->view_off = all->off_ptr() + all->offsets_base[g];
+  s->view_noff = (uint64_t)n + 1;
+  s->view_data = all->data_ptr() + all->data_base[g] * es;
+  s->view_nwords = s->view_off[n] * es;
+  s->shared = all;
+  s->stats = all->stats;
   return s;
 }
+
 
 // Games of confs without a thermometer codec: the multi-word solver, one
 // request at a time.
@@ -174,8 +176,8 @@ geq_status retire(Engine &e, Session &ss, const std::vector<uint32_t> &games, st
     if (ss.req[g]) want.push_back(g);
   geq_solve_stats stt{};
   geq_status st = e.solve_stats(*ss.dg, &stt);
-  geq_solution part;
-  if (!st && !want.empty()) st = e.download_games(*ss.dg, want, ss.first_only, part);
+  std::shared_ptr<geq_solution> part = std::make_shared<geq_solution>();
+  if (!st && !want.empty()) st = e.download_games(*ss.dg, want, ss.first_only, *part);
   for (uint32_t g : games) {
     ss.retired[g] = 1;
     ss.live--;
@@ -185,10 +187,11 @@ geq_status retire(Engine &e, Session &ss, const std::vector<uint32_t> &games, st
     for (uint32_t g : want) fail_req(ss.req[g], st, msg, done);
     return st;
   }
-  part.stats = stt;
+  part->stats = stt;
+  const std::shared_ptr<const geq_solution> all = part;
   for (uint32_t i = 0; i < want.size(); i++) {
     Request *r = ss.req[want[i]];
-    r->sol = split_one(part, i);
+    r->sol = view_one(all, i);
     done.push_back(r);
   }
   return GEQ_OK;
