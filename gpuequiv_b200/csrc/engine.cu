@@ -2138,6 +2138,9 @@ struct DeviceGamesImpl {
     double round_ms = 0.0;
     std::chrono::steady_clock::time_point t_start{};
   } prog;
+  HostBuf hstep;            // page-locked: the control block and active flags read back by a step
+  uint8_t *d_act = nullptr; // active flags on the device
+  bool step_active = false;
 
   template <class T>
   bool alloc(T *&p, size_t n) {
@@ -2942,62 +2945,100 @@ geq_status Engine::download_games(DeviceGamesImpl &dg, const std::vector<uint32_
   return GEQ_OK;
 }
 
-geq_status Engine::solve_step(DeviceGamesImpl &dg, bool &done) {
+__global__ void k_active_games(const KParams p, const unsigned long long *node_base, uint32_t n_games,
+                               uint8_t *active);
+
+// One step in two halves: step_enqueue launches a CUDA graph of R rounds (or
+// one round as plain launches) and the read-back of the control block -- and,
+// with `active`, of the games that still have frontier positions -- into
+// page-locked memory of the upload, without waiting; step_finish, once the
+// stream has been synchronised, handles errors and arena compaction and
+// reports whether the frontier is empty.  Several uploads' steps can be
+// enqueued back to back and finished after one synchronisation.
+geq_status Engine::step_enqueue(DeviceGamesImpl &dg, bool active) {
   State &s = *st;
   cudaStream_t S = s.stream;
   DeviceGamesImpl::Progress &pr = dg.prog;
-  done = false;
   set_lane_limits(dg.kp, tuning);
   const bool profile = (tuning.flags & GEQ_TUNE_PROFILE) != 0;
   const bool use_graph = !(tuning.flags & (GEQ_TUNE_NO_GRAPH | GEQ_TUNE_PROFILE));
   const uint32_t R = use_graph ? std::max<uint32_t>(1, tuning.rounds_per_graph) : 1;
+  const size_t hbytes = sizeof(Ctr) + dg.n_games;
+  if (!dg.hstep.p && !dg.hstep.alloc(s.hpool, hbytes)) return fail(GEQ_ERR_OUT_OF_MEMORY, "step read-back");
+  if (use_graph) {
+    // the shared graph is pointed at this upload's parameters when they differ
+    cudaGraphExec_t gexec = nullptr;
+    geq_status g = round_graph(*this, dg.kp, dg.generic, R, gexec);
+    if (g) return g;
+    CU(cudaGraphLaunch(gexec, S));
+  } else {
+    cudaEvent_t ea = profile ? s.eva : nullptr, eb = profile ? s.evb : nullptr;
+    if (dg.generic) launch_round<CodecGen>(*this, dg.kp, S, ea, eb);
+    else launch_round<CodecStd>(*this, dg.kp, S, ea, eb);
+  }
+  pr.launches += 4ull * R;
+  CU(cudaMemcpyAsync(dg.hstep.p, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
+  dg.step_active = active && dg.n_games > 0;
+  if (dg.step_active) {
+    if (!dg.d_act && !dg.alloc(dg.d_act, dg.n_games)) return fail(GEQ_ERR_OUT_OF_MEMORY, "active flags");
+    CU(cudaMemsetAsync(dg.d_act, 0, dg.n_games, S));
+    k_active_games<<<(unsigned)std::max(1, n_sms * 4), 256, 0, S>>>(dg.kp, dg.d_node_base, dg.n_games, dg.d_act);
+    CU(cudaMemcpyAsync((char *)dg.hstep.p + sizeof(Ctr), dg.d_act, dg.n_games, cudaMemcpyDeviceToHost, S));
+  }
+  CU(cudaGetLastError());
+  return GEQ_OK;
+}
+
+geq_status Engine::step_finish(DeviceGamesImpl &dg, bool &done, const uint8_t *&active) {
+  State &s = *st;
+  DeviceGamesImpl::Progress &pr = dg.prog;
+  done = false;
+  active = nullptr;
+  const Ctr c = *(const Ctr *)dg.hstep.p;
+  if (tuning.flags & GEQ_TUNE_PROFILE) {
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, s.eva, s.evb));
+    pr.round_ms += ms;
+    pr.round_launches++;
+  }
+  if (c.error) {
+    const char *what = (c.error & DERR_BOUNDS) ? "index out of range" :
+                       (c.error & DERR_LIST) ? "energy list too long" : "combination too large";
+    return fail((c.error & DERR_BOUNDS) ? GEQ_ERR_INTERNAL : GEQ_ERR_OUT_OF_MEMORY,
+                "device error %u (%s, line %u)", c.error, what, c.err_line);
+  }
+  if (c.overflow || c.arena_top > c.arena_cap - c.arena_cap / 4) {
+    geq_status a = compact(*this, dg, pr.launches);
+    if (a) return a;
+    pr.compactions++;
+    if (c.overflow) return GEQ_OK;  // the halted rounds run at the next step; nothing retires now
+  }
+  if (c.fsize[c.cur] == 0) {
+    done = true;
+    dg.next_stamp = c.stamp + 2u;
+    return GEQ_OK;
+  }
   // The device work of every launch is bounded; this bounds the host loop in
   // case the frontier never empties (GEQ_SOLVE_TIMEOUT_S seconds, default 600).
   const char *lim_env = std::getenv("GEQ_SOLVE_TIMEOUT_S");
   const double limit_s = lim_env ? std::atof(lim_env) : 600.0;
-  for (;;) {
-    if (use_graph) {
-      // the shared graph is pointed at this upload's parameters every step
-      cudaGraphExec_t gexec = nullptr;
-      geq_status g = round_graph(*this, dg.kp, dg.generic, R, gexec);
-      if (g) return g;
-      CU(cudaGraphLaunch(gexec, S));
-    } else {
-      cudaEvent_t ea = profile ? s.eva : nullptr, eb = profile ? s.evb : nullptr;
-      if (dg.generic) launch_round<CodecGen>(*this, dg.kp, S, ea, eb);
-      else launch_round<CodecStd>(*this, dg.kp, S, ea, eb);
-    }
-    pr.launches += 4ull * R;
-    CU(cudaMemcpyAsync(s.h_ctr, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
-    CU(cudaStreamSynchronize(S));
-    const Ctr c = *s.h_ctr;
-    if (profile) {
-      float ms = 0.f;
-      CU(cudaEventElapsedTime(&ms, s.eva, s.evb));
-      pr.round_ms += ms;
-      pr.round_launches++;
-    }
-    if (c.error) {
-      const char *what = (c.error & DERR_BOUNDS) ? "index out of range" :
-                         (c.error & DERR_LIST) ? "energy list too long" : "combination too large";
-      return fail((c.error & DERR_BOUNDS) ? GEQ_ERR_INTERNAL : GEQ_ERR_OUT_OF_MEMORY,
-                  "device error %u (%s, line %u)", c.error, what, c.err_line);
-    }
-    if (c.overflow || c.arena_top > c.arena_cap - c.arena_cap / 4) {
-      geq_status a = compact(*this, dg, pr.launches);
-      if (a) return a;
-      pr.compactions++;
-      if (c.overflow) continue;  // the halted rounds run again
-    }
-    if (c.fsize[c.cur] == 0) {
-      done = true;
-      dg.next_stamp = c.stamp + 2u;
-      return GEQ_OK;
-    }
-    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - pr.t_start).count();
-    if (el > limit_s) return fail(GEQ_ERR_TIMEOUT, "no fixpoint after %llu rounds (%.0f s)", c.rounds, el);
-    return GEQ_OK;
-  }
+  const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - pr.t_start).count();
+  if (el > limit_s) return fail(GEQ_ERR_TIMEOUT, "no fixpoint after %llu rounds (%.0f s)", c.rounds, el);
+  if (dg.step_active) active = (const uint8_t *)dg.hstep.p + sizeof(Ctr);
+  return GEQ_OK;
+}
+
+geq_status Engine::sync() {
+  CU(cudaStreamSynchronize(st->stream));
+  return GEQ_OK;
+}
+
+geq_status Engine::solve_step(DeviceGamesImpl &dg, bool &done) {
+  geq_status r = step_enqueue(dg, false);
+  if (!r) r = sync();
+  const uint8_t *active = nullptr;
+  if (!r) r = step_finish(dg, done, active);
+  return r;
 }
 
 geq_status Engine::solve_stats(DeviceGamesImpl &dg, geq_solve_stats *stats) {

@@ -198,6 +198,12 @@ class Engine {
   // rounds per step (done: the frontier is empty); counters of the solve so far
   geq_status solve_begin(DeviceGamesImpl &dg);
   geq_status solve_step(DeviceGamesImpl &dg, bool &done);
+  // one step in two halves around a synchronisation of the engine's stream
+  // (several uploads' steps back to back): with `active`, the games that
+  // still have frontier positions are read back too (null when unknown)
+  geq_status step_enqueue(DeviceGamesImpl &dg, bool active);
+  geq_status step_finish(DeviceGamesImpl &dg, bool &done, const uint8_t *&active);
+  geq_status sync();
   geq_status solve_stats(DeviceGamesImpl &dg, geq_solve_stats *stats);
   // active[g] = 1 while game g has a position in the frontier
   geq_status active_games(DeviceGamesImpl &dg, std::vector<uint8_t> &active);

@@ -314,23 +314,21 @@ void start_compares(Engine &e, int device, uint64_t max_positions, std::vector<R
   out.push_back(std::move(ss));
 }
 
-// One step of a session, then the games that reached their fixpoint retire.
-// false: the session is finished (or failed) and can be dropped.
 double ms_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
-bool step_session(Engine &e, Session &ss, std::vector<Request *> &done, double &retire_ms) {
+// The second half of a session's step (its graph of rounds was enqueued and
+// the stream synchronised): the games that reached their fixpoint retire.
+// false: the session is finished (or failed) and can be dropped.
+bool finish_session(Engine &e, Session &ss, geq_status enq, std::vector<Request *> &done, double &retire_ms) {
   bool fin = false;
-  geq_status st = e.solve_step(*ss.dg, fin);
+  const uint8_t *active = nullptr;
+  geq_status st = enq ? enq : e.step_finish(*ss.dg, fin, active);
   std::vector<uint32_t> ret;
-  if (!st) {
-    std::vector<uint8_t> active;
-    if (!fin) st = e.active_games(*ss.dg, active);
-    if (!st)
-      for (uint32_t g = 0; g < ss.retired.size(); g++)
-        if (!ss.retired[g] && (fin || !active[g])) ret.push_back(g);
-  }
+  if (!st && (fin || active))
+    for (uint32_t g = 0; g < ss.retired.size(); g++)
+      if (!ss.retired[g] && (fin || !active[g])) ret.push_back(g);
   if (st) {
     const std::string msg = geq_last_error();
     for (uint32_t g = 0; g < ss.retired.size(); g++)
@@ -347,6 +345,23 @@ bool step_session(Engine &e, Session &ss, std::vector<Request *> &done, double &
     retire_ms += ms_since(t0);
   }
   return ss.live > 0;
+}
+
+// One step of every resident session: all graphs enqueued back to back on the
+// pipeline's stream, one synchronisation, then each session's retirements.
+void step_sessions(Engine &e, std::vector<std::unique_ptr<Session>> &active, uint64_t &used,
+                   std::vector<Request *> &done, double &retire_ms) {
+  std::vector<geq_status> enq(active.size(), GEQ_OK);
+  for (size_t k = 0; k < active.size(); k++) enq[k] = e.step_enqueue(*active[k]->dg, true);
+  const geq_status sy = e.sync();
+  for (size_t k = 0, j = 0; k < active.size(); j++) {
+    if (finish_session(e, *active[k], sy ? sy : enq[j], done, retire_ms)) {
+      k++;
+    } else {
+      used -= std::min(used, active[k]->footprint);
+      active.erase(active.begin() + k);
+    }
+  }
 }
 
 void pipeline(geq_server *s, Engine *e) {
@@ -417,14 +432,7 @@ void pipeline(geq_server *s, Engine *e) {
     }
     // one step of every resident session
     const auto t1 = std::chrono::steady_clock::now();
-    for (size_t k = 0; k < active.size();) {
-      if (step_session(*e, *active[k], done, retire_ms)) {
-        k++;
-      } else {
-        used -= std::min(used, active[k]->footprint);
-        active.erase(active.begin() + k);
-      }
-    }
+    if (!active.empty()) step_sessions(*e, active, used, done, retire_ms);
     step_ms = ms_since(t1) - retire_ms;
     {
       std::lock_guard<std::mutex> lk(s->mu);
@@ -435,11 +443,10 @@ void pipeline(geq_server *s, Engine *e) {
     finish(s, done);
   }
   // stopped: the sessions in flight finish
-  for (auto &ss : active) {
+  while (!active.empty()) {
     std::vector<Request *> done;
     double retire_ms = 0;
-    while (step_session(*e, *ss, done, retire_ms)) {
-    }
+    step_sessions(*e, active, used, done, retire_ms);
     finish(s, done);
   }
 }
