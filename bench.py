@@ -39,6 +39,14 @@ UNIT = "games/s"
 FALLBACK_HBM_GBS = 6650.0
 
 
+_T0 = time.perf_counter()
+
+
+def progress(msg: str) -> None:
+    """One line of progress on stderr (the JSON result line goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -51,7 +59,7 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch shape)")
     ap.add_argument("--serve-rates", default="5000,10000",
                     help="Poisson arrival rates (req/s) of the game-request serving leg; empty: none")
-    ap.add_argument("--query-rates", default="200,1000,5000",
+    ap.add_argument("--query-rates", default="200,1000",
                     help="Poisson arrival rates (req/s) of the serving configuration (equivalence queries on LTSs "
                          "of 20-20,000 states); empty: none")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrivals per serving rate (s)")
@@ -301,9 +309,10 @@ class Load:
     slow request does not hold back the recording of others.  Latency =
     submit -> the request's solution in the caller's hands."""
 
-    def __init__(self, srv, items, queries: bool, threads: int = 4):
+    def __init__(self, srv, items, queries: bool, threads: int = 4, drain_s: float = 60.0):
         from gpuequiv_b200._lib import lib
         self.lib, self.h, self.items, self.queries, self.threads = lib, srv.h, items, queries, threads
+        self.drain_s = drain_s  # after the last arrival, wait this long for the rest
 
     def _submit(self, item):
         import ctypes as C
@@ -329,9 +338,10 @@ class Load:
             self.lib.geq_solution_free(sol)
         return t.value, st
 
-    def _pollers(self, total_fn, done):
+    def _pollers(self, total_fn, done, deadline):
         """Poller threads appending (ticket, time, status) to `done` until
-        total_fn() requests have finished (total_fn None: not known yet)."""
+        total_fn() requests have finished (total_fn None: not known yet) or
+        deadline[0] (set once the last request is submitted) has passed."""
         import threading
 
         def poller():
@@ -339,11 +349,13 @@ class Load:
                 n = total_fn()
                 if n is not None and len(done) >= n:
                     return
+                if deadline[0] is not None and time.perf_counter() > deadline[0]:
+                    return
                 r = self._poll_any(50)
                 if r is not None:
                     done.append((r[0], time.perf_counter(), r[1]))
 
-        th = [threading.Thread(target=poller) for _ in range(max(1, self.threads // 2))]
+        th = [threading.Thread(target=poller, daemon=True) for _ in range(max(1, self.threads // 2))]
         for x in th:
             x.start()
         return th
@@ -367,13 +379,24 @@ class Load:
         th = [threading.Thread(target=submitter, args=(k,)) for k in range(self.threads)]
         for x in th:
             x.start()
-        pol = self._pollers(lambda: n, done)
-        for x in th + pol:
+        deadline = [None]
+        pol = self._pollers(lambda: n, done, deadline)
+        for x in th:
             x.join()
+        deadline[0] = time.perf_counter() + self.drain_s
+        for x in pol:
+            x.join()
+        return self._result(subs, done, t0)
+
+    @staticmethod
+    def _result(subs, done, t0):
+        """Latencies and statuses of the finished requests; the ones still
+        unfinished at the deadline count with status -1."""
         sub = dict(subs)
-        lat = np.array([(td - sub[t]) * 1e3 for t, td, _ in done])
-        status = np.array([st for _, _, st in done], np.int32)
-        t_end = max(td for _, td, _ in done)
+        fin = {t for t, _, _ in done}
+        lat = np.array([(td - sub[t]) * 1e3 for t, td, _ in done if t in sub])
+        status = np.array([st for t, _, st in done if t in sub] + [-1] * sum(1 for t in sub if t not in fin), np.int32)
+        t_end = max([td for _, td, _ in done] or [t0])
         return lat, status, t_end - t0
 
     def closed_loop(self, pick, outstanding: int, seconds: float):
@@ -409,27 +432,28 @@ class Load:
             x.start()
         rel.start()
         total = [None]
-        pol = self._pollers(lambda: total[0], done)
+        deadline = [None]
+        pol = self._pollers(lambda: total[0], done, deadline)
         for x in th:
             x.join()
         total[0] = len(subs)
+        deadline[0] = time.perf_counter() + self.drain_s
         for x in pol:
             x.join()
         stop[0] = True
         rel.join()
-        sub = dict(subs)
-        lat = np.array([(td - sub[t]) * 1e3 for t, td, _ in done])
-        status = np.array([st for _, _, st in done], np.int32)
-        span = max(td for _, td, _ in done) - t0
-        return lat, status, span
+        return self._result(subs, done, t0)
 
 
 def _lat_summary(lat_ms, status, span_s):
+    fin = status >= 0
     ok = status == 0
     refused = int((status == 2).sum())  # GEQ_ERR_OUT_OF_MEMORY: the game exceeds the position bound
-    failed = int((~ok).sum()) - refused
-    l = lat_ms[ok] if ok.any() else np.zeros(1)
+    unfinished = int((~fin).sum())      # still running when the drain deadline passed
+    failed = int(fin.sum() - ok.sum()) - refused
+    l = lat_ms[ok[:len(lat_ms)]] if ok.any() else np.zeros(1)
     return {"requests": int(len(status)), "served": int(ok.sum()), "refused": refused, "failed": failed,
+            "unfinished_at_deadline": unfinished,
             "refusal_rate": refused / max(1, len(status)), "seconds": round(float(span_s), 3),
             "throughput_games_s": float(ok.sum() / span_s) if span_s > 0 else None,
             "p50_ms": float(np.percentile(l, 50)), "p99_ms": float(np.percentile(l, 99)), "mean_ms": float(l.mean())}
@@ -453,6 +477,7 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
             n = max(1, int(rng.poisson(lam * seconds)))
             arrivals = np.sort(rng.uniform(0, seconds, n))
             pick = rng.integers(0, len(items), n)
+            progress(f"  open loop {lam:.0f} req/s, {n} requests")
             st0 = srv.stats()
             lat, status, span = load.open_loop(arrivals, pick)
             st = srv.stats()
@@ -464,6 +489,7 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
             out["runs"].append(r)
         if saturation_s > 0:
             pick = np.arange(len(items))
+            progress(f"  closed loop, {outstanding} in flight")
             st0 = srv.stats()
             lat, status, span = load.closed_loop(pick, outstanding, saturation_s)
             st = srv.stats()
@@ -742,6 +768,7 @@ def run_ours(args, d: Dist):
     in_bytes = sum(g.row_offsets.nbytes + g.column_indices.nbytes + g.weights.array.nbytes + g.attacker_pos.nbytes
                    for g in graphs)
 
+    progress("resident solve")
     # ---- value: games resident in HBM ----
     dg = geq.DeviceGames(graphs, ctx)
     tune = None
@@ -778,6 +805,7 @@ def run_ours(args, d: Dist):
     res_offs, res_data = dg.download_raw()
     b_min = sum(geq.b_min(g, o) for g, o in zip(graphs, res_offs))
 
+    progress("roofline")
     # ---- roofline of the round kernel (one profiled solve, not timed) ----
     ctx.set_tuning(flags=TUNE_PROFILE)
     st_prof = dg.solve()
@@ -790,6 +818,7 @@ def run_ours(args, d: Dist):
     alg_per_launch = st_prof["algorithmic_bytes"] / k_launch
     traffic = DRAM_PER_ALGORITHMIC_BYTE * alg_per_launch
 
+    progress("e2e")
     # ---- e2e: host buffers through the C ABI (geq_energy_game_run_batch) ----
     views = geq.c_views(graphs)
     for _ in range(max(1, args.warmup // 2)):
@@ -805,10 +834,12 @@ def run_ours(args, d: Dist):
     e2e_s = d.max(float(np.median(e2e_t)))
     e2e = total_games / e2e_s
 
+    progress("lts pipeline")
     # ---- LTS -> verdict: compare_batch from the unminimised LTSs (host
     # minimisation, games built on the device, solved, start energies back) ----
     lts_jobs, lts_pipe = run_lts_pipeline(ctx, seeds, graphs, args, d)
 
+    progress("plain")
     # ---- plain CUDA: one call per game (sample) ----
     idx = sample_indices(len(graphs), args.plain_sample)
     pviews = [geq.c_views([graphs[i]]) for i in idx]
@@ -820,6 +851,7 @@ def run_ours(args, d: Dist):
     plain_s = time.perf_counter() - t
     plain_rate = len(idx) / plain_s  # every k-th job: the batch's size mix
 
+    progress("serving")
     # ---- serving loop (not part of value) ----
     # game requests drawn from this batch: Poisson arrivals, then saturation
     rates = [float(x) for x in args.serve_rates.split(",") if x.strip()]
@@ -836,9 +868,10 @@ def run_ours(args, d: Dist):
     serving_q = None
     if qrates or args.saturation_seconds > 0:
         pool = serving_queries(args.query_pool, seed=7 + 1000 * d.rank)
+        progress("serving: queries")
         serving_q = run_serving(ctx, pool, True, qrates, args.serve_seconds, 200 + 1000 * d.rank,
                                 args.saturation_seconds, max_game_positions=args.query_bound,
-                                outstanding=2048)
+                                outstanding=256)
         # the plain form on the same distribution: one compare() call per
         # query, for queries whose game is within the bound
         acc = [j for j in pool[::max(1, len(pool) // 96)][:96] if within_bound(j, args.query_bound)][:64]
@@ -853,10 +886,12 @@ def run_ours(args, d: Dist):
         sat = serving_q["saturation"]
         serving_q["saturation_vs_plain"] = (sat["throughput_games_s"] / plain_q) if sat and plain_q else None
 
+    progress("small + large")
     # ---- small configuration: equivalences() of 100 seeded 40-state LTSs ----
     small = run_small(ctx, list(range(100)), check=d.rank == 0)
     large = run_large(ctx, args.large_states, check=d.rank == 0) if args.large_states else None
 
+    progress("stress")
     # ---- stress configuration: one 2M-position / 10M-edge game, resident ----
     stress = None
     if args.stress:
@@ -888,6 +923,7 @@ def run_ours(args, d: Dist):
                                "round_kernel_launches": s_prof["round_kernel_launches"],
                                "b_min": s_bmin, "b_min_over_algorithmic_bytes": s_bmin / s_prof["algorithmic_bytes"]}}
 
+    progress("cpu baseline")
     # ---- CPU baseline: the oracle on one host thread (rank 0, N=1), on every
     # 16th job; its lists are the check of the timed solve's lists ----
     cpu, parity = None, None
@@ -951,7 +987,7 @@ def run_ours(args, d: Dist):
                                                 f"on seeded LTSs of log-uniform 20-20,000 states (pool of "
                                                 f"{args.query_pool}), geq_server_submit_compare (minimisation, "
                                                 f"GameBuild, solve on the device), games above "
-                                                f"{args.query_bound} positions refused; then a closed loop of 2048 "
+                                                f"{args.query_bound} positions refused; then a closed loop of 256 "
                                                 f"queries in flight", **(serving_q or {})}},
             "gpu_launches": int(launches),
             "clocks": ck,

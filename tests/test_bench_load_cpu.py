@@ -56,7 +56,16 @@ class FakeLib:
 def make_load(delay):
     load = bench.Load.__new__(bench.Load)
     load.lib, load.h, load.items, load.queries, load.threads = FakeLib(delay), None, [C.c_int(0)] * 4, False, 4
+    load.drain_s = 10.0
     return load
+
+
+def test_unfinished_requests_count_at_the_deadline():
+    load = make_load(lambda k: 30.0 if k == 3 else 0.001)  # request 3 never finishes in time
+    load.drain_s = 0.3
+    lat, status, span = load.open_loop(np.linspace(0, 0.05, 20), np.zeros(20, np.int64))
+    assert len(status) == 20 and (status == -1).sum() == 1 and len(lat) == 19
+    assert span < 5
 
 
 def test_open_loop_collects_every_request_once():
