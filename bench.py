@@ -460,9 +460,10 @@ def _lat_summary(lat_ms, status, span_s):
 
 
 def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, saturation_s: float,
-                max_game_positions: int = 0, outstanding: int = 8192) -> dict:
+                max_game_positions: int = 0, outstanding: int = 8192, saturation_items=None) -> dict:
     """One server: open-loop Poisson arrivals at each rate, then a closed-loop
-    saturation run (`outstanding` requests kept in flight)."""
+    saturation run (`outstanding` requests kept in flight) over
+    `saturation_items` (default: all items)."""
     from gpuequiv_b200.serving import Server
     rng = np.random.default_rng(seed)
     out = {"runs": [], "saturation": None}
@@ -488,7 +489,7 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
                       "pipeline_thread_ms": {k: round(st[k] - st0[k], 1) for k in ("admit_ms", "step_ms", "retire_ms")}})
             out["runs"].append(r)
         if saturation_s > 0:
-            pick = np.arange(len(items))
+            pick = np.arange(len(items)) if saturation_items is None else np.asarray(saturation_items, np.int64)
             progress(f"  closed loop, {outstanding} in flight")
             st0 = srv.stats()
             lat, status, span = load.closed_loop(pick, outstanding, saturation_s)
@@ -868,13 +869,16 @@ def run_ours(args, d: Dist):
     serving_q = None
     if qrates or args.saturation_seconds > 0:
         pool = serving_queries(args.query_pool, seed=7 + 1000 * d.rank)
+        # the queries whose game is within the bound (host GameBuild with the
+        # bound, on the first 256 of the pool): the saturation run and the
+        # plain form both take these, so that they compare like with like
+        acc_idx = [i for i in range(min(256, len(pool))) if within_bound(pool[i], args.query_bound)]
         progress("serving: queries")
         serving_q = run_serving(ctx, pool, True, qrates, args.serve_seconds, 200 + 1000 * d.rank,
                                 args.saturation_seconds, max_game_positions=args.query_bound,
-                                outstanding=256)
-        # the plain form on the same distribution: one compare() call per
-        # query, for queries whose game is within the bound
-        acc = [j for j in pool[::max(1, len(pool) // 96)][:96] if within_bound(j, args.query_bound)][:64]
+                                outstanding=256, saturation_items=acc_idx)
+        # the plain form on the same queries: one compare() call each
+        acc = [pool[i] for i in acc_idx[:64]]
         for j in acc[:8]:
             geq.compare_batch([j], context=ctx)
         t = time.perf_counter()
@@ -883,6 +887,7 @@ def run_ours(args, d: Dist):
         plain_q = len(acc) / (time.perf_counter() - t) if acc else None
         serving_q["plain_per_query"] = {"value": plain_q, "unit": UNIT,
                                         "sample": f"{len(acc)} pool queries within the bound, one compare() each"}
+        serving_q["saturation_queries"] = f"the {len(acc_idx)} of the first 256 pool queries within the bound"
         sat = serving_q["saturation"]
         serving_q["saturation_vs_plain"] = (sat["throughput_games_s"] / plain_q) if sat and plain_q else None
 
