@@ -347,14 +347,21 @@ bool finish_session(Engine &e, Session &ss, geq_status enq, std::vector<Request 
   return ss.live > 0;
 }
 
-// One step of every resident session: all graphs enqueued back to back on the
-// pipeline's stream, one synchronisation, then each session's retirements.
-void step_sessions(Engine &e, std::vector<std::unique_ptr<Session>> &active, uint64_t &used,
-                   std::vector<Request *> &done, double &retire_ms) {
+// One step of every resident session, in two halves: enqueue_steps puts all
+// their graphs back to back on the pipeline's stream; finish_steps
+// synchronises once and retires, for the first n sessions (sessions admitted
+// in between are appended behind them and step from the next turn).
+std::vector<geq_status> enqueue_steps(Engine &e, std::vector<std::unique_ptr<Session>> &active) {
   std::vector<geq_status> enq(active.size(), GEQ_OK);
   for (size_t k = 0; k < active.size(); k++) enq[k] = e.step_enqueue(*active[k]->dg, true);
+  return enq;
+}
+void finish_steps(Engine &e, std::vector<std::unique_ptr<Session>> &active, size_t n,
+                  const std::vector<geq_status> &enq, uint64_t &used, std::vector<Request *> &done,
+                  double &retire_ms) {
+  if (!n) return;
   const geq_status sy = e.sync();
-  for (size_t k = 0, j = 0; k < active.size(); j++) {
+  for (size_t k = 0, j = 0; j < n; j++) {
     if (finish_session(e, *active[k], sy ? sy : enq[j], done, retire_ms)) {
       k++;
     } else {
@@ -405,6 +412,12 @@ void pipeline(geq_server *s, Engine *e) {
     }
     std::vector<Request *> done;
     double admit_ms = 0, step_ms = 0, retire_ms = 0;
+    // the resident sessions' next step goes to the device first; the new
+    // batch is staged on the host and uploaded behind it on the same stream,
+    // so its packing overlaps their rounds
+    const auto t1 = std::chrono::steady_clock::now();
+    const size_t n_old = active.size();
+    const std::vector<geq_status> enq = enqueue_steps(*e, active);
     if (!batch.empty()) {
       const auto t0 = std::chrono::steady_clock::now();
       std::vector<Request *> games, compares, wide;
@@ -430,10 +443,8 @@ void pipeline(geq_server *s, Engine *e) {
       }
       admit_ms = ms_since(t0);
     }
-    // one step of every resident session
-    const auto t1 = std::chrono::steady_clock::now();
-    if (!active.empty()) step_sessions(*e, active, used, done, retire_ms);
-    step_ms = ms_since(t1) - retire_ms;
+    finish_steps(*e, active, n_old, enq, used, done, retire_ms);
+    step_ms = ms_since(t1) - retire_ms - admit_ms;
     {
       std::lock_guard<std::mutex> lk(s->mu);
       s->stats.admit_ms += admit_ms;
@@ -446,7 +457,8 @@ void pipeline(geq_server *s, Engine *e) {
   while (!active.empty()) {
     std::vector<Request *> done;
     double retire_ms = 0;
-    step_sessions(*e, active, used, done, retire_ms);
+    const std::vector<geq_status> enq = enqueue_steps(*e, active);
+    finish_steps(*e, active, active.size(), enq, used, done, retire_ms);
     finish(s, done);
   }
 }

@@ -278,8 +278,9 @@ typedef struct geq_server_stats {
   uint64_t games_in_batches;     /* sum of batch sizes */
   uint64_t max_batch_footprint;  /* bytes, largest resident footprint estimate */
   double admit_ms;               /* pipeline threads' wall time: staging, upload (and
-                                    minimisation + GameBuild of queries) of batches */
-  double step_ms;                /* ... rounds of resident batches */
+                                    minimisation + GameBuild of queries) of batches,
+                                    which queue behind the resident batches' rounds */
+  double step_ms;                /* ... rounds of resident batches (the rest of them) */
   double retire_ms;              /* ... reading back and answering finished games */
 } geq_server_stats;
 /* The server solves on the device of `ctx` and copies its tuning; ctx may be
