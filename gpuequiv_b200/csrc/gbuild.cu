@@ -115,9 +115,9 @@ __global__ void __launch_bounds__(SCAN_T) k_scan_down(const uint32_t *in, uint32
 // Single-pass scans of up to three arrays, each with its item count read on
 // the device (chained scan with decoupled look-back): block b scans tiles b,
 // b + G, b + 2G, ... of SCAN_TILE values.  A tile publishes its sum at once,
-// then looks back over the tiles before it -- adding published sums until it
-// meets a published inclusive prefix -- and publishes its own inclusive
-// prefix.  The status words carry the scan's sequence number (bumped by the
+// then looks back over the tiles before it -- one warp reading the status
+// words of 32 tiles at a time, adding published sums until it meets a
+// published inclusive prefix -- and publishes its own inclusive prefix.  The status words carry the scan's sequence number (bumped by the
 // last block of every launch), so no clearing is needed between launches.
 // The look-back waits are bounded: a tile that gives up sums its
 // predecessors' inputs itself, so the result never depends on how the blocks
@@ -133,6 +133,7 @@ struct LbCtl {
 };
 constexpr uint32_t LB_AGG = 1u, LB_INC = 2u;
 constexpr uint32_t LB_SPIN_LIMIT = 1u << 16;
+constexpr uint32_t LB_FULL = 0xffffffffu;
 
 __device__ __forceinline__ uint32_t ld_vol(const uint32_t *p) { return *(const volatile uint32_t *)p; }
 __device__ __forceinline__ unsigned long long ld_vol(const unsigned long long *p) {
@@ -167,23 +168,37 @@ __global__ void __launch_bounds__(SCAN_T) k_lbscan(ScanR a, const unsigned long 
       }
       unsigned long long total;
       unsigned long long e = block_scan(s, total);
-      if (threadIdx.x == 0) {
+      if (threadIdx.x < 32) {
+        // warp 0 looks back 32 tiles at a time: lane k reads tile hi - k
+        const uint32_t lane = threadIdx.x;
         unsigned long long prefix = 0;
         uint32_t gaveup = 0;
         if (!status) {
           gaveup = 1;
         } else if (t == 0) {
-          ic[0] = total;
-          __threadfence();
-          *(volatile uint32_t *)&fl[0] = tag | LB_INC;
+          if (lane == 0) {
+            ic[0] = total;
+            __threadfence();
+            *(volatile uint32_t *)&fl[0] = tag | LB_INC;
+          }
         } else {
-          ag[t] = total;
-          __threadfence();
-          *(volatile uint32_t *)&fl[t] = tag | LB_AGG;
-          uint32_t j = t - 1, spins = 0;
+          if (lane == 0) {
+            ag[t] = total;
+            __threadfence();
+            *(volatile uint32_t *)&fl[t] = tag | LB_AGG;
+          }
+          long long hi = (long long)t - 1;
+          uint32_t spins = 0;
           for (;;) {
-            const uint32_t f = ld_vol(&fl[j]);
-            if ((f & ~3u) != tag || (f & 3u) == 0u) {
+            const long long j = hi - (long long)lane;
+            const uint32_t f = j >= 0 ? ld_vol(&fl[j]) : 0u;
+            const bool ready = j >= 0 && (f & ~3u) == tag && (f & 3u) != 0u;
+            const uint32_t incm = __ballot_sync(LB_FULL, ready && (f & 3u) == LB_INC);
+            const uint32_t waitm = __ballot_sync(LB_FULL, j >= 0 && !ready);
+            // tiles hi .. the nearest inclusive prefix (or the whole window)
+            // must all have published; tile 0 always publishes an inclusive one
+            const uint32_t need = incm ? ((incm & (0u - incm)) << 1) - 1u : LB_FULL;
+            if (waitm & need) {
               if (++spins > LB_SPIN_LIMIT) {
                 gaveup = 1;
                 break;
@@ -192,16 +207,20 @@ __global__ void __launch_bounds__(SCAN_T) k_lbscan(ScanR a, const unsigned long 
               continue;
             }
             __threadfence();
-            if ((f & 3u) == LB_INC) {
-              prefix += ld_vol(&ic[j]);
-              break;
-            }
-            prefix += ld_vol(&ag[j]);
-            j--;  // tile 0 always publishes an inclusive prefix
+            const bool mine = ((need >> lane) & 1u) != 0u && j >= 0;
+            unsigned long long x = 0;
+            if (mine) x = ((f & 3u) == LB_INC) ? ld_vol(&ic[j]) : ld_vol(&ag[j]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(LB_FULL, x, o);
+            prefix += x;
+            if (incm) break;
+            hi -= 32;
           }
         }
-        s_prefix = prefix;
-        s_gaveup = gaveup;
+        if (lane == 0) {
+          s_prefix = prefix;
+          s_gaveup = gaveup;
+        }
       }
       __syncthreads();
       if (s_gaveup) {
