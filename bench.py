@@ -288,7 +288,7 @@ def workload_config(rows, world: int) -> dict:
 # ncu capture of the 1,024-job batch (--solve-only --jobs 1024), divided by
 # the algorithmic bytes those launches counted.  Traffic grows with the work
 # of a launch, so the full-size figure is this ratio x its algorithmic bytes.
-DRAM_PER_ALGORITHMIC_BYTE = 1.77
+DRAM_PER_ALGORITHMIC_BYTE = 1.61
 
 
 def peak_hbm():
