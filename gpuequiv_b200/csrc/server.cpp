@@ -56,8 +56,13 @@ struct Request {
   uint32_t p = 0, q = 0;
   geq_energy_conf conf{};
   uint32_t n = 0;
-  std::vector<uint32_t> row, col, wt, reach;
-  std::vector<uint8_t> att;
+  // a game's copy: row | col | wt | attacker bytes | reach in one block that
+  // is handed back to the server's pool when the request is answered
+  std::unique_ptr<uint32_t[]> buf;
+  size_t buf_words = 0;
+  const uint32_t *row = nullptr, *col = nullptr, *wt = nullptr, *reach = nullptr;
+  const uint8_t *att = nullptr;
+  uint32_t n_reach = 0;
   uint64_t footprint = 0;
   int state = 0;  // 0 queued, 1 running, 2 done
   geq_status st = GEQ_OK;
@@ -84,9 +89,47 @@ struct geq_server {
   uint64_t next_ticket = 1;
   bool stop = false;
   geq_server_stats stats{};
+  // input blocks of answered requests, reused by submit: a fresh block of a
+  // few hundred KB costs page faults on every request (and unmapping it
+  // costs every thread of the process a TLB flush)
+  std::mutex pool_mu;
+  std::vector<std::pair<std::unique_ptr<uint32_t[]>, size_t>> free_bufs;
+  uint64_t free_words = 0;
 };
 
 namespace {
+
+constexpr uint64_t POOL_MAX_WORDS = 128ull << 20;  // 512 MiB of idle input blocks at most
+constexpr size_t POOL_SCAN = 16;                   // free blocks examined per request
+
+// A block of at least `words` words: one of the free blocks when one is big
+// enough, else a new one (a quarter larger, so that it serves later games too).
+void take_buf(geq_server *s, Request &r, size_t words) {
+  {
+    std::lock_guard<std::mutex> lk(s->pool_mu);
+    auto &f = s->free_bufs;
+    for (size_t k = 0; k < std::min(POOL_SCAN, f.size()); k++) {
+      auto &b = f[f.size() - 1 - k];
+      if (b.second < words) continue;
+      r.buf = std::move(b.first);
+      r.buf_words = b.second;
+      s->free_words -= b.second;
+      b = std::move(f.back());
+      f.pop_back();
+      return;
+    }
+  }
+  r.buf_words = words + words / 4 + 64;
+  r.buf.reset(new uint32_t[r.buf_words]);
+}
+// Called with s->mu held, when the request leaves the server.
+void recycle_buf(geq_server *s, Request &r) {
+  if (!r.buf) return;
+  std::lock_guard<std::mutex> lk(s->pool_mu);
+  if (s->free_words + r.buf_words > POOL_MAX_WORDS) return;
+  s->free_words += r.buf_words;
+  s->free_bufs.emplace_back(std::move(r.buf), r.buf_words);
+}
 
 // One game of a batch solution as a solution of its own that views the
 // batch's lists (no copy; the batch lives until its last view is freed).
@@ -115,12 +158,12 @@ void run_wide(Engine &e, int device, std::vector<Request *> &batch) {
     GameInput &gi = in[0];
     gi.g.conf = r->conf;
     gi.g.n_vertices = r->n;
-    gi.g.row_offsets = r->row.data();
-    gi.g.column_indices = r->col.data();
-    gi.g.weights = r->wt.data();
-    gi.g.attacker_pos = r->att.data();
-    gi.to_reach = r->reach.data();
-    gi.n_reach = (uint32_t)r->reach.size();
+    gi.g.row_offsets = r->row;
+    gi.g.column_indices = r->col;
+    gi.g.weights = r->wt;
+    gi.g.attacker_pos = r->att;
+    gi.to_reach = r->reach;
+    gi.n_reach = r->n_reach;
     std::unique_ptr<geq_solution> sol(new geq_solution());
     const geq_status st = solve_wide(e, device, in, *sol);
     if (st) {
@@ -209,12 +252,12 @@ void start_games(Engine &e, std::vector<Request *> &batch, uint64_t footprint,
     GameInput &gi = in[i];
     gi.g.conf = r.conf;
     gi.g.n_vertices = r.n;
-    gi.g.row_offsets = r.row.data();
-    gi.g.column_indices = r.col.data();
-    gi.g.weights = r.wt.data();
-    gi.g.attacker_pos = r.att.data();
-    gi.to_reach = r.reach.data();
-    gi.n_reach = (uint32_t)r.reach.size();
+    gi.g.row_offsets = r.row;
+    gi.g.column_indices = r.col;
+    gi.g.weights = r.wt;
+    gi.g.attacker_pos = r.att;
+    gi.to_reach = r.reach;
+    gi.n_reach = r.n_reach;
   }
   if (batch.size() == 1) {
     std::unique_ptr<geq_solution> one(new geq_solution());
@@ -505,12 +548,27 @@ geq_status geq_server_submit(geq_server *s, const geq_game_graph *graph, uint64_
   std::unique_ptr<Request> r(new Request());
   r->conf = graph->conf;
   r->n = graph->n_vertices;
-  r->row.assign(graph->row_offsets, graph->row_offsets + n + 1);
-  r->col.assign(graph->column_indices, graph->column_indices + m);
-  r->wt.assign(graph->weights, graph->weights + m * us);
-  r->att.assign(graph->attacker_pos, graph->attacker_pos + n);
-  for (auto &a : r->att) a = a ? 1 : 0;
-  r->reach = standard_reach_of(*graph);
+  take_buf(s, *r, (n + 1) + m + m * us + (n + 3) / 4 + n);
+  uint32_t *w = r->buf.get();
+  std::memcpy(w, graph->row_offsets, (n + 1) * 4);
+  r->row = w;
+  w += n + 1;
+  if (m) std::memcpy(w, graph->column_indices, m * 4);
+  r->col = w;
+  w += m;
+  if (m) std::memcpy(w, graph->weights, m * us * 4);
+  r->wt = w;
+  w += m * us;
+  uint8_t *att = (uint8_t *)w;
+  for (uint64_t v = 0; v < n; v++) att[v] = graph->attacker_pos[v] ? 1 : 0;
+  r->att = att;
+  w += (n + 3) / 4;
+  // standard reach: the defenders without successors (energygame.rs:347-352)
+  uint32_t nr = 0;
+  for (uint64_t v = 0; v < n; v++)
+    if (!att[v] && graph->row_offsets[v + 1] == graph->row_offsets[v]) w[nr++] = (uint32_t)v;
+  r->reach = w;
+  r->n_reach = nr;
   r->footprint = game_footprint(n, m);
   if (BATCH_BASE_BYTES + r->footprint > s->budget)
     return fail(GEQ_ERR_OUT_OF_MEMORY, "game of %llu positions needs ~%llu device bytes, a pipeline may use %llu",
@@ -574,6 +632,7 @@ geq_status geq_server_poll(geq_server *s, uint64_t ticket, int32_t timeout_ms, g
   const geq_status st = r->st;
   if (st) set_last_error(r->err);
   else *out = r->sol.release();
+  recycle_buf(s, *r);
   s->reqs.erase(it);
   return st;
 }
@@ -602,6 +661,7 @@ geq_status geq_server_poll_any(geq_server *s, int32_t timeout_ms, uint64_t *tick
   const geq_status st = r->st;
   if (st) set_last_error(r->err);
   else *out = r->sol.release();
+  recycle_buf(s, *r);
   s->reqs.erase(it);
   return st;
 }
