@@ -474,6 +474,9 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
         warm = np.arange(min(len(items), 512))
         load.open_loop(np.zeros(min(32, len(warm))), warm[:32])
         load.open_loop(np.zeros(len(warm)), warm)
+        if saturation_s > 0:  # the page-locked input pool up to the saturation run's depth
+            load.closed_loop(np.arange(len(items)) if saturation_items is None
+                             else np.asarray(saturation_items, np.int64), outstanding, 1.5)
         for lam in rates:
             n = max(1, int(rng.poisson(lam * seconds)))
             arrivals = np.sort(rng.uniform(0, seconds, n))

@@ -1787,6 +1787,44 @@ __global__ void k_pack_edges(const uint32_t *col, const uint32_t *wt, unsigned l
     cw[k] = (unsigned long long)col[k] | ((unsigned long long)Cd::pack_edge(wt[k]) << 32);
 }
 
+// Packed game blocks (row | col | wt | attacker bytes | reach, one after the
+// other in `raw`, game g from word boff[g]) into the batch's arrays: rows and
+// columns stay game-local (k_fix_rows / k_fix_cols rebase them), reach
+// entries get the game's position base.  One thread per word of `raw`.
+__global__ void k_unpack_games(const uint32_t *raw, const unsigned long long *boff, const unsigned long long *nb,
+                               const unsigned long long *eb, const unsigned long long *rb, uint32_t n_games,
+                               unsigned long long words, uint32_t *row, uint32_t *col, uint32_t *wt,
+                               uint8_t *flags, uint32_t *reach, unsigned long long N, unsigned long long M) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) row[N] = (uint32_t)M;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < words;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = n_games - 1;  // the game whose block holds word i
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (boff[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    const uint32_t g = lo;
+    const unsigned long long n = nb[g + 1] - nb[g], m = eb[g + 1] - eb[g];
+    unsigned long long k = i - boff[g];
+    const uint32_t x = raw[i];
+    if (k < n + 1) {
+      if (k < n) row[nb[g] + k] = x;
+      continue;
+    }
+    k -= n + 1;
+    if (k < m) { col[eb[g] + k] = x; continue; }
+    k -= m;
+    if (k < m) { wt[eb[g] + k] = x; continue; }
+    k -= m;
+    const unsigned long long aw = (n + 3) / 4;
+    if (k < aw) {
+      for (unsigned long long b = 0; b < 4 && 4 * k + b < n; b++) flags[nb[g] + 4 * k + b] = (uint8_t)(x >> (8 * b));
+      continue;
+    }
+    k -= aw;
+    if (k < rb[g + 1] - rb[g]) reach[rb[g] + k] = x + (uint32_t)nb[g];
+  }
+}
 __global__ void k_init_reach(unsigned long long *desc, const uint32_t *reach, unsigned long long n_reach) {
   for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n_reach;
        i += (unsigned long long)gridDim.x * blockDim.x)
@@ -2036,7 +2074,7 @@ void *HostPool::get(size_t bytes, size_t &cap) {
       }
   }
   void *p = nullptr;
-  if (cudaHostAlloc(&p, cap, cudaHostAllocDefault) != cudaSuccess) {
+  if (cudaHostAlloc(&p, cap, flags_) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
   }
@@ -2387,6 +2425,9 @@ uint64_t Engine::game_node_base(const DeviceGamesImpl &dg, uint32_t g) { return 
 geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
   State &s = *st;
   if (games.empty()) return fail(GEQ_ERR_INVALID_INPUT, "no games");
+  bool packed = true;
+  for (const GameInput &gi : games) packed = packed && gi.block && !gi.init;
+  if (packed) return upload_blocks(games, out);
 #if GEQ_PATH_PROFILE
   const auto tu0 = std::chrono::steady_clock::now();
   auto tsince = [&]() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tu0).count(); };
@@ -2510,6 +2551,117 @@ geq_status Engine::upload(std::vector<GameInput> &games, GamesPtr &out) {
 #endif
   if (ust) return ust;
   return finish_upload(dg, any_init, out);
+}
+
+// Games that each sit in one packed host block (GameInput::block, page-locked
+// when the caller could get it so): one copy per block into a device scratch
+// area, unpacked there into the batch's arrays by k_unpack_games, so the
+// host copies nothing; the small per-game tables go through the staging
+// buffer.  The device half is the one of upload().
+geq_status Engine::upload_blocks(std::vector<GameInput> &games, GamesPtr &out) {
+  State &s = *st;
+  const uint32_t G = (uint32_t)games.size();
+  GamesPtr dg(new DeviceGamesImpl());
+  dg->owner = &s;
+  s.live.insert(dg.get());
+  dg->conf = Conf(games[0].g.conf);
+  if (!dg->conf.supported())
+    return fail(GEQ_ERR_UNSUPPORTED, "EnergyConf {%u, %u} is outside the device codecs", dg->conf.elements,
+                dg->conf.max);
+  dg->generic = !dg->conf.standard() || (tuning.flags & GEQ_TUNE_FORCE_GENERIC);
+  dg->n_games = G;
+  dg->node_base.assign(G + 1, 0);
+  dg->edge_base.assign(G + 1, 0);
+  dg->std_reach = true;
+  dg->rows_on_device = true;
+  unsigned long long n_reach = 0, words = 0;
+  for (uint32_t g = 0; g < G; g++) {
+    const GameInput &gi = games[g];
+    if (!(Conf(gi.g.conf) == dg->conf)) return fail(GEQ_ERR_INVALID_INPUT, "games of one batch need one EnergyConf");
+    const uint64_t n = gi.g.n_vertices, m = gi.g.row_offsets[n];
+    if (gi.block_words != packed_game_words(n, m, gi.n_reach))
+      return fail(GEQ_ERR_INTERNAL, "packed block of game %u has %zu words, expected %zu", g, gi.block_words,
+                  packed_game_words(n, m, gi.n_reach));
+    dg->std_reach = dg->std_reach && gi.std_reach;
+    dg->rows_on_device = dg->rows_on_device && gi.rows_unchecked;
+    dg->node_base[g + 1] = dg->node_base[g] + n;
+    dg->edge_base[g + 1] = dg->edge_base[g] + m;
+    n_reach += gi.n_reach;
+    words += gi.block_words;
+  }
+  dg->N = dg->node_base.back();
+  dg->M = dg->edge_base.back();
+  if (dg->N >= 0xFFFFFFF0ull || dg->M >= 0xFFFFFFF0ull)
+    return fail(GEQ_ERR_INVALID_INPUT, "too many positions/edges for 32-bit ids (%llu, %llu)", dg->N, dg->M);
+  const unsigned long long N = dg->N, M = dg->M;
+  dg->init_total = 1;  // the zero energy of standard initialisation
+  dg->n_reach = n_reach;
+  // the input block's layout is upload()'s (no initial lists); two tables
+  // follow it: each game's first word in the scratch area and reach base
+  const size_t off_row = 0, off_col = off_row + (N + 1) * 4, off_wt = off_col + M * 4, off_flags = off_wt + M * 4;
+  const size_t off_reach = (off_flags + N + 15) & ~size_t(15);
+  const size_t off_init = off_reach + n_reach * 4;
+  const size_t off_base = (off_init + 4 + 15) & ~size_t(15);
+  const size_t off_boff = off_base + (G + 1) * 8 * 3;
+  const size_t off_rb = off_boff + (G + 1) * 8;
+  const size_t total_bytes = off_rb + (G + 1) * 8;
+  const size_t tail = total_bytes - off_init;  // staged: init word and the tables
+  geq_status stt = ensure_stage(s, tail);
+  if (stt) return stt;
+  char *H = s.stage;
+  ((uint32_t *)H)[0] = 0;
+  unsigned long long *h_nb = (unsigned long long *)(H + (off_base - off_init));
+  unsigned long long *h_eb = h_nb + (G + 1), *h_gn = h_eb + (G + 1);
+  unsigned long long *h_boff = (unsigned long long *)(H + (off_boff - off_init));
+  unsigned long long *h_rb = (unsigned long long *)(H + (off_rb - off_init));
+  unsigned long long w = 0, r = 0;
+  for (uint32_t g = 0; g < G; g++) {
+    h_nb[g] = dg->node_base[g];
+    h_eb[g] = dg->edge_base[g];
+    h_gn[g] = games[g].g.n_vertices;
+    h_boff[g] = w;
+    h_rb[g] = r;
+    w += games[g].block_words;
+    r += games[g].n_reach;
+  }
+  h_nb[G] = N;
+  h_eb[G] = M;
+  h_gn[G] = 0;
+  h_boff[G] = w;
+  h_rb[G] = r;
+  DeviceGamesImpl &D = *dg;
+  if (!D.alloc(D.inbuf, total_bytes))
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation of %zu input bytes failed", total_bytes);
+  D.row = (uint32_t *)(D.inbuf + off_row);
+  D.col = (uint32_t *)(D.inbuf + off_col);
+  D.wt = (uint32_t *)(D.inbuf + off_wt);
+  D.flags = (uint8_t *)(D.inbuf + off_flags);
+  D.reach = (uint32_t *)(D.inbuf + off_reach);
+  D.init_data = (uint32_t *)(D.inbuf + off_init);
+  D.d_node_base = (unsigned long long *)(D.inbuf + off_base);
+  geq_status ast = alloc_work(D, false);
+  if (ast) return ast;
+  uint32_t *raw = (uint32_t *)s.pool.get(std::max<size_t>(words, 1) * 4);
+  if (!raw) return fail(GEQ_ERR_OUT_OF_MEMORY, "device scratch of %llu words for the game blocks", words);
+  struct Give {
+    DevPool &pool;
+    void *p;
+    size_t b;
+    ~Give() { pool.put(p, b); }  // later users of the pool run behind this upload on the stream
+  } give{s.pool, raw, std::max<size_t>(words, 1) * 4};
+  cudaStream_t S = s.stream;
+  for (uint32_t g = 0; g < G; g++)
+    if (games[g].block_words)
+      CU(cudaMemcpyAsync(raw + h_boff[g], games[g].block, games[g].block_words * 4, cudaMemcpyHostToDevice, S));
+  CU(cudaMemcpyAsync(D.inbuf + off_init, H, tail, cudaMemcpyHostToDevice, S));
+  if (words) {
+    const unsigned grid = (unsigned)std::max<unsigned long long>(
+        1, std::min<unsigned long long>((words + 255) / 256, (unsigned long long)n_sms * 8));
+    k_unpack_games<<<grid, 256, 0, S>>>(raw, (const unsigned long long *)(D.inbuf + off_boff), D.d_node_base,
+                                        D.d_node_base + (G + 1), (const unsigned long long *)(D.inbuf + off_rb), G,
+                                        words, D.row, D.col, D.wt, D.flags, D.reach, N, M);
+  }
+  return finish_upload(dg, false, out);
 }
 
 // Games already on the device in the solver's input layout (built by the

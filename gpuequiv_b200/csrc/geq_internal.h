@@ -53,7 +53,17 @@ struct GameInput {
   std::vector<uint32_t> reach_storage;  // standard reach when none was given
   bool std_reach = false;       // standard reach, to be computed on the device (no list)
   bool rows_unchecked = false;  // row monotonicity left to the device (large batches)
+  // optional: the game packed in one host block, row (n+1) | col (m) | wt (m)
+  // | attacker bytes ((n+3)/4 words) | reach (n_reach), that g and to_reach
+  // point into; a batch whose games all have one is copied block by block
+  // and unpacked on the device (no host staging copy)
+  const uint32_t *block = nullptr;
+  size_t block_words = 0;
 };
+// Words of a packed game block (see GameInput::block).
+inline size_t packed_game_words(uint64_t n, uint64_t m, uint64_t n_reach) {
+  return (n + 1) + 2 * m + (n + 3) / 4 + n_reach;
+}
 
 // Validation of a graph view (TryFrom<SerdeGameGraph> checks,
 // energygame.rs:65-83, plus update-code checks).
@@ -93,6 +103,9 @@ void parallel_for(uint32_t n, F f, uint32_t max_threads = 0) {
 // lent block, whichever is later.
 class HostPool {
  public:
+  HostPool() = default;
+  // flags: cudaHostAlloc flags of new blocks; limit: bytes of idle blocks kept
+  HostPool(unsigned flags, size_t limit) : flags_(flags), limit_(limit) {}
   static size_t round_size(size_t bytes);
   void *get(size_t bytes, size_t &cap);  // nullptr when page-locked memory is unavailable
   void put(void *p, size_t cap);
@@ -102,6 +115,7 @@ class HostPool {
   std::mutex mu_;
   std::map<size_t, std::vector<void *>> free_;
   size_t cached_ = 0;
+  unsigned flags_ = 0;
   size_t limit_ = (size_t)4 << 30;
 };
 
@@ -191,6 +205,7 @@ class Engine {
   static geq_status create(int device, std::unique_ptr<Engine> &out);
   ~Engine();
   geq_status upload(std::vector<GameInput> &games, GamesPtr &out);
+  geq_status upload_blocks(std::vector<GameInput> &games, GamesPtr &out);
   // games already on the device (BuiltGames), standard reach
   geq_status upload_built(const BuiltGames &b, GamesPtr &out);
   geq_status solve(DeviceGamesImpl &dg, geq_solve_stats *stats);

@@ -56,10 +56,10 @@ struct Request {
   uint32_t p = 0, q = 0;
   geq_energy_conf conf{};
   uint32_t n = 0;
-  // a game's copy: row | col | wt | attacker bytes | reach in one block that
-  // is handed back to the server's pool when the request is answered
-  std::unique_ptr<uint32_t[]> buf;
-  size_t buf_words = 0;
+  // a game's copy: row | col | wt | attacker bytes | reach in one page-locked
+  // block from the server's pool (back to the pool when the request is
+  // answered); the pipeline copies it to the device as it is
+  HostBuf blk;
   const uint32_t *row = nullptr, *col = nullptr, *wt = nullptr, *reach = nullptr;
   const uint8_t *att = nullptr;
   uint32_t n_reach = 0;
@@ -89,46 +89,28 @@ struct geq_server {
   uint64_t next_ticket = 1;
   bool stop = false;
   geq_server_stats stats{};
-  // input blocks of answered requests, reused by submit: a fresh block of a
-  // few hundred KB costs page faults on every request (and unmapping it
-  // costs every thread of the process a TLB flush)
-  std::mutex pool_mu;
-  std::vector<std::pair<std::unique_ptr<uint32_t[]>, size_t>> free_bufs;
-  uint64_t free_words = 0;
+  // page-locked input blocks, reused: a fresh heap block of a few hundred KB
+  // costs page faults on every request (and unmapping it a TLB flush on
+  // every thread), and a pageable block would be copied once more to reach
+  // the device
+  std::shared_ptr<HostPool> inpool;
 };
 
 namespace {
 
-constexpr uint64_t POOL_MAX_WORDS = 128ull << 20;  // 512 MiB of idle input blocks at most
-constexpr size_t POOL_SCAN = 16;                   // free blocks examined per request
+constexpr size_t INPOOL_IDLE_BYTES = (size_t)4 << 30;  // idle page-locked input blocks kept
 
-// A block of at least `words` words: one of the free blocks when one is big
-// enough, else a new one (a quarter larger, so that it serves later games too).
-void take_buf(geq_server *s, Request &r, size_t words) {
-  {
-    std::lock_guard<std::mutex> lk(s->pool_mu);
-    auto &f = s->free_bufs;
-    for (size_t k = 0; k < std::min(POOL_SCAN, f.size()); k++) {
-      auto &b = f[f.size() - 1 - k];
-      if (b.second < words) continue;
-      r.buf = std::move(b.first);
-      r.buf_words = b.second;
-      s->free_words -= b.second;
-      b = std::move(f.back());
-      f.pop_back();
-      return;
-    }
-  }
-  r.buf_words = words + words / 4 + 64;
-  r.buf.reset(new uint32_t[r.buf_words]);
-}
-// Called with s->mu held, when the request leaves the server.
-void recycle_buf(geq_server *s, Request &r) {
-  if (!r.buf) return;
-  std::lock_guard<std::mutex> lk(s->pool_mu);
-  if (s->free_words + r.buf_words > POOL_MAX_WORDS) return;
-  s->free_words += r.buf_words;
-  s->free_bufs.emplace_back(std::move(r.buf), r.buf_words);
+// A request's input block from the server's page-locked pool (heap memory
+// when none can be had); a new block is allocated with the server's device
+// current, so the caller's current device is left as it was.
+bool take_block(geq_server *s, Request &r, size_t words) {
+  int dev = -1;
+  cudaGetDevice(&dev);
+  if (dev != s->device) cudaSetDevice(s->device);
+  const bool ok = r.blk.alloc(s->inpool, words * 4);
+  if (dev != s->device && dev >= 0) cudaSetDevice(dev);
+  cudaGetLastError();
+  return ok;
 }
 
 // One game of a batch solution as a solution of its own that views the
@@ -258,6 +240,8 @@ void start_games(Engine &e, std::vector<Request *> &batch, uint64_t footprint,
     gi.g.attacker_pos = r.att;
     gi.to_reach = r.reach;
     gi.n_reach = r.n_reach;
+    gi.block = (const uint32_t *)r.blk.p;  // one word per update (a device codec conf)
+    gi.block_words = packed_game_words(r.n, r.row[r.n], r.n_reach);
   }
   if (batch.size() == 1) {
     std::unique_ptr<geq_solution> one(new geq_solution());
@@ -524,6 +508,7 @@ geq_status geq_server_create(geq_context *ctx, const geq_server_config *cfg, geq
   if (!s->cfg.hbm_budget_bytes) s->cfg.hbm_budget_bytes = 150ull * 1000 * 1000 * 1000;
   if (!s->cfg.max_queued) s->cfg.max_queued = 1000000;
   s->budget = s->cfg.hbm_budget_bytes / s->cfg.n_pipelines;
+  s->inpool = std::make_shared<HostPool>(cudaHostAllocPortable, INPOOL_IDLE_BYTES);
   for (uint32_t i = 0; i < s->cfg.n_pipelines; i++) {
     std::unique_ptr<Engine> e;
     geq_status st = Engine::create(ctx->device, e);
@@ -548,8 +533,9 @@ geq_status geq_server_submit(geq_server *s, const geq_game_graph *graph, uint64_
   std::unique_ptr<Request> r(new Request());
   r->conf = graph->conf;
   r->n = graph->n_vertices;
-  take_buf(s, *r, (n + 1) + m + m * us + (n + 3) / 4 + n);
-  uint32_t *w = r->buf.get();
+  if (!take_block(s, *r, (n + 1) + m + m * us + (n + 3) / 4 + n))
+    return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for a game of %llu positions", (unsigned long long)n);
+  uint32_t *w = (uint32_t *)r->blk.p;
   std::memcpy(w, graph->row_offsets, (n + 1) * 4);
   r->row = w;
   w += n + 1;
@@ -632,7 +618,6 @@ geq_status geq_server_poll(geq_server *s, uint64_t ticket, int32_t timeout_ms, g
   const geq_status st = r->st;
   if (st) set_last_error(r->err);
   else *out = r->sol.release();
-  recycle_buf(s, *r);
   s->reqs.erase(it);
   return st;
 }
@@ -661,7 +646,6 @@ geq_status geq_server_poll_any(geq_server *s, int32_t timeout_ms, uint64_t *tick
   const geq_status st = r->st;
   if (st) set_last_error(r->err);
   else *out = r->sol.release();
-  recycle_buf(s, *r);
   s->reqs.erase(it);
   return st;
 }
