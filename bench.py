@@ -300,149 +300,129 @@ def peak_hbm():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+class LoadApi:
+    """ctypes mirror of the native load driver's callback table
+    (gpuequiv_b200/csrc/loadgen.cpp: geq_load_api, geq_load_server)."""
+    import ctypes as C
+    SUBMIT = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint64))
+    POLL = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_int32, C.POINTER(C.c_uint64), C.POINTER(C.c_void_p))
+    FREE = C.CFUNCTYPE(None, C.c_void_p)
+
+    class Api(C.Structure):
+        pass
+
+    class Server(C.Structure):
+        pass
+
+
+_LOADGEN = []
+
+
+def _loadgen():
+    import ctypes as C
+    if _LOADGEN:
+        return _LOADGEN[0]
+    path = os.path.join(ROOT, "gpuequiv_b200", "libgeq_load.so")
+    ll = C.CDLL(path)
+    LoadApi.Api._fields_ = [("ctx", C.c_void_p), ("submit", LoadApi.SUBMIT), ("poll_any", LoadApi.POLL),
+                            ("free_answer", LoadApi.FREE)]
+    LoadApi.Server._fields_ = [("server", C.c_void_p), ("games", C.c_void_p), ("game_stride", C.c_size_t),
+                               ("lts", C.POINTER(C.c_void_p)), ("p", C.POINTER(C.c_uint32)),
+                               ("q", C.POINTER(C.c_uint32)), ("server_submit", C.c_void_p),
+                               ("server_submit_compare", C.c_void_p), ("server_poll_any", C.c_void_p),
+                               ("solution_free", C.c_void_p)]
+    ll.geq_load_server_api.argtypes = [C.POINTER(LoadApi.Server), C.POINTER(LoadApi.Api)]
+    ll.geq_load_server_api.restype = None
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    u32p = C.POINTER(C.c_uint32)
+    ll.geq_load_open.argtypes = [C.POINTER(LoadApi.Api), u32p, dp, C.c_uint64, C.c_uint32, C.c_uint32, C.c_double,
+                                 dp, ip, dp]
+    ll.geq_load_open.restype = C.c_int64
+    ll.geq_load_closed.argtypes = [C.POINTER(LoadApi.Api), u32p, C.c_uint32, C.c_uint32, C.c_double, C.c_uint64,
+                                   C.c_uint32, C.c_uint32, C.c_uint64, C.c_double, dp, ip,
+                                   C.POINTER(C.c_uint64), dp]
+    ll.geq_load_closed.restype = C.c_int64
+    _LOADGEN.append(ll)
+    return ll
+
+
 class Load:
-    """Drives a geq_server from host threads through the C ABI: arrival i
-    submits item pick[i] (a game view or an (lts, p, q) query) at its arrival
-    time (open loop) or whenever fewer than `outstanding` requests are in
-    flight (closed loop).  Finished requests are taken from the server's
-    completion queue (geq_server_poll_any) in the order they finish, so one
-    slow request does not hold back the recording of others.  Latency =
-    submit -> the request's solution in the caller's hands."""
+    """Drives a geq_server through the C ABI from native threads (the load
+    driver gpuequiv_b200/csrc/loadgen.cpp, built as libgeq_load.so): arrival
+    i submits item pick[i] (a game view or an (lts, p, q) query) at its
+    arrival time (open loop), or `outstanding` requests are kept in flight
+    (closed loop).  Finished requests are taken from the server's completion
+    queue (geq_server_poll_any) in the order they finish.  Latency = submit
+    -> the request's solution in the caller's hands.  A Python driver was
+    measured to cap the closed loop near 30k requests/s by itself (the
+    interpreter lock around every submit and poll); this one does not.
+    `api`: a LoadApi.Api to drive instead of the server (tests)."""
 
-    def __init__(self, srv, items, queries: bool, threads: int = 4, drain_s: float = 60.0):
-        from gpuequiv_b200._lib import lib
-        self.lib, self.h, self.items, self.queries, self.threads = lib, srv.h, items, queries, threads
-        self.drain_s = drain_s  # after the last arrival, wait this long for the rest
-
-    def _submit(self, item):
+    def __init__(self, srv, items, queries: bool, threads: int = 4, drain_s: float = 60.0, api=None):
         import ctypes as C
-        t = C.c_uint64()
-        if self.queries:
-            lts, p, q = item
-            st = self.lib.geq_server_submit_compare(self.h, lts.h, p, q, C.byref(t))
-        else:
-            st = self.lib.geq_server_submit(self.h, C.byref(item), C.byref(t))
-        if st:
-            raise RuntimeError(f"submit failed: status {st}")
-        return t.value
+        self.ll = _loadgen()
+        self.threads, self.drain_s = threads, drain_s
+        if api is None:
+            from gpuequiv_b200._lib import geq_game_graph, lib
+            ls = LoadApi.Server()
+            ls.server = srv.h.value if hasattr(srv.h, "value") else srv.h
+            addr = lambda f: C.cast(f, C.c_void_p).value  # noqa: E731
+            if queries:
+                self._lts = (C.c_void_p * len(items))(*[lts.h.value for lts, _, _ in items])
+                self._p = np.ascontiguousarray([p for _, p, _ in items], np.uint32)
+                self._q = np.ascontiguousarray([q for _, _, q in items], np.uint32)
+                ls.lts = self._lts
+                ls.p = self._p.ctypes.data_as(C.POINTER(C.c_uint32))
+                ls.q = self._q.ctypes.data_as(C.POINTER(C.c_uint32))
+            else:
+                ls.games = C.addressof(items)  # a ctypes array of geq_game_graph
+                ls.game_stride = C.sizeof(geq_game_graph)
+            ls.server_submit = addr(lib.geq_server_submit)
+            ls.server_submit_compare = addr(lib.geq_server_submit_compare)
+            ls.server_poll_any = addr(lib.geq_server_poll_any)
+            ls.solution_free = addr(lib.geq_solution_free)
+            self._ls, self._items = ls, items
+            api = LoadApi.Api()
+            self.ll.geq_load_server_api(C.byref(ls), C.byref(api))
+        self.api = api
 
-    def _poll_any(self, timeout_ms):
-        """(ticket, status) of a finished request, or None after timeout_ms."""
-        import ctypes as C
-        sol = C.c_void_p()
-        t = C.c_uint64()
-        st = self.lib.geq_server_poll_any(self.h, timeout_ms, C.byref(t), C.byref(sol))
-        if t.value == 0:
-            return None
-        if st == 0:
-            self.lib.geq_solution_free(sol)
-        return t.value, st
-
-    def _pollers(self, total_fn, done, deadline):
-        """Poller threads appending (ticket, time, status) to `done` until
-        total_fn() requests have finished (total_fn None: not known yet) or
-        deadline[0] (set once the last request is submitted) has passed."""
-        import threading
-
-        def poller():
-            while True:
-                n = total_fn()
-                if n is not None and len(done) >= n:
-                    return
-                if deadline[0] is not None and time.perf_counter() > deadline[0]:
-                    return
-                r = self._poll_any(50)
-                if r is not None:
-                    done.append((r[0], time.perf_counter(), r[1]))
-
-        th = [threading.Thread(target=poller, daemon=True) for _ in range(max(1, self.threads // 2))]
-        for x in th:
-            x.start()
-        return th
+    def _threads(self):
+        return max(1, self.threads // 2), max(1, self.threads // 2)
 
     def open_loop(self, arrivals, pick):
-        import threading
+        import ctypes as C
         n = len(arrivals)
-        subs, done = [], []
-        t0 = time.perf_counter() + 0.05
+        arr = np.ascontiguousarray(arrivals, np.float64)
+        pk = np.ascontiguousarray(pick, np.uint32)
+        lat = np.zeros(max(n, 1), np.float64)
+        st = np.full(max(n, 1), -1, np.int32)
+        span = C.c_double(0.0)
+        ns, npoll = self._threads()
+        r = self.ll.geq_load_open(C.byref(self.api), pk.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                  arr.ctypes.data_as(C.POINTER(C.c_double)), n, ns, npoll, self.drain_s,
+                                  lat.ctypes.data_as(C.POINTER(C.c_double)), st.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  C.byref(span))
+        if r < 0:
+            raise RuntimeError("load driver: invalid arguments")
+        return lat[:n], st[:n], span.value
 
-        def submitter(k):
-            mine = []
-            for i in range(k, n, self.threads):
-                wait = t0 + arrivals[i] - time.perf_counter()
-                if wait > 0:
-                    time.sleep(wait)
-                ts = time.perf_counter()
-                mine.append((self._submit(self.items[pick[i]]), ts))
-            subs.extend(mine)
-
-        th = [threading.Thread(target=submitter, args=(k,)) for k in range(self.threads)]
-        for x in th:
-            x.start()
-        deadline = [None]
-        pol = self._pollers(lambda: n, done, deadline)
-        for x in th:
-            x.join()
-        deadline[0] = time.perf_counter() + self.drain_s
-        for x in pol:
-            x.join()
-        return self._result(subs, done, t0)
-
-    @staticmethod
-    def _result(subs, done, t0):
-        """Latencies and statuses of the finished requests; the ones still
-        unfinished at the deadline count with status -1."""
-        sub = dict(subs)
-        fin = {t for t, _, _ in done}
-        lat = np.array([(td - sub[t]) * 1e3 for t, td, _ in done if t in sub])
-        status = np.array([st for t, _, st in done if t in sub] + [-1] * sum(1 for t in sub if t not in fin), np.int32)
-        t_end = max([td for _, td, _ in done] or [t0])
-        return lat, status, t_end - t0
-
-    def closed_loop(self, pick, outstanding: int, seconds: float):
-        import threading
-        subs, done = [], []
-        slots = threading.Semaphore(outstanding)
-        t0 = time.perf_counter()
-        t_end = t0 + seconds
-        n_sub = [0]
-        stop = [False]
-
-        def submitter(k):
-            rng = np.random.default_rng(k)
-            mine = []
-            while time.perf_counter() < t_end:
-                if not slots.acquire(timeout=0.05):
-                    continue
-                ts = time.perf_counter()
-                mine.append((self._submit(self.items[pick[int(rng.integers(len(pick)))]]), ts))
-            subs.extend(mine)
-
-        def releaser():
-            seen = 0
-            while not stop[0]:
-                while seen < len(done):
-                    slots.release()
-                    seen += 1
-                time.sleep(0.0005)
-
-        th = [threading.Thread(target=submitter, args=(k,)) for k in range(2)]
-        rel = threading.Thread(target=releaser)
-        for x in th:
-            x.start()
-        rel.start()
-        total = [None]
-        deadline = [None]
-        pol = self._pollers(lambda: total[0], done, deadline)
-        for x in th:
-            x.join()
-        total[0] = len(subs)
-        deadline[0] = time.perf_counter() + self.drain_s
-        for x in pol:
-            x.join()
-        stop[0] = True
-        rel.join()
-        return self._result(subs, done, t0)
+    def closed_loop(self, pick, outstanding: int, seconds: float, cap_rate: float = 400_000.0):
+        import ctypes as C
+        pk = np.ascontiguousarray(pick, np.uint32)
+        cap = int(seconds * cap_rate) + outstanding + 1024
+        lat = np.zeros(cap, np.float64)
+        st = np.full(cap, -1, np.int32)
+        nsub = C.c_uint64(0)
+        span = C.c_double(0.0)
+        ns, npoll = self._threads()
+        r = self.ll.geq_load_closed(C.byref(self.api), pk.ctypes.data_as(C.POINTER(C.c_uint32)), len(pk),
+                                    outstanding, seconds, cap, ns, npoll, 1, self.drain_s,
+                                    lat.ctypes.data_as(C.POINTER(C.c_double)),
+                                    st.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(nsub), C.byref(span))
+        if r < 0:
+            raise RuntimeError("load driver: invalid arguments")
+        n = int(nsub.value)
+        return lat[:n], st[:n], span.value
 
 
 def _lat_summary(lat_ms, status, span_s):

@@ -70,6 +70,21 @@ def build(checked: bool = False, force: bool = False, verbose: bool = False) -> 
         list(ex.map(run, jobs))
     if force or jobs or not _newer(out, objs):
         run([nvcc()] + ARCH + ["-shared", "-o", out] + objs + ["-lcudart_static", "-ldl", "-lrt", "-lpthread"])
+    if not checked:
+        build_loadgen(force)
+    return out
+
+
+def build_loadgen(force: bool = False) -> str:
+    """libgeq_load.so: the serving loop's native load driver (csrc/loadgen.cpp,
+    no CUDA), used by the bench and its CPU test."""
+    src = os.path.join(CSRC, "loadgen.cpp")
+    out = os.path.join(HERE, "libgeq_load.so")
+    if force or not _newer(out, [src]):
+        r = subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", src, "-o", out],
+                           capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("build failed: loadgen.cpp\n" + r.stdout + r.stderr)
     return out
 
 

@@ -1,7 +1,8 @@
-"""bench.py's serving load driver (Load) against a fake server on the CPU:
-every submitted request is collected once from the completion queue, with
-its own latency, in open and closed loop, also when requests finish out of
-order."""
+"""bench.py's serving load driver (the native driver of
+gpuequiv_b200/csrc/loadgen.cpp behind bench.Load) against a fake server on
+the CPU: every submitted request is collected once from the completion
+queue, with its own latency, in open and closed loop, also when requests
+finish out of order or not before the drain deadline."""
 import ctypes as C
 import os
 import sys
@@ -15,9 +16,10 @@ sys.path.insert(0, ROOT)
 import bench  # noqa: E402
 
 
-class FakeLib:
-    """geq_server_submit / _poll_any / geq_solution_free: request k finishes
-    delay(k) seconds after its submission, in whatever order that gives."""
+class FakeServer:
+    """submit / poll_any / free as C callbacks: request k finishes delay(k)
+    seconds after its submission, in whatever order that gives; every 7th
+    answers with status 2."""
 
     def __init__(self, delay):
         self.delay = delay
@@ -25,16 +27,23 @@ class FakeLib:
         self.next = 1
         self.pending = []  # (finish time, ticket)
         self.freed = 0
+        self.inflight = 0
+        self.max_seen = 0
+        self.cb = (bench.LoadApi.SUBMIT(self.submit), bench.LoadApi.POLL(self.poll_any), bench.LoadApi.FREE(self.free))
+        bench._loadgen()  # the structures' fields
+        self.api = bench.LoadApi.Api(None, *self.cb)
 
-    def geq_server_submit(self, h, item, t):
+    def submit(self, ctx, item, t):
         with self.mu:
             k = self.next
             self.next += 1
             self.pending.append((time.perf_counter() + self.delay(k), k))
-        C.cast(t, C.POINTER(C.c_uint64)).contents.value = k
+            self.inflight += 1
+            self.max_seen = max(self.max_seen, self.inflight)
+        t[0] = k
         return 0
 
-    def geq_server_poll_any(self, h, timeout_ms, t, sol):
+    def poll_any(self, ctx, timeout_ms, t, sol):
         end = time.perf_counter() + timeout_ms / 1e3
         while True:
             with self.mu:
@@ -43,43 +52,47 @@ class FakeLib:
                 if ready:
                     x = min(ready)
                     self.pending.remove(x)
-                    C.cast(t, C.POINTER(C.c_uint64)).contents.value = x[1]
-                    return 2 if x[1] % 7 == 0 else 0
+                    self.inflight -= 1
+                    t[0] = x[1]
+                    if x[1] % 7 == 0:
+                        return 2
+                    sol[0] = 1
+                    return 0
             if time.perf_counter() > end:
+                t[0] = 0
                 return 4
             time.sleep(0.0002)
 
-    def geq_solution_free(self, sol):
-        self.freed += 1
+    def free(self, sol):
+        with self.mu:
+            self.freed += 1
 
 
-def make_load(delay):
-    load = bench.Load.__new__(bench.Load)
-    load.lib, load.h, load.items, load.queries, load.threads = FakeLib(delay), None, [C.c_int(0)] * 4, False, 4
-    load.drain_s = 10.0
-    return load
+def make_load(fake, drain_s=10.0):
+    return bench.Load(None, None, False, threads=4, drain_s=drain_s, api=fake.api)
 
 
 def test_unfinished_requests_count_at_the_deadline():
-    load = make_load(lambda k: 30.0 if k == 3 else 0.001)  # request 3 never finishes in time
-    load.drain_s = 0.3
-    lat, status, span = load.open_loop(np.linspace(0, 0.05, 20), np.zeros(20, np.int64))
-    assert len(status) == 20 and (status == -1).sum() == 1 and len(lat) == 19
+    fake = FakeServer(lambda k: 30.0 if k == 3 else 0.001)  # request 3 never finishes in time
+    lat, status, span = make_load(fake, drain_s=0.3).open_loop(np.linspace(0, 0.05, 20), np.zeros(20, np.int64))
+    assert len(status) == 20 and (status == -1).sum() == 1 and (status >= 0).sum() == 19
     assert span < 5
 
 
 def test_open_loop_collects_every_request_once():
-    load = make_load(lambda k: 0.02 if k % 5 == 0 else 0.001)  # every 5th finishes late
+    fake = FakeServer(lambda k: 0.02 if k % 5 == 0 else 0.001)  # every 5th finishes late
     n = 400
-    lat, status, span = load.open_loop(np.linspace(0, 0.2, n), np.zeros(n, np.int64))
-    assert len(lat) == n and len(status) == n
+    lat, status, span = make_load(fake).open_loop(np.linspace(0, 0.2, n), np.zeros(n, np.int64))
+    assert len(lat) == n and len(status) == n and (status >= 0).all()
     assert (status == 2).sum() == len([k for k in range(1, n + 1) if k % 7 == 0])
+    assert fake.freed == (status == 0).sum()
     assert np.percentile(lat, 50) < 10 and lat.max() >= 19  # the late ones do not hold back the others
     assert 0.2 <= span < 2.0
 
 
 def test_closed_loop_keeps_outstanding_bounded():
-    load = make_load(lambda k: 0.002)
-    lat, status, span = load.closed_loop(np.zeros(4, np.int64), 16, 0.3)
-    assert len(lat) == len(status) > 50
+    fake = FakeServer(lambda k: 0.002)
+    lat, status, span = make_load(fake).closed_loop(np.zeros(4, np.int64), 16, 0.3)
+    assert len(lat) == len(status) > 50 and (status >= 0).all()
+    assert fake.max_seen <= 16
     assert lat.max() < 1000
