@@ -99,11 +99,11 @@ struct Run {
     while (ns > prev && !last_ns.compare_exchange_weak(prev, ns)) {
     }
   }
-  // request i with item `item`: false when the submit itself failed
-  void submit(uint64_t i, uint32_t item) {
+  // request i with item `item` (`reserved`: its place in flight is taken)
+  void submit(uint64_t i, uint32_t item, bool reserved = false) {
     uint64_t ticket = 0;
     t_sub[i] = Clock::now();
-    inflight.fetch_add(1);
+    if (!reserved) inflight.fetch_add(1);
     const int32_t st = api.submit(api.ctx, item, &ticket);
     submitted.fetch_add(1);
     if (st != 0 || ticket == 0) {
@@ -224,13 +224,17 @@ int64_t geq_load_closed(const geq_load_api *api, const uint32_t *pick, uint32_t 
     sub.emplace_back([&, k]() {
       uint64_t rng = seed * 0x100000001B3ull + k + 1;
       while (Clock::now() < t_end) {
-        if (r.inflight.load() >= (int64_t)outstanding) {
+        if (r.inflight.fetch_add(1) >= (int64_t)outstanding) {  // a place in flight
+          r.inflight.fetch_sub(1);
           std::this_thread::sleep_for(std::chrono::microseconds(20));
           continue;
         }
         const uint64_t i = r.next.fetch_add(1);
-        if (i >= r.cap) return;
-        r.submit(i, pick[splitmix(rng) % n_pick]);
+        if (i >= r.cap) {
+          r.inflight.fetch_sub(1);
+          return;
+        }
+        r.submit(i, pick[splitmix(rng) % n_pick], true);
       }
     });
   for (auto &t : sub) t.join();
