@@ -63,6 +63,7 @@ def parse():
                     help="Poisson arrival rates (req/s) of the serving configuration (equivalence queries on LTSs "
                          "of 20-20,000 states); empty: none")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrivals per serving rate (s)")
+    ap.add_argument("--serve-pipelines", type=int, default=0, help="serving pipelines (0: the library default)")
     ap.add_argument("--saturation-seconds", type=float, default=6.0,
                     help="closed-loop saturation run of each serving leg (s); 0: none")
     ap.add_argument("--query-bound", type=int, default=200_000,
@@ -440,14 +441,15 @@ def _lat_summary(lat_ms, status, span_s):
 
 
 def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, saturation_s: float,
-                max_game_positions: int = 0, outstanding: int = 8192, saturation_items=None) -> dict:
+                max_game_positions: int = 0, outstanding: int = 8192, saturation_items=None,
+                n_pipelines: int = 0) -> dict:
     """One server: open-loop Poisson arrivals at each rate, then a closed-loop
     saturation run (`outstanding` requests kept in flight) over
     `saturation_items` (default: all items)."""
     from gpuequiv_b200.serving import Server
     rng = np.random.default_rng(seed)
     out = {"runs": [], "saturation": None}
-    with Server(ctx, max_game_positions=max_game_positions) as srv:
+    with Server(ctx, n_pipelines=n_pipelines, max_game_positions=max_game_positions) as srv:
         load = Load(srv, items, queries)
         # warm the pipelines (CUDA graphs, device and host pools): single
         # requests, then a burst
@@ -851,7 +853,7 @@ def run_ours(args, d: Dist):
     serving = None
     if rates or args.saturation_seconds > 0:
         serving = run_serving(ctx, views, False, rates, args.serve_seconds, 100 + 1000 * d.rank,
-                              args.saturation_seconds)
+                              args.saturation_seconds, n_pipelines=args.serve_pipelines)
         sat = serving["saturation"]
         serving["saturation_vs_plain"] = sat["throughput_games_s"] / plain_rate if sat and plain_rate else None
     # the serving configuration: equivalence queries on LTSs of 20-20,000
@@ -868,7 +870,7 @@ def run_ours(args, d: Dist):
         progress("serving: queries")
         serving_q = run_serving(ctx, pool, True, qrates, args.serve_seconds, 200 + 1000 * d.rank,
                                 args.saturation_seconds, max_game_positions=args.query_bound,
-                                outstanding=256, saturation_items=acc_idx)
+                                outstanding=256, saturation_items=acc_idx, n_pipelines=args.serve_pipelines)
         # the plain form on the same queries: one compare() call each
         acc = [pool[i] for i in acc_idx[:64]]
         for j in acc[:8]:
