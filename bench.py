@@ -980,8 +980,9 @@ def run_ours(args, d: Dist):
             "stress": stress,
             "serving": {"workload": "game requests (geq_server_submit) drawn from this batch's games: Poisson "
                                     "arrivals, then a closed loop of 8192 requests in flight (saturation); "
-                                    "geq_server with 2 pipelines, 150 GB admission budget; latency = submit -> "
-                                    "lists in the caller's hands",
+                                    f"geq_server with {args.serve_pipelines or 3} pipelines, 150 GB admission "
+                                    "budget; load from native threads; latency = submit -> lists in the "
+                                    "caller's hands",
                         **(serving or {}),
                         "queries": {"workload": f"serving configuration: Poisson arrivals of compare(p, q) queries "
                                                 f"on seeded LTSs of log-uniform 20-20,000 states (pool of "

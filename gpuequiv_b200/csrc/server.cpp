@@ -501,7 +501,8 @@ geq_status geq_server_create(geq_context *ctx, const geq_server_config *cfg, geq
   std::unique_ptr<geq_server> s(new geq_server());
   s->device = ctx->device;
   if (cfg) s->cfg = *cfg;
-  if (!s->cfg.n_pipelines) s->cfg.n_pipelines = 2;
+  // 3: measured against 2 and 4 at the saturation and arrival-rate runs
+  if (!s->cfg.n_pipelines) s->cfg.n_pipelines = 3;
   if (s->cfg.n_pipelines > 8) return fail(GEQ_ERR_INVALID_INPUT, "at most 8 pipelines");
   if (!s->cfg.max_batch_games) s->cfg.max_batch_games = 4096;
   if (!s->cfg.max_wait_us) s->cfg.max_wait_us = 200;
