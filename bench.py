@@ -59,7 +59,7 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (default launch shape)")
     ap.add_argument("--serve-rates", default="5000,10000",
                     help="Poisson arrival rates (req/s) of the game-request serving leg; empty: none")
-    ap.add_argument("--query-rates", default="200,1000",
+    ap.add_argument("--query-rates", default="200,1000,5000",
                     help="Poisson arrival rates (req/s) of the serving configuration (equivalence queries on LTSs "
                          "of 20-20,000 states); empty: none")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="arrivals per serving rate (s)")
