@@ -390,6 +390,10 @@ class Load:
     def _threads(self):
         return max(1, self.threads // 2), max(1, self.threads // 2)
 
+    # the closed loop's submitters: a submit copies its game (a few hundred
+    # KB) into the server, so a few threads are needed to keep 8,192 in flight
+    CLOSED_SUBMIT_THREADS = 8
+
     def open_loop(self, arrivals, pick):
         import ctypes as C
         n = len(arrivals)
@@ -415,7 +419,7 @@ class Load:
         st = np.full(cap, -1, np.int32)
         nsub = C.c_uint64(0)
         span = C.c_double(0.0)
-        ns, npoll = self._threads()
+        ns, npoll = max(self._threads()[0], self.CLOSED_SUBMIT_THREADS), self._threads()[1]
         r = self.ll.geq_load_closed(C.byref(self.api), pk.ctypes.data_as(C.POINTER(C.c_uint32)), len(pk),
                                     outstanding, seconds, cap, ns, npoll, 1, self.drain_s,
                                     lat.ctypes.data_as(C.POINTER(C.c_double)),

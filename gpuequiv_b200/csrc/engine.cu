@@ -2795,7 +2795,14 @@ geq_status Engine::finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out) {
     else k_pack_edges<CodecStd><<<grid, 256, 0, S>>>(D.col, D.wt, M, D.cw);
   }
   CU(cudaMemcpyAsync(&s.h_ctr->pad, s.d_err, 4, cudaMemcpyDeviceToHost, S));
+#if GEQ_PATH_PROFILE
+  const auto tw0 = std::chrono::steady_clock::now();
+#endif
   CU(cudaStreamSynchronize(S));
+#if GEQ_PATH_PROFILE
+  std::fprintf(stderr, "GEQ_UPLOAD wait_ms %.2f\n",
+               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count());
+#endif
   s.pool.put(roff, (N + 1) * 8);
   CU(cudaGetLastError());
   const uint32_t h_err = s.h_ctr->pad;
