@@ -69,7 +69,7 @@ def parse():
     ap.add_argument("--query-bound", type=int, default=200_000,
                     help="position bound of a served query's game (larger games are refused)")
     ap.add_argument("--query-pool", type=int, default=2048, help="distinct queries the arrivals draw from")
-    ap.add_argument("--large-states", type=int, default=12800,
+    ap.add_argument("--large-states", type=int, default=16000,
                     help="states of the single-LTS equivalences() leg (the large generator; 0: none)")
     ap.add_argument("--no-stress", dest="stress", action="store_false", help="skip the stress-game leg")
     ap.add_argument("--solve-only", action="store_true",
