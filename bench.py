@@ -390,9 +390,10 @@ class Load:
     def _threads(self):
         return max(1, self.threads // 2), max(1, self.threads // 2)
 
-    # the closed loop's submitters: a submit copies its game (a few hundred
-    # KB) into the server, so a few threads are needed to keep 8,192 in flight
-    CLOSED_SUBMIT_THREADS = 8
+    # the closed loop's submitters: two keep the server at its capacity
+    # (measured: eight submitters left throughput where it was, 24-37k
+    # games/s, and raised p50 from 10 ms to 145 ms by queueing)
+    CLOSED_SUBMIT_THREADS = 2
 
     def open_loop(self, arrivals, pick):
         import ctypes as C
