@@ -390,10 +390,10 @@ class Load:
     def _threads(self):
         return max(1, self.threads // 2), max(1, self.threads // 2)
 
-    # the closed loop's submitters: two keep the server at its capacity
-    # (measured: eight submitters left throughput where it was, 24-37k
-    # games/s, and raised p50 from 10 ms to 145 ms by queueing)
-    CLOSED_SUBMIT_THREADS = 2
+    # the closed loop's submitters: a submit copies its game (a few hundred
+    # KB) into the server; two threads cannot keep 8,192 requests in flight
+    # (measured: 37k games/s with a shallow queue), eight can
+    CLOSED_SUBMIT_THREADS = 8
 
     def open_loop(self, arrivals, pick):
         import ctypes as C
@@ -463,7 +463,7 @@ def run_serving(ctx, items, queries: bool, rates, seconds: float, seed: int, sat
         load.open_loop(np.zeros(len(warm)), warm)
         if saturation_s > 0:  # the page-locked input pool up to the saturation run's depth
             load.closed_loop(np.arange(len(items)) if saturation_items is None
-                             else np.asarray(saturation_items, np.int64), outstanding, 1.5)
+                             else np.asarray(saturation_items, np.int64), outstanding, 3.0)
         for lam in rates:
             n = max(1, int(rng.poisson(lam * seconds)))
             arrivals = np.sort(rng.uniform(0, seconds, n))

@@ -504,7 +504,9 @@ geq_status geq_server_create(geq_context *ctx, const geq_server_config *cfg, geq
   // 3: measured against 2 and 4 at the saturation and arrival-rate runs
   if (!s->cfg.n_pipelines) s->cfg.n_pipelines = 3;
   if (s->cfg.n_pipelines > 8) return fail(GEQ_ERR_INVALID_INPUT, "at most 8 pipelines");
-  if (!s->cfg.max_batch_games) s->cfg.max_batch_games = 4096;
+  // 512: at saturation (a deep queue) batches of 512 games gave more games/s
+  // and a shorter tail than batches of 256 or 4,096
+  if (!s->cfg.max_batch_games) s->cfg.max_batch_games = 512;
   if (!s->cfg.max_wait_us) s->cfg.max_wait_us = 200;
   if (!s->cfg.hbm_budget_bytes) s->cfg.hbm_budget_bytes = 150ull * 1000 * 1000 * 1000;
   if (!s->cfg.max_queued) s->cfg.max_queued = 1000000;

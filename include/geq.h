@@ -263,7 +263,7 @@ void geq_device_games_free(geq_device_games *dg);
 typedef struct geq_server geq_server;
 typedef struct geq_server_config {
   uint32_t n_pipelines;       /* pipeline threads/streams (0: 3) */
-  uint32_t max_batch_games;   /* requests per batch at most (0: 4096) */
+  uint32_t max_batch_games;   /* requests per batch at most (0: 512) */
   uint32_t max_wait_us;       /* a pipeline waits this long for more requests
                                  once it holds fewer than max_batch_games (0: 200) */
   uint32_t max_game_positions; /* compare queries: a query whose game would have more
