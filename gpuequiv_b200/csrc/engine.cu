@@ -342,7 +342,10 @@ struct WarpCtx {
 
 // Successor of edge k: its update and list descriptor (lane-local).
 // ---- antichains in lane-private shared-memory columns ----------------------
-constexpr uint32_t TK = 16;   // antichain members per column
+#ifndef GEQ_LANE_TK
+#define GEQ_LANE_TK 16
+#endif
+constexpr uint32_t TK = GEQ_LANE_TK;  // antichain members per column
 constexpr uint32_t TD = 16;   // successors per lane
 constexpr uint32_t TW = 64;   // candidates (attacker) / combinations per step (defender)
 constexpr int TSCR = 2 * TK;  // scratch words per lane: two antichain columns
