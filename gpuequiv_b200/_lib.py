@@ -83,7 +83,6 @@ TUNE_BUILD_WARP_ALL = 64
 TUNE_FORCE_WIDE = 128
 TUNE_READY = 256
 TUNE_NO_EDGE_PAIRS = 512
-TUNE_SORT_CHUNKS = 1024
 
 STATUS = {0: "OK", 1: "NO_DEVICE", 2: "OUT_OF_MEMORY", 3: "INVALID_INPUT", 4: "TIMEOUT",
           5: "UNSUPPORTED", 6: "CUDA", 7: "IO", 8: "PARSE", 9: "BUSY", 10: "INTERNAL"}

@@ -158,7 +158,6 @@ struct KParams {
   // per defender: successors whose list is still empty (null: not counted,
   // every predecessor of a changed position is pushed)
   uint32_t *missing;
-  uint32_t sort_chunks;  // k_sort_chunks orders each 256-slot chunk of the frontier
 };
 
 // Energy-list descriptors (one u64 per position):
@@ -1569,61 +1568,6 @@ __global__ void k_ffill(const KParams p) {
     if (c->overflow) c->halt = 1u;
   }
 }
-// GEQ_TUNE_SORT_CHUNKS: every chunk of 256 frontier slots reordered, stably,
-// by (kind, successor count): the lanes of a warp then meet positions of one
-// kind and similar degree, while a chunk keeps the neighbourhood that the
-// position order gives.  The order inside a round does not change what a
-// round computes (every position reads the previous round's lists).
-__global__ void __launch_bounds__(256) k_sort_chunks(const KParams p) {
-  Ctr *c = p.ctr;
-  if (!p.sort_chunks || c->halt) return;
-  __shared__ uint32_t hist[8][64];
-  __shared__ uint32_t base[64];
-  __shared__ uint32_t vals[256];
-  const uint32_t cur = c->cur;
-  const uint32_t fs = c->fsize[cur];
-  uint32_t *F = cur ? p.front1 : p.front0;
-  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  for (uint32_t c0 = blockIdx.x * 256u; c0 < fs; c0 += gridDim.x * 256u) {
-    const uint32_t sl = c0 + threadIdx.x;
-    const bool act = sl < fs;
-    const uint32_t v = act ? F[sl] : 0u;
-    uint32_t key = 63u;  // past the chunk's end: after every position
-    if (act && CHECK_IDX(c, v, p.n_nodes)) {
-      const uint32_t deg = min(p.row[v + 1] - p.row[v], 30u);
-      key = (p.flags[v] & 1u) ? deg : 32u + deg;
-    }
-    for (uint32_t i = threadIdx.x; i < 8u * 64u; i += 256u) (&hist[0][0])[i] = 0u;
-    __syncthreads();
-    const uint32_t peers = __match_any_sync(FULL, key);
-    const uint32_t rank = (uint32_t)__popc(peers & lanemask_lt());
-    if (rank == 0u) hist[warp][key] = (uint32_t)__popc(peers);
-    __syncthreads();
-    if (warp == 0) {
-      // exclusive scan over the 64 keys of their counts in all warps
-      uint32_t a = 0, b = 0;
-      for (int w = 0; w < 8; w++) {
-        a += hist[w][lane];
-        b += hist[w][lane + 32u];
-      }
-      const uint32_t ia = warp_incl_scan(a, lane);
-      const uint32_t ta = __shfl_sync(FULL, ia, 31);
-      const uint32_t ib = warp_incl_scan(b, lane);
-      base[lane] = ia - a;
-      base[lane + 32u] = ta + ib - b;
-    }
-    __syncthreads();
-    if (act) {
-      uint32_t off = base[key] + rank;
-      for (uint32_t w = 0; w < warp; w++) off += hist[w][key];
-      if (off < 256u) vals[off] = v;
-    }
-    __syncthreads();
-    if (act) F[sl] = vals[threadIdx.x];
-    __syncthreads();
-  }
-}
-
 // Attacker positions as a bitmap (frontier ordering by kind).
 __global__ void k_abits(const uint8_t *flags, unsigned long long n, uint32_t words, uint32_t *abits) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < words; i += gridDim.x * blockDim.x) {
@@ -2879,7 +2823,6 @@ geq_status Engine::finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out) {
   kp.bigq = D.bigq;
   kp.cw = D.cw;
   kp.missing = nullptr;
-  kp.sort_chunks = 0;
   kp.el = D.conf.elements; kp.mx = D.conf.max; kp.eb = D.conf.energy_bits(); kp.em = D.conf.energy_mask();
   kp.ub = D.conf.update_bits(); kp.um = D.conf.update_mask();
   kp.small_limit = (tuning.flags & GEQ_TUNE_FORCE_LARGE) ? 0u : std::min<uint32_t>(tuning.small_limit, 32);
@@ -2947,7 +2890,6 @@ static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent
   if (eb) cudaEventRecord(eb, S);
   k_commit<<<kp.fblocks, 256, 0, S>>>(kp);
   k_ffill<<<kp.fblocks, 256, 0, S>>>(kp);
-  k_sort_chunks<<<(unsigned)std::max(1, E.n_sms * 4), 256, 0, S>>>(kp);
 }
 
 // One captured graph of R rounds per codec, shared by every upload: before a
@@ -3019,7 +2961,6 @@ geq_status Engine::solve_begin(DeviceGamesImpl &dg) {
   if (dg.next_stamp > 0xF0000000u) dg.next_stamp = 1;
   CU(cudaMemsetAsync(dg.mark, 0, 2ull * dg.kp.mwords * 4, S));
   dg.kp.cw = (tuning.flags & GEQ_TUNE_NO_EDGE_PAIRS) ? nullptr : dg.cw;
-  dg.kp.sort_chunks = (tuning.flags & GEQ_TUNE_SORT_CHUNKS) ? 1u : 0u;
   // GEQ_TUNE_READY: defenders wait for their successors' lists (counted per
   // defender, set up at the first such solve); else every predecessor of a
   // changed position is pushed, as the reference's visit lists do
@@ -3049,8 +2990,7 @@ geq_status Engine::solve_begin(DeviceGamesImpl &dg) {
     }
     k_fcount<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
     k_ffill<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
-    k_sort_chunks<<<(unsigned)std::max(1, n_sms * 4), 256, 0, S>>>(dg.kp);
-    pr.launches += 4;
+    pr.launches += 3;
   } else if (dg.n_reach) {
     const unsigned grid = (unsigned)std::max<unsigned long long>(
         1, std::min<unsigned long long>((dg.n_reach + 7) / 8, (unsigned long long)n_sms * 16));
@@ -3062,8 +3002,7 @@ geq_status Engine::solve_begin(DeviceGamesImpl &dg) {
     }
     k_fcount<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
     k_ffill<<<dg.kp.fblocks, 256, 0, S>>>(dg.kp);
-    k_sort_chunks<<<(unsigned)std::max(1, n_sms * 4), 256, 0, S>>>(dg.kp);
-    pr.launches += 4;
+    pr.launches += 3;
   }
   CU(cudaGetLastError());
   return GEQ_OK;
@@ -3199,7 +3138,7 @@ geq_status Engine::step_enqueue(DeviceGamesImpl &dg, bool active) {
     if (dg.generic) launch_round<CodecGen>(*this, dg.kp, S, ea, eb);
     else launch_round<CodecStd>(*this, dg.kp, S, ea, eb);
   }
-  pr.launches += 5ull * R;
+  pr.launches += 4ull * R;
   CU(cudaMemcpyAsync(dg.hstep.p, dg.ctr, sizeof(Ctr), cudaMemcpyDeviceToHost, S));
   dg.step_active = active && dg.n_games > 0;
   if (dg.step_active) {

@@ -340,7 +340,6 @@ typedef struct geq_tuning {
                                      only once it has none (the reference visits and skips it); measured
                                      slower on the spectroscopy batch, off by default */
 #define GEQ_TUNE_NO_EDGE_PAIRS 512u /* the lane path reads col / wt and decodes updates (cross-check) */
-#define GEQ_TUNE_SORT_CHUNKS 1024u  /* every 256 frontier slots reordered by (kind, successor count) */
 geq_status geq_context_set_tuning(geq_context *ctx, const geq_tuning *t);
 void geq_context_get_tuning(const geq_context *ctx, geq_tuning *t);
 

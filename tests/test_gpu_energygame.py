@@ -30,8 +30,6 @@ MODES = {
     "lanes_small": dict(lane_limits=(4, 8, 4)),
     # defenders pushed only once every successor has energies
     "ready": dict(flags=256),
-    # frontier chunks reordered by (kind, successor count)
-    "sorted_chunks": dict(flags=1024),
 }
 
 
