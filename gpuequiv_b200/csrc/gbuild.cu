@@ -24,6 +24,11 @@ namespace geq {
 namespace gb {
 
 constexpr int EACH_T = 256;
+// blocks per SM of the level kernels' grids (grid-stride loops over the
+// level's items; the count is only known on the device)
+#ifndef GEQ_EACH_BLOCKS_PER_SM
+#define GEQ_EACH_BLOCKS_PER_SM 8
+#endif
 constexpr int SCAN_T = 256;
 constexpr int SCAN_ITEMS = 8;
 constexpr uint32_t SCAN_TILE = SCAN_T * SCAN_ITEMS;
@@ -513,7 +518,8 @@ struct DevBackend {
   }
   // ---- device-counted launches (the level loop) ----
   uint32_t grid_for(uint32_t cap) const {
-    return std::max<uint32_t>(1, std::min<uint32_t>((cap + EACH_T - 1) / EACH_T, (uint32_t)n_sms * 8));
+    return std::max<uint32_t>(
+        1, std::min<uint32_t>((cap + EACH_T - 1) / EACH_T, (uint32_t)n_sms * GEQ_EACH_BLOCKS_PER_SM));
   }
   template <class F>
   void each_d(const unsigned long long *np, uint32_t cap, const unsigned long long *go, const F &f) {
