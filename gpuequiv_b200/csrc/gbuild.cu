@@ -272,6 +272,9 @@ __global__ void __launch_bounds__(SCAN_T) k_lbscan(ScanR a, const unsigned long 
 // splits are placed by ballots in the reference's order.  Same output as
 // gen_one.
 constexpr int GH_WARPS = 8;
+#ifndef GEQ_GH_BLOCKS_PER_SM
+#define GEQ_GH_BLOCKS_PER_SM 2  // k_gen_heavy blocks per SM (32 KB of shared memory each)
+#endif
 constexpr uint32_t GH_BM_WORDS = 1024;  // jobs of up to 32768 states; larger ones: gen_one by lane 0
 constexpr uint32_t FULLMASK = 0xffffffffu;
 
@@ -513,7 +516,7 @@ struct DevBackend {
   }
   void gen_heavy(const View &v, const unsigned long long *go) {
     if (v.heavy_min == 0xffffffffu) return;
-    k_gen_heavy<<<(unsigned)n_sms * 2, GH_WARPS * 32, 0, s>>>(v, go);
+    k_gen_heavy<<<(unsigned)n_sms * GEQ_GH_BLOCKS_PER_SM, GH_WARPS * 32, 0, s>>>(v, go);
     launches++;
   }
   // ---- device-counted launches (the level loop) ----
