@@ -272,8 +272,11 @@ __global__ void __launch_bounds__(SCAN_T) k_lbscan(ScanR a, const unsigned long 
 // splits are placed by ballots in the reference's order.  Same output as
 // gen_one.
 constexpr int GH_WARPS = 8;
+#ifndef GEQ_BUILD_HEAVY_MIN
+#define GEQ_BUILD_HEAVY_MIN 4  // attack positions with this many q's or more take the warp path
+#endif
 #ifndef GEQ_GH_BLOCKS_PER_SM
-#define GEQ_GH_BLOCKS_PER_SM 2  // k_gen_heavy blocks per SM (32 KB of shared memory each)
+#define GEQ_GH_BLOCKS_PER_SM 4  // k_gen_heavy blocks per SM (32 KB of shared memory each); measured: 2 → 72.5 ms, 4 → 67.6, 6 → 69.1 per build of the batch
 #endif
 constexpr uint32_t GH_BM_WORDS = 1024;  // jobs of up to 32768 states; larger ones: gen_one by lane 0
 constexpr uint32_t FULLMASK = 0xffffffffu;
@@ -760,7 +763,7 @@ static geq_status device_build(Engine &eng, int device, uint32_t n_jobs, const L
   in.jsb = (const uint32_t *)(db.din + o_jsb);
   in.max_pos = max_pos;
   // attack positions with at least this many q's take the warp path
-  in.heavy_min = (eng.tuning.flags & GEQ_TUNE_BUILD_WARP_ALL) ? 1u : 4u;
+  in.heavy_min = (eng.tuning.flags & GEQ_TUNE_BUILD_WARP_ALL) ? 1u : (uint32_t)GEQ_BUILD_HEAVY_MIN;
   if (staged) {
     *staged = in;
     db.upload_ms = std::chrono::duration<double, std::milli>(clk::now() - t0).count();
