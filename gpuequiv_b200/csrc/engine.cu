@@ -342,6 +342,11 @@ struct WarpCtx {
 
 // Successor of edge k: its update and list descriptor (lane-local).
 // ---- antichains in lane-private shared-memory columns ----------------------
+// blocks per SM of k_commit / k_fcount / k_ffill (each owns a slice of the
+// frontier bitmap)
+#ifndef GEQ_FRONTIER_BLOCKS_PER_SM
+#define GEQ_FRONTIER_BLOCKS_PER_SM 2
+#endif
 #ifndef GEQ_LANE_TK
 #define GEQ_LANE_TK 16
 #endif
@@ -2743,7 +2748,7 @@ geq_status Engine::alloc_work(DeviceGamesImpl &D, bool any_init) {
   if (!D.alloc(D.rrow, N + 1) || !D.alloc(D.rcol, M) || !D.alloc(D.desc, N) ||
       (!any_init && !D.alloc(D.desc_init, N)) || !D.alloc(D.slot_new, N) || !D.alloc(D.mark, 2 * ((N + 31) / 32)) ||
       !D.alloc(D.front0, N) || !D.alloc(D.front1, N) || !D.alloc(D.ctr, 1) ||
-      !D.alloc(D.fpart, 2 * (size_t)std::max(1, n_sms * 2)) || !D.alloc(D.abits, (N + 31) / 32) ||
+      !D.alloc(D.fpart, 2 * (size_t)std::max(1, n_sms * GEQ_FRONTIER_BLOCKS_PER_SM)) || !D.alloc(D.abits, (N + 31) / 32) ||
       !D.alloc(D.bigq, N) || !D.alloc(D.cw, M))
     return fail(GEQ_ERR_OUT_OF_MEMORY, "device allocation for %llu positions / %llu edges failed", N, M);
   unsigned long long cap = std::max<unsigned long long>(4ull * (D.init_total + N) + (1ull << 20), 1ull << 22);
@@ -2818,7 +2823,7 @@ geq_status Engine::finish_upload(GamesPtr &dg, bool any_init, GamesPtr &out) {
   kp.slot_new = D.slot_new; kp.ctr = D.ctr; kp.n_nodes = N; kp.n_edges = M;
   kp.mwords = (uint32_t)((N + 31) / 32);
   kp.fpart = D.fpart;
-  kp.fblocks = (uint32_t)std::max(1, n_sms * 2);
+  kp.fblocks = (uint32_t)std::max(1, n_sms * GEQ_FRONTIER_BLOCKS_PER_SM);
   kp.abits = D.abits;
   kp.bigq = D.bigq;
   kp.cw = D.cw;
