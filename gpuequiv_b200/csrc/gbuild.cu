@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(SCAN_T) k_lbscan(ScanR a, const unsigned long 
 // gen_one.
 constexpr int GH_WARPS = 8;
 #ifndef GEQ_BUILD_HEAVY_MIN
-#define GEQ_BUILD_HEAVY_MIN 4  // attack positions with this many q's or more take the warp path
+#define GEQ_BUILD_HEAVY_MIN 6  // attack positions with this many q's or more take the warp path; measured: 2 → 70.4 ms, 3 → 68.2, 4 → 66.6, 6 → 64.8, 8 → 64.7, 12 → 66.0 per build of the batch
 #endif
 #ifndef GEQ_GH_BLOCKS_PER_SM
 #define GEQ_GH_BLOCKS_PER_SM 4  // k_gen_heavy blocks per SM (32 KB of shared memory each); measured: 2 → 72.5 ms, 4 → 67.6, 6 → 69.1 per build of the batch
