@@ -15,7 +15,7 @@ import os
 
 from .energygame import Context, DeviceGames
 
-CANDIDATES = [(bps, r) for bps in (3, 4, 5) for r in (4, 8, 16)]
+CANDIDATES = [(bps, r) for bps in (3, 4, 5) for r in (4, 8, 16, 32)]
 # (successors, candidates per step, list length) of the lane path
 LANE_LIMITS = [(16, 64, 16), (16, 32, 16), (16, 16, 16), (8, 64, 16), (8, 32, 16), (16, 64, 8), (12, 48, 12)]
 
