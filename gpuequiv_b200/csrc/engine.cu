@@ -345,7 +345,7 @@ struct WarpCtx {
 // blocks per SM of k_commit / k_fcount / k_ffill (each owns a slice of the
 // frontier bitmap)
 #ifndef GEQ_FRONTIER_BLOCKS_PER_SM
-#define GEQ_FRONTIER_BLOCKS_PER_SM 4  // measured: 1 → 36.7 ms, 2 → 35.3, 4 → 34.5 per solve of the batch
+#define GEQ_FRONTIER_BLOCKS_PER_SM 8  // measured: 1 → 36.7 ms, 2 → 35.3, 4 → 34.5-34.7, 6 → 34.4, 8 → 34.1-34.3 per solve of the batch
 #endif
 #ifndef GEQ_LANE_TK
 #define GEQ_LANE_TK 16

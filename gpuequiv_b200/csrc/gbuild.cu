@@ -30,7 +30,10 @@ constexpr int EACH_T = 256;
 #define GEQ_EACH_BLOCKS_PER_SM 16  // measured: 2 → 99 ms, 4 → 80.5, 8 → 74.4, 12 → 73.0, 16 → 72.3 per build of the batch
 #endif
 constexpr int SCAN_T = 256;
-constexpr int SCAN_ITEMS = 8;
+#ifndef GEQ_SCAN_ITEMS
+#define GEQ_SCAN_ITEMS 8  // values per thread of a scan tile
+#endif
+constexpr int SCAN_ITEMS = GEQ_SCAN_ITEMS;
 constexpr uint32_t SCAN_TILE = SCAN_T * SCAN_ITEMS;
 
 template <class F>
