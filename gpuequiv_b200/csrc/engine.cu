@@ -3419,6 +3419,21 @@ geq_status run_batch_pipelined(int device, Engine &ea, Engine &eb, std::vector<G
   a_up.set_value();
   if (!st_a) st_a = ea.solve(*da, &sa);
   if (!st_a) st_a = ea.download_prepare(*da, ra);
+  // the first half's lists go to the host while the second half may still
+  // be solving: the offsets' size is known (every position of the batch),
+  // the words are not, so the data block is sized from the first half's
+  // total scaled to the second half's positions, with headroom, and
+  // replaced below when the second half needs more
+  const uint64_t na = da ? da->N + da->n_games : 0;
+  const uint64_t n_off = total + n_games;
+  if (!st_a) {
+    const double scale = (double)(total - da->N) / (double)std::max<uint64_t>(1, da->N);
+    const uint64_t guess = ra.total + (uint64_t)((double)ra.total * scale * 1.25) + (1u << 20);
+    if (!sol.off_buf.alloc(ea.st->hpool, n_off * 8) || !sol.data_buf.alloc(ea.st->hpool, guess * 4))
+      st_a = fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu result words", (unsigned long long)guess);
+    else
+      st_a = ea.download_copy(*da, ra, (uint64_t *)sol.off_buf.p, (uint32_t *)sol.data_buf.p);
+  }
   tb.join();
   if (st_a || st_b) {
     if (da) ea.download_release(*da, ra);
@@ -3427,19 +3442,22 @@ geq_status run_batch_pipelined(int device, Engine &ea, Engine &eb, std::vector<G
     return st_a ? st_a : st_b;
   }
   sol.energy_size = 1;
-  const uint64_t na = da->N + da->n_games;
-  sol.n_offsets = na + db->N + db->n_games;
+  sol.n_offsets = n_off;
   sol.n_words = ra.total + rb.total;
-  if (!sol.off_buf.alloc(ea.st->hpool, sol.n_offsets * 8) || !sol.data_buf.alloc(ea.st->hpool, sol.n_words * 4)) {
-    ea.download_release(*da, ra);
-    eb.download_release(*db, rb);
-    return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu result words", (unsigned long long)sol.n_words);
+  if (sol.data_buf.cap < sol.n_words * 4) {
+    HostBuf bigger;
+    if (!bigger.alloc(ea.st->hpool, sol.n_words * 4)) {
+      eb.download_release(*db, rb);
+      return fail(GEQ_ERR_OUT_OF_MEMORY, "host memory for %llu result words", (unsigned long long)sol.n_words);
+    }
+    std::memcpy(bigger.p, sol.data_buf.p, ra.total * 4);
+    std::swap(sol.data_buf.p, bigger.p);
+    std::swap(sol.data_buf.cap, bigger.cap);
+    std::swap(sol.data_buf.pool, bigger.pool);
   }
   uint64_t *off = (uint64_t *)sol.off_buf.p;
   uint32_t *data = (uint32_t *)sol.data_buf.p;
-  geq_status st = ea.download_copy(*da, ra, off, data);
-  if (!st) st = eb.download_copy(*db, rb, off + na, data + ra.total);
-  else eb.download_release(*db, rb);
+  geq_status st = eb.download_copy(*db, rb, off + na, data + ra.total);
   if (st) return st;
   sol.n_vertices.resize(n_games);
   sol.offsets_base.resize(n_games);

@@ -95,3 +95,45 @@ def test_split_batch_matches_one_engine(geq, ctx):
         exp = canonical(sol.offsets, sol.data)
         got = canonical(offs[i], data[i])
         assert np.array_equal(got[0], exp[0]) and np.array_equal(got[1], exp[1]), f"game {i} differs from the oracle"
+
+
+def test_split_batch_result_block_grows(geq, ctx):
+    """The two-halves form copies the first half's lists to the host while
+    the second half solves, into a block sized from the first half; here the
+    first half has no energies at all and the second many (every attacker
+    ends with six incomparable unit energies), so the block must grow: the
+    lists still equal those of one engine, and the expected ones."""
+    from gpuequiv_b200._lib import TUNE_NO_SPLIT
+    conf = geq.EnergyConf.STANDARD
+    graphs = []
+    for _ in range(2):  # attackers without moves: empty lists
+        n = 600_000
+        graphs.append(geq.GameGraph.from_csr(np.zeros(n + 1, np.uint32), np.zeros(0, np.uint32),
+                                             np.zeros(0, np.uint32), np.ones(n, np.uint8), conf))
+    m = 180_000  # attackers, each with six defender sinks behind decrements of dims 0..5
+    n = 7 * m
+    row = np.zeros(n + 1, np.uint32)
+    row[1:m + 1] = 6 * np.arange(1, m + 1, dtype=np.uint32)
+    row[m + 1:] = 6 * m
+    col = (m + np.arange(6 * m, dtype=np.uint32)).astype(np.uint32)
+    wt = (np.uint32(1) << (4 * np.tile(np.arange(6, dtype=np.uint32), m))).astype(np.uint32)
+    att = np.zeros(n, np.uint8)
+    att[:m] = 1
+    graphs.append(geq.GameGraph.from_csr(row, col, wt, att, conf))
+    assert sum(g.n_vertices() for g in graphs) >= 2 ** 21
+    offs, data, stats = geq.run_batch_raw(graphs, ctx)
+    ctx.set_tuning(flags=TUNE_NO_SPLIT)
+    try:
+        offs1, data1, _ = geq.run_batch_raw(graphs, ctx)
+    finally:
+        ctx.set_tuning()
+    for i in range(len(graphs)):
+        a, b = canonical(offs[i], data[i]), canonical(offs1[i], data1[i])
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]), f"game {i} differs"
+    assert int(offs[0][-1]) == 0 and int(offs[1][-1]) == 0
+    o, d = np.asarray(offs[2], np.int64), np.asarray(data[2]).reshape(-1)
+    assert np.all(np.diff(o[:m + 1]) == 6) and np.all(np.diff(o[m:]) == 1)
+    units = sorted(1 << (2 * k) for k in range(6))
+    for v in (0, m // 2, m - 1):
+        assert sorted(int(x) for x in d[o[v]:o[v + 1]]) == units
+    assert not d[o[m]:].any()  # the sinks: the zero energy
