@@ -3407,18 +3407,32 @@ geq_status run_batch_pipelined(int device, Engine &ea, Engine &eb, std::vector<G
   std::string err_b;
   std::promise<void> a_up;
   std::future<void> a_up_done = a_up.get_future();
+#if GEQ_PATH_PROFILE
+  const auto tp0 = std::chrono::steady_clock::now();
+  double tl[12] = {};
+  auto mark = [&](int i) { tl[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp0).count(); };
+#else
+  auto mark = [](int) {};
+#endif
   std::thread tb([&]() {
     cudaSetDevice(device);
     a_up_done.wait();
+    mark(5);
     st_b = eb.upload(ib, db);
+    mark(6);
     if (!st_b) st_b = eb.solve(*db, &sb);
+    mark(7);
     if (!st_b) st_b = eb.download_prepare(*db, rb);
+    mark(8);
     if (st_b) err_b = geq_last_error();
   });
   st_a = ea.upload(ia, da);
+  mark(0);
   a_up.set_value();
   if (!st_a) st_a = ea.solve(*da, &sa);
+  mark(1);
   if (!st_a) st_a = ea.download_prepare(*da, ra);
+  mark(2);
   // the first half's lists go to the host while the second half may still
   // be solving: the offsets' size is known (every position of the batch),
   // the words are not, so the data block is sized from the first half's
@@ -3434,7 +3448,9 @@ geq_status run_batch_pipelined(int device, Engine &ea, Engine &eb, std::vector<G
     else
       st_a = ea.download_copy(*da, ra, (uint64_t *)sol.off_buf.p, (uint32_t *)sol.data_buf.p);
   }
+  mark(3);
   tb.join();
+  mark(4);
   if (st_a || st_b) {
     if (da) ea.download_release(*da, ra);
     if (db) eb.download_release(*db, rb);
@@ -3459,6 +3475,13 @@ geq_status run_batch_pipelined(int device, Engine &ea, Engine &eb, std::vector<G
   uint32_t *data = (uint32_t *)sol.data_buf.p;
   geq_status st = eb.download_copy(*db, rb, off + na, data + ra.total);
   if (st) return st;
+  mark(9);
+#if GEQ_PATH_PROFILE
+  std::fprintf(stderr,
+               "GEQ_SPLIT a_up %.1f a_solve %.1f a_prep %.1f a_copy %.1f join %.1f | b_start %.1f b_up %.1f b_solve %.1f "
+               "b_prep %.1f | b_copy %.1f\n",
+               tl[0], tl[1], tl[2], tl[3], tl[4], tl[5], tl[6], tl[7], tl[8], tl[9]);
+#endif
   sol.n_vertices.resize(n_games);
   sol.offsets_base.resize(n_games);
   sol.data_base.resize(n_games);
