@@ -139,7 +139,7 @@ class Dist:
 
 # ---- clocks ---------------------------------------------------------------------
 class Clocks:
-    """nvidia-smi sampled every 200 ms during the timed region."""
+    """nvidia-smi sampled every 50 ms during the timed region."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -147,11 +147,24 @@ class Clocks:
 
     def __init__(self, gpu: int):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.skip = 0
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200", "-i", str(gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "50", "-i", str(gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+
+    def start(self) -> None:
+        """Wait (at most 2 s) until the sampler runs; samples taken before
+        this call are not counted."""
+        t_end = time.perf_counter() + 2.0
+        while self.p and time.perf_counter() < t_end:
+            with open(self.f.name) as g:
+                n = sum(1 for _ in g)
+            if n:
+                self.skip = n
+                return
+            time.sleep(0.02)
 
     def stop(self) -> dict:
         if self.p:
@@ -164,7 +177,7 @@ class Clocks:
         self.f.seek(0)
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.f.read().splitlines():
+        for line in self.f.read().splitlines()[self.skip:]:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -786,8 +799,9 @@ def run_ours(args, d: Dist):
         dg.close()
         ctx.close()
         return
-    d.barrier()
     clocks = Clocks(d.local_rank)
+    clocks.start()
+    d.barrier()
     dev_ms, launches, st_last = 0.0, 0, None
     t0 = time.perf_counter()
     for _ in range(args.steps):
