@@ -347,6 +347,10 @@ struct WarpCtx {
 #ifndef GEQ_FRONTIER_BLOCKS_PER_SM
 #define GEQ_FRONTIER_BLOCKS_PER_SM 8  // measured: 1 → 36.7 ms, 2 → 35.3, 4 → 34.5-34.7, 6 → 34.4, 8 → 34.1-34.3 per solve of the batch
 #endif
+// resident blocks per SM of k_round_big (its register budget and grid)
+#ifndef GEQ_BIG_BLOCKS_PER_SM
+#define GEQ_BIG_BLOCKS_PER_SM 3
+#endif
 #ifndef GEQ_LANE_TK
 #define GEQ_LANE_TK 16
 #endif
@@ -1333,7 +1337,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) k_round(const KParams p) {
 // The large positions k_round queued: one warp per position with the warp
 // routines (tree fold, register and bitmap paths), then its predecessors.
 template <class Cd>
-__global__ void __launch_bounds__(BLOCK, 3) k_round_big(const KParams p) {
+__global__ void __launch_bounds__(BLOCK, GEQ_BIG_BLOCKS_PER_SM) k_round_big(const KParams p) {
   __shared__ uint32_t smem[WARPS_PER_BLOCK * SM_WORDS];
   __shared__ uint32_t tscr[WARPS_PER_BLOCK * TSCR * 32];
   Ctr *c = p.ctr;
@@ -2891,7 +2895,7 @@ static void launch_round(Engine &E, const KParams &kp, cudaStream_t S, cudaEvent
   else if (bps == 3) k_round<Cd, 3><<<grid, BLOCK, 0, S>>>(kp);
   else if (bps == 4) k_round<Cd, 4><<<grid, BLOCK, 0, S>>>(kp);
   else k_round<Cd, 5><<<grid, BLOCK, 0, S>>>(kp);
-  k_round_big<Cd><<<(unsigned)std::max(1, E.n_sms * 3), BLOCK, 0, S>>>(kp);
+  k_round_big<Cd><<<(unsigned)std::max(1, E.n_sms * GEQ_BIG_BLOCKS_PER_SM), BLOCK, 0, S>>>(kp);
   if (eb) cudaEventRecord(eb, S);
   k_commit<<<kp.fblocks, 256, 0, S>>>(kp);
   k_ffill<<<kp.fblocks, 256, 0, S>>>(kp);
