@@ -349,7 +349,7 @@ struct WarpCtx {
 #endif
 // resident blocks per SM of k_round_big (its register budget and grid)
 #ifndef GEQ_BIG_BLOCKS_PER_SM
-#define GEQ_BIG_BLOCKS_PER_SM 4  // measured: 2 → 36.2 ms, 3 → 34.2, 4 → 33.5 per solve of the batch (5 spills)
+#define GEQ_BIG_BLOCKS_PER_SM 4  // measured: 2 → 36.2 ms, 3 → 34.2, 4 → 33.5-33.7, 5 → 33.55 (with spills) per solve of the batch
 #endif
 #ifndef GEQ_LANE_TK
 #define GEQ_LANE_TK 16
