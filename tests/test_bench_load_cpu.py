@@ -96,3 +96,24 @@ def test_closed_loop_keeps_outstanding_bounded():
     assert len(lat) == len(status) > 50 and (status >= 0).all()
     assert fake.max_seen <= 16
     assert lat.max() < 1000
+
+
+def test_refused_submits_are_recorded_at_once():
+    """A submit that fails (a full queue, a malformed game) is recorded with
+    its status and never waited for."""
+    fake = FakeServer(lambda k: 0.001)
+    real_submit = fake.submit
+
+    def submit(ctx, item, t):
+        if item == 1:
+            t[0] = 0
+            return 7  # GEQ_ERR_BUSY
+        return real_submit(ctx, item, t)
+
+    fake.cb = (bench.LoadApi.SUBMIT(submit),) + fake.cb[1:]
+    fake.api = bench.LoadApi.Api(None, *fake.cb)
+    pick = np.array([0, 1] * 50, np.int64)
+    lat, status, span = make_load(fake, drain_s=2.0).open_loop(np.linspace(0, 0.05, 100), pick)
+    assert (status[pick == 1] == 7).all()
+    assert (status[pick == 0] >= 0).all() and (status[pick == 0] != 7).all()
+    assert span < 3
